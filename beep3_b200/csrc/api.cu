@@ -1,0 +1,427 @@
+// C ABI entry points (declared in include/beep3_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace bp {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+Ctx* as_ctx(bp_ctx c) { return reinterpret_cast<Ctx*>(c); }
+Problem* as_problem(bp_problem p) { return reinterpret_cast<Problem*>(p); }
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) BP_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Structure-of-arrays copy of [n][7] points: 7 arrays of n values.
+template <typename T>
+std::vector<T> soa7(const std::vector<double>& aos) {
+  const size_t n = aos.size() / 7;
+  std::vector<T> out(aos.size());
+  for (size_t i = 0; i < n; ++i)
+    for (int f = 0; f < 7; ++f) out[f * n + i] = (T)aos[7 * i + f];
+  return out;
+}
+
+void check_points(const char* what, int n, const int32_t* off, const double* pts, std::vector<int32_t>& h_off,
+                  std::vector<double>& h_pts) {
+  if (!off || !pts) throw std::invalid_argument(std::string(what) + ": missing point list");
+  h_off.assign(off, off + n + 1);
+  if (h_off[0] != 0) throw std::invalid_argument(std::string(what) + ": offsets must start at 0");
+  for (int i = 0; i < n; ++i)
+    if (h_off[i + 1] <= h_off[i]) throw std::invalid_argument(std::string(what) + ": every patch needs points");
+  h_pts.assign(pts, pts + 7 * (size_t)h_off[n]);
+  for (double v : h_pts)
+    if (!std::isfinite(v)) throw std::invalid_argument(std::string(what) + ": non-finite point data");
+}
+
+}  // namespace
+}  // namespace bp
+
+using namespace bp;
+
+extern "C" {
+
+BP_API const char* bp_last_error(void) { return g_last_error.c_str(); }
+BP_API int32_t bp_abi_version(void) { return BP_ABI_VERSION; }
+
+BP_API int32_t bp_ctx_create(int32_t device, uint64_t hbm_budget_bytes, bp_ctx* out) {
+  return guarded_engine([&]() -> int32_t {
+    if (!out) return fail(BP_ERR_INVALID, "bp_ctx_create: null out");
+    int ndev = 0;
+    BP_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(BP_ERR_INVALID, "bp_ctx_create: no such device");
+    DeviceGuard g(device);
+    auto c = new Ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    BP_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    BP_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    *out = reinterpret_cast<bp_ctx>(c);
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_ctx_destroy(bp_ctx ctx) {
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c) return BP_OK;
+    DeviceGuard g(c->device);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_ctx_set_stream(bp_ctx ctx, void* stream) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return fail(BP_ERR_INVALID, "bp_ctx_set_stream: null context");
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return BP_OK;
+}
+
+BP_API int32_t bp_ctx_memory(bp_ctx ctx, uint64_t* used, uint64_t* budget) {
+  Ctx* c = as_ctx(ctx);
+  if (!c) return fail(BP_ERR_INVALID, "bp_ctx_memory: null context");
+  if (used) *used = c->used;
+  if (budget) *budget = c->budget;
+  return BP_OK;
+}
+
+BP_API int32_t bp_ctx_synchronize(bp_ctx ctx) {
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c) return fail(BP_ERR_INVALID, "bp_ctx_synchronize: null context");
+    DeviceGuard g(c->device);
+    BP_CUDA(cudaStreamSynchronize(c->stream));
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_problem_create(bp_ctx ctx, const bp_patches* pp, const bp_params* prm, bp_problem* out) {
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c || !pp || !prm || !out) return fail(BP_ERR_INVALID, "bp_problem_create: null argument");
+    const int n = pp->n_patches;
+    if (n <= 0) return fail(BP_ERR_INVALID, "bp_problem_create: no patches");
+    if (!pp->centroid || !pp->normal || !pp->area || !pp->dielectric_ratio)
+      return fail(BP_ERR_INVALID, "bp_problem_create: missing patch arrays");
+    if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
+      return fail(BP_ERR_INVALID, "bp_problem_create: unknown precision");
+    if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, "bp_problem_create: bad kappa");
+    if (prm->nterms != 9 && prm->nterms != 18)
+      return fail(BP_ERR_UNSUPPORTED, "bp_problem_create: FMM order must be 9 or 18 (tabulated quadratures)");
+    DeviceGuard g(c->device);
+    auto P = std::make_unique<Problem>();
+    P->ctx = c;
+    P->n = n;
+    P->params = *prm;
+    P->fp64 = prm->precision == BP_PREC_FP64;
+    P->h_centroid.assign(pp->centroid, pp->centroid + 3 * (size_t)n);
+    P->h_normal.assign(pp->normal, pp->normal + 3 * (size_t)n);
+    P->h_area.assign(pp->area, pp->area + n);
+    P->h_eps.assign(pp->dielectric_ratio, pp->dielectric_ratio + n);
+    P->h_gc.assign(n, 0.5);
+    if (pp->gc) P->h_gc.assign(pp->gc, pp->gc + n);
+    for (int i = 0; i < n; ++i) {
+      if (!(P->h_eps[i] > 0)) return fail(BP_ERR_INVALID, "bp_problem_create: dielectric ratio must be > 0");
+      for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(P->h_centroid[3 * i + k]) || !std::isfinite(P->h_normal[3 * i + k]))
+          return fail(BP_ERR_INVALID, "bp_problem_create: non-finite patch geometry");
+    }
+    check_points("qualocation", n, pp->qual_offsets, pp->qual_points, P->h_qual_off, P->h_qual);
+    check_points("quadrature", n, pp->quad_offsets, pp->quad_points, P->h_quad_off, P->h_quad);
+    check_points("galerkin", n, pp->galerkin_offsets, pp->galerkin_points, P->h_gal_off, P->h_gal);
+    // adaptive tree (host)
+    auto t0 = std::chrono::steady_clock::now();
+    build_reference_tree(P->h_centroid.data(), n, prm->cube_centre, prm->cube_edge, prm->nbsize, P->tree);
+    P->tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    // device copies
+    P->d_centroid = upload(c, P->h_centroid);
+    P->d_normal = upload(c, P->h_normal);
+    P->d_area = upload(c, P->h_area);
+    P->d_eps = upload(c, P->h_eps);
+    P->d_qual_off = upload(c, P->h_qual_off);
+    P->d_quad_off = upload(c, P->h_quad_off);
+    P->d_gal_off = upload(c, P->h_gal_off);
+    P->d_qual = upload(c, soa7<double>(P->h_qual));
+    P->d_quad = upload(c, soa7<double>(P->h_quad));
+    P->d_gal = upload(c, soa7<double>(P->h_gal));
+    if (!P->fp64) {
+      P->d_qual_f = upload(c, soa7<float>(P->h_qual));
+      P->d_quad_f = upload(c, soa7<float>(P->h_quad));
+    }
+    P->d_x.alloc(c, sizeof(double) * 2 * (size_t)n);
+    P->d_y.alloc(c, sizeof(double) * 2 * (size_t)n);
+    nf_build_structure(*P);
+    nf_assemble(*P);
+    if (fmm_active(*P)) fmm_setup(*P);
+    BP_CUDA(cudaStreamSynchronize(c->stream));
+    *out = reinterpret_cast<bp_problem>(P.release());
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_problem_destroy(bp_problem p) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P) return BP_OK;
+    DeviceGuard g(P->ctx->device);
+    cudaStreamSynchronize(P->ctx->stream);
+    delete P;
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info) {
+  Problem* P = as_problem(p);
+  if (!P || !info) return fail(BP_ERR_INVALID, "bp_problem_info_get: null argument");
+  info->n_patches = P->n;
+  info->n_levels = P->tree.n_levels;
+  info->n_nodes = (int64_t)P->tree.nodes.size();
+  info->n_leaves = P->nf.n_leaves;
+  info->n_nearfield_pairs = P->nf.n_pairs;
+  info->n_nearfield_cols = P->nf.h_col_off.empty() ? 0 : P->nf.h_col_off.back();
+  info->fmm_active = fmm_active(*P) ? 1 : 0;
+  info->device_bytes = P->ctx->used;
+  info->tree_ms = P->tree_ms;
+  info->assemble_ms = P->assemble_ms;
+  return BP_OK;
+}
+
+static int32_t export_tree(const TreeInfo& T, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info,
+                           double* node_geom, int32_t* contents) {
+  if (n_nodes) *n_nodes = (int32_t)T.nodes.size();
+  if (n_levels) *n_levels = T.n_levels;
+  for (size_t k = 0; k < T.nodes.size(); ++k) {
+    const TreeNode& nd = T.nodes[k];
+    if (node_info) {
+      int32_t* o = node_info + 18 * k;
+      o[0] = nd.level;
+      o[1] = (int32_t)nd.ix;
+      o[2] = (int32_t)nd.iy;
+      o[3] = (int32_t)nd.iz;
+      o[4] = nd.flags;
+      o[5] = nd.parent;
+      o[6] = (int32_t)nd.content_start;
+      o[7] = nd.content_count;
+      o[8] = nd.mp_idx;
+      o[9] = nd.lc_idx;
+      for (int c = 0; c < 8; ++c) o[10 + c] = nd.children[c];
+    }
+    if (node_geom) {
+      for (int d = 0; d < 3; ++d) node_geom[4 * k + d] = nd.centre[d];
+      node_geom[4 * k + 3] = nd.edge;
+    }
+  }
+  if (contents) std::copy(T.contents.begin(), T.contents.end(), contents);
+  return BP_OK;
+}
+
+BP_API int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info,
+                               double* node_geom, int32_t* contents) {
+  Problem* P = as_problem(p);
+  if (!P) return fail(BP_ERR_INVALID, "bp_problem_tree: null problem");
+  return export_tree(P->tree, n_nodes, n_levels, node_info, node_geom, contents);
+}
+
+BP_API int32_t bp_tree_create(int32_t n, const double* points, const double cube_centre[3], double cube_edge,
+                              int32_t nbsize, bp_tree* out) {
+  return guarded([&]() -> int32_t {
+    if (n <= 0 || !points || !cube_centre || !out) return fail(BP_ERR_INVALID, "bp_tree_create: bad argument");
+    auto T = std::make_unique<TreeInfo>();
+    build_reference_tree(points, n, cube_centre, cube_edge, nbsize, *T);
+    *out = reinterpret_cast<bp_tree>(T.release());
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_tree_export(bp_tree t, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info, double* node_geom,
+                              int32_t* contents) {
+  if (!t) return fail(BP_ERR_INVALID, "bp_tree_export: null tree");
+  return export_tree(*reinterpret_cast<TreeInfo*>(t), n_nodes, n_levels, node_info, node_geom, contents);
+}
+
+BP_API int32_t bp_tree_destroy(bp_tree t) {
+  delete reinterpret_cast<TreeInfo*>(t);
+  return BP_OK;
+}
+
+BP_API int32_t bp_matvec_device(bp_problem p, const double* x_dev, double* y_dev) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !x_dev || !y_dev) return fail(BP_ERR_INVALID, "bp_matvec_device: null argument");
+    if (x_dev == y_dev) return fail(BP_ERR_INVALID, "bp_matvec_device: x and y must not alias");
+    DeviceGuard g(P->ctx->device);
+    matvec_device(*P, x_dev, y_dev);
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_matvec_profile(bp_problem p, const double* x_dev, double* y_dev, int32_t reps, double* stage_ms,
+                                 int32_t* stage_launches, int32_t* n_stages) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !x_dev || !y_dev || !stage_ms || reps <= 0) return fail(BP_ERR_INVALID, "bp_matvec_profile: bad argument");
+    DeviceGuard g(P->ctx->device);
+    StageTimes st;
+    for (int r = 0; r < reps; ++r) matvec_device(*P, x_dev, y_dev, &st);
+    BP_CUDA(cudaStreamSynchronize(P->ctx->stream));
+    for (int s = 0; s < kStages; ++s) {
+      stage_ms[s] = st.ms(s) / reps;
+      if (stage_launches) stage_launches[s] = st.launches[s] / reps;
+    }
+    if (n_stages) *n_stages = kStages;
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_matvec(bp_problem p, const double* x, double* y) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !x || !y) return fail(BP_ERR_INVALID, "bp_matvec: null argument");
+    DeviceGuard g(P->ctx->device);
+    const size_t bytes = sizeof(double) * 2 * (size_t)P->n;
+    cudaStream_t st = P->ctx->stream;
+    BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
+    matvec_device(*P, P->d_x.as<double>(), P->d_y.as<double>());
+    BP_CUDA(cudaMemcpyAsync(y, P->d_y.get(), bytes, cudaMemcpyDeviceToHost, st));
+    BP_CUDA(cudaStreamSynchronize(st));
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_dev, double tol, int32_t max_iters,
+                               int32_t restart, int32_t* iterations, double* rel_residual) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !rhs_dev || !x_dev) return fail(BP_ERR_INVALID, "bp_solve_device: null argument");
+    if (!(tol > 0)) return fail(BP_ERR_INVALID, "bp_solve_device: tol must be positive");
+    DeviceGuard g(P->ctx->device);
+    double rr = 0;
+    int its = gmres_device(*P, rhs_dev, x_dev, tol, max_iters, restart, &rr);
+    if (iterations) *iterations = its;
+    if (rel_residual) *rel_residual = rr;
+    if (rr > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
+                        int32_t* iterations, double* rel_residual) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !rhs || !x) return fail(BP_ERR_INVALID, "bp_solve: null argument");
+    if (!(tol > 0)) return fail(BP_ERR_INVALID, "bp_solve: tol must be positive");
+    DeviceGuard g(P->ctx->device);
+    const size_t bytes = sizeof(double) * 2 * (size_t)P->n;
+    cudaStream_t st = P->ctx->stream;
+    DevBuf b(P->ctx, bytes);
+    BP_CUDA(cudaMemcpyAsync(b.get(), rhs, bytes, cudaMemcpyHostToDevice, st));
+    BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
+    double rr = 0;
+    int its = gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, &rr);
+    BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
+    BP_CUDA(cudaStreamSynchronize(st));
+    if (iterations) *iterations = its;
+    if (rel_residual) *rel_residual = rr;
+    if (rr > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charges, double eps_solvent, double* rhs) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !rhs || (n_charges > 0 && !charges_xyzq) || n_charges < 0)
+      return fail(BP_ERR_INVALID, "bp_rhs: bad argument");
+    if (!(eps_solvent > 0)) return fail(BP_ERR_INVALID, "bp_rhs: eps_solvent must be positive");
+    DeviceGuard g(P->ctx->device);
+    Ctx* c = P->ctx;
+    DevBuf dch(c, sizeof(double) * 4 * (size_t)std::max(1, n_charges));
+    if (n_charges)
+      BP_CUDA(cudaMemcpyAsync(dch.get(), charges_xyzq, sizeof(double) * 4 * (size_t)n_charges, cudaMemcpyHostToDevice,
+                              c->stream));
+    rhs_device(*P, dch.as<double>(), n_charges, eps_solvent, P->d_y.as<double>());
+    BP_CUDA(cudaMemcpyAsync(rhs, P->d_y.get(), sizeof(double) * 2 * (size_t)P->n, cudaMemcpyDeviceToHost, c->stream));
+    BP_CUDA(cudaStreamSynchronize(c->stream));
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_energy_coefficients(bp_problem p, int32_t first, int32_t count, const double* charges_xyzq,
+                                      int32_t n_charges, double total_area, double* coef_f, double* coef_h) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !coef_f || !coef_h || first < 0 || count <= 0 || first + count > P->n || n_charges < 0 ||
+        (n_charges > 0 && !charges_xyzq) || !(total_area > 0))
+      return fail(BP_ERR_INVALID, "bp_energy_coefficients: bad argument");
+    DeviceGuard g(P->ctx->device);
+    Ctx* c = P->ctx;
+    DevBuf dch(c, sizeof(double) * 4 * (size_t)std::max(1, n_charges));
+    if (n_charges)
+      BP_CUDA(cudaMemcpyAsync(dch.get(), charges_xyzq, sizeof(double) * 4 * (size_t)n_charges, cudaMemcpyHostToDevice,
+                              c->stream));
+    DevBuf out(c, sizeof(double) * 2 * (size_t)count);
+    energy_coefficients_device(*P, first, count, dch.as<double>(), n_charges, out.as<double>(),
+                               out.as<double>() + count);
+    std::vector<double> h(2 * (size_t)count);
+    BP_CUDA(cudaMemcpy(h.data(), out.get(), sizeof(double) * 2 * (size_t)count, cudaMemcpyDeviceToHost));
+    // Gauss-law renormalisation of the f coefficients (host, compensated sums)
+    double net = 0.0;
+    for (int k = 0; k < n_charges; ++k) net += charges_xyzq[4 * k + 3];
+    double total_f = 0.0;
+    for (int k = 0; k < count; ++k) total_f -= h[k];
+    const double gauss_error = net - total_f;
+    for (int k = 0; k < count; ++k) {
+      coef_f[k] = h[k] - (P->h_area[first + k] / total_area) * gauss_error;
+      coef_h[k] = h[count + k];
+    }
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_energy(bp_problem p, int32_t first, int32_t count, const double* coef_f, const double* coef_h,
+                         double eps_ratio, const double* x, double* energy) {
+  Problem* P = as_problem(p);
+  if (!P || !coef_f || !coef_h || !x || !energy || first < 0 || count <= 0 || first + count > P->n)
+    return fail(BP_ERR_INVALID, "bp_energy: bad argument");
+  // Kahan-compensated sum (src/bem/mesh.cpp:1388-1400); 0.5 * N_A e^2 /
+  // (eps0 * Angstrom * 1000) converts to kJ/mol (src/bem/constants.h:51).
+  const double Avogadro = 6.02214179e23, e = 1.60217646e-19, eps0 = 8.85418782e-12, Ang = 1.0e-10;
+  const double conv = Avogadro * e * e / (eps0 * Ang * 1000.0);
+  double sum = 0.0, comp = 0.0;
+  for (int k = 0; k < count; ++k) {
+    const double f = x[first + k], h = x[P->n + first + k];
+    const double frag = h * eps_ratio * coef_h[k] - f * coef_f[k];
+    const double yv = frag - comp;
+    const double t = sum + yv;
+    comp = (t - sum) - yv;
+    sum = t;
+  }
+  *energy = sum * 0.5 * conv;
+  return BP_OK;
+}
+
+}  // extern "C"

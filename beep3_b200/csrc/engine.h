@@ -1,0 +1,254 @@
+// Internal engine types: context, budgeted device buffers, problem state.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "octree.h"
+
+namespace bp {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct BudgetError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define BP_CUDA(call)                                                                               \
+  do {                                                                                              \
+    cudaError_t err__ = (call);                                                                     \
+    if (err__ != cudaSuccess)                                                                       \
+      throw ::bp::CudaError(std::string(#call) + ": " + cudaGetErrorString(err__) + " @" __FILE__ ":" + \
+                            std::to_string(__LINE__));                                              \
+  } while (0)
+
+#define BP_LAUNCH_CHECK() BP_CUDA(cudaGetLastError())
+
+template <typename F>
+int32_t guarded_engine(F&& f) {
+  try {
+    return f();
+  } catch (const BudgetError& e) {
+    return fail(BP_ERR_BUDGET, e.what());
+  } catch (const CudaError& e) {
+    return fail(BP_ERR_CUDA, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(BP_ERR_NOMEM, "host allocation failed");
+  } catch (const std::invalid_argument& e) {
+    return fail(BP_ERR_INVALID, e.what());
+  } catch (const std::exception& e) {
+    return fail(BP_ERR_INTERNAL, e.what());
+  } catch (...) {
+    return fail(BP_ERR_INTERNAL, "unknown exception");
+  }
+}
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;
+  uint64_t used = 0;
+  std::mutex mu;
+  int sm_count = 148;
+
+  void charge(uint64_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (budget && used + bytes > budget)
+      throw BudgetError("device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget (" +
+                        std::to_string(used) + " of " + std::to_string(budget) + " in use)");
+    used += bytes;
+  }
+  void release(uint64_t bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    used -= bytes;
+  }
+};
+
+// Device allocation charged to a context's budget; freed on destruction.
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(Ctx* ctx, size_t bytes) { alloc(ctx, bytes); }
+  ~DevBuf() { reset(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { swap(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      reset();
+      swap(o);
+    }
+    return *this;
+  }
+  void alloc(Ctx* ctx, size_t bytes) {
+    reset();
+    if (bytes == 0) return;
+    ctx->charge(bytes);
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      ctx->release(bytes);
+      throw CudaError(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    ctx_ = ctx;
+    ptr_ = p;
+    bytes_ = bytes;
+  }
+  void reset() {
+    if (ptr_) {
+      cudaFree(ptr_);
+      ctx_->release(bytes_);
+    }
+    ptr_ = nullptr;
+    bytes_ = 0;
+    ctx_ = nullptr;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr_);
+  }
+  void* get() const { return ptr_; }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void swap(DevBuf& o) {
+    std::swap(ctx_, o.ctx_);
+    std::swap(ptr_, o.ptr_);
+    std::swap(bytes_, o.bytes_);
+  }
+  Ctx* ctx_ = nullptr;
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+template <typename T>
+DevBuf upload(Ctx* ctx, const std::vector<T>& v) {
+  DevBuf b(ctx, v.size() * sizeof(T));
+  if (!v.empty()) BP_CUDA(cudaMemcpyAsync(b.get(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  return b;
+}
+
+// Work item of the near-field kernels: a chunk of the rows of one leaf.
+struct NfItem {
+  int32_t leaf;
+  int32_t row_begin;  // offset inside the leaf's row list
+  int32_t row_count;
+  int32_t qual_total; // qualocation points of those rows (shared-memory sizing)
+};
+
+// Near-field block-sparse structure: per leaf a dense |rows| x |cols| block
+// of (A, B, C, D) coefficients, rows = the leaf's patches, cols = the
+// patches of its 27-box neighbourhood.
+struct NearField {
+  int n_leaves = 0;
+  int64_t n_pairs = 0;
+  int n_items = 0;
+  int max_qual_chunk = 0;
+  int max_cols = 0;
+  DevBuf rows, row_off, cols, col_off, coef_off, items;
+  DevBuf coef;  // 4 * n_pairs of float or double
+  std::vector<int64_t> h_row_off, h_col_off, h_coef_off;
+  std::vector<int32_t> h_rows, h_cols;
+  std::vector<NfItem> h_items;
+};
+
+struct Problem;
+struct FmmState;  // far-field state (fmm.cu)
+void fmm_destroy(FmmState*);
+
+struct Problem {
+  Ctx* ctx = nullptr;
+  int n = 0;
+  bp_params params{};
+  bool fp64 = true;
+  TreeInfo tree;
+  // patches (original order)
+  std::vector<double> h_centroid, h_normal, h_area, h_eps, h_gc;
+  std::vector<int32_t> h_qual_off, h_quad_off, h_gal_off;
+  std::vector<double> h_qual, h_quad, h_gal;
+  DevBuf d_centroid, d_normal, d_area, d_eps;               // double
+  DevBuf d_qual_off, d_quad_off, d_gal_off;                 // int32
+  DevBuf d_qual, d_quad, d_gal;                             // SoA of double, 7 arrays
+  DevBuf d_qual_f, d_quad_f;                                // SoA of float (mixed)
+  DevBuf d_diag;                                            // 4n double (singular + corrections)
+  NearField nf;
+  std::unique_ptr<FmmState, void (*)(FmmState*)> fmm{nullptr, fmm_destroy};
+  // matvec scratch
+  DevBuf d_x, d_y;  // 2n double each
+  // Krylov workspace
+  DevBuf d_V, d_w, d_scal;
+  int krylov_m = 0;
+  double tree_ms = 0, assemble_ms = 0;
+};
+
+// Optional per-stage timing of a matvec with CUDA events on the stream.
+constexpr int kStages = 8;  // near, P2M, M2M, M->X, X->X, X->L, L2L, L2P
+struct StageTimes {
+  struct Rec {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  int launches[kStages] = {0, 0, 0, 0, 0, 0, 0, 0};
+  cudaStream_t stream = nullptr;
+  int open_stage = -1;
+  cudaEvent_t open_ev = nullptr;
+  void begin(int s, cudaStream_t st) {
+    stream = st;
+    open_stage = s;
+    BP_CUDA(cudaEventCreate(&open_ev));
+    BP_CUDA(cudaEventRecord(open_ev, st));
+  }
+  void end(int launches_in_stage) {
+    cudaEvent_t e;
+    BP_CUDA(cudaEventCreate(&e));
+    BP_CUDA(cudaEventRecord(e, stream));
+    recs.push_back({open_stage, open_ev, e});
+    launches[open_stage] += launches_in_stage;
+    open_ev = nullptr;
+  }
+  double ms(int s) const {
+    double t = 0;
+    for (const Rec& r : recs)
+      if (r.stage == s) {
+        float f = 0;
+        cudaEventElapsedTime(&f, r.a, r.b);
+        t += f;
+      }
+    return t;
+  }
+  ~StageTimes() {
+    for (Rec& r : recs) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+  }
+};
+
+// nearfield.cu
+void nf_build_structure(Problem& P);
+void nf_assemble(Problem& P);
+void nf_apply(Problem& P, const double* x_dev, double* y_dev);
+// fmm.cu
+bool fmm_active(const Problem& P);
+void fmm_setup(Problem& P);
+void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st);
+// krylov.cu
+void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st = nullptr);
+int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,
+                 double* rel_resid);
+// sources.cu
+void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev);
+void energy_coefficients_device(Problem& P, int first, int count, const double* charges_dev, int n_charges,
+                                double* cf_dev, double* ch_dev);
+
+}  // namespace bp

@@ -1,0 +1,228 @@
+// Matvec driver and device-resident GMRES.
+//
+// GMRES restated from BEEP::gmres (src/beep/beep.cpp:1262-1483): residual
+// r = A x - b, classical Gram-Schmidt Arnoldi (two dgemv per step), Givens
+// rotations on a packed upper-triangular U (column j starts at j(j+1)/2),
+// stop when |y_j| <= tol * ||b||, back substitution and x -= V y.  The
+// reference runs a single cycle of max_iters; a positive `restart` repeats
+// cycles of that length until convergence or max_iters.
+//
+// Everything stays on the device in FP64: V is (m+1) columns of 2N doubles,
+// the dot products are deterministic two-pass reductions (fixed block
+// partials, then one block per column), and the 2x2 rotations run in a
+// single-thread kernel.  The host only reads the residual estimate once per
+// Arnoldi step to decide whether to stop.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "engine.h"
+
+namespace bp {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kDotBlocks = 296;  // 2 per SM on a 148-SM part
+
+// DBL_MIN guard used by the reference to avoid 0/0 (src/beep/beep.cpp:1360)
+__device__ __forceinline__ double near0(double v) { return v == 0.0 ? 2.2250738585072014e-308 : v; }
+
+// partial[k * gridDim.x + b] = sum over block b's slice of V[:,k] . w
+__global__ void dot_partials(const double* __restrict__ V, int64_t ld, const double* __restrict__ w, int64_t len,
+                             double* __restrict__ partial) {
+  const int k = blockIdx.y;
+  const double* v = V + ld * k;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    s += v[i] * w[i];
+  __shared__ double red[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) partial[(int64_t)k * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// out[k] = sum_b partial[k * nb + b] (fixed order), optionally sqrt
+__global__ void reduce_partials(const double* __restrict__ partial, int nb, double* __restrict__ out, int take_sqrt) {
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(int64_t)k * nb + b];
+  __shared__ double red[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) out[k] = take_sqrt ? sqrt(s) : s;
+  }
+}
+
+// w -= V[:, 0..ncols) * u
+__global__ void orth_update(const double* __restrict__ V, int64_t ld, int ncols, const double* __restrict__ u,
+                            double* __restrict__ w, int64_t len) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < ncols; ++k) s += V[ld * k + i] * u[k];
+    w[i] -= s;
+  }
+}
+
+// r = r - b ; then v0 = r / near0(||r||) is done by scale_by_norm
+__global__ void sub_inplace(double* __restrict__ r, const double* __restrict__ b, int64_t len) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    r[i] -= b[i];
+}
+
+__global__ void scale_by_norm(double* __restrict__ v, const double* __restrict__ norm, int64_t len) {
+  const double inv = 1.0 / near0(*norm);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] *= inv;
+}
+
+// x -= V[:, 0..j) y
+__global__ void update_x(const double* __restrict__ V, int64_t ld, int j, const double* __restrict__ y,
+                         double* __restrict__ x, int64_t len) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < j; ++k) s += V[ld * k + i] * y[k];
+    x[i] -= s;
+  }
+}
+
+// Givens step for Arnoldi column j (src/beep/beep.cpp:1399-1416).
+// U[u0j .. u0j+j] holds V^T w; h = ||w|| after orthogonalisation.
+__global__ void givens_step(double* __restrict__ U, int u0j, int j, const double* __restrict__ hptr,
+                            double* __restrict__ c, double* __restrict__ s, double* __restrict__ y) {
+  int uij = u0j;
+  const double h = *hptr;
+  for (int i = 0; i < j; ++i) {
+    const double tmp = c[i] * U[uij] - s[i] * U[uij + 1];
+    U[uij + 1] = s[i] * U[uij] + c[i] * U[uij + 1];
+    U[uij] = tmp;
+    ++uij;
+  }
+  const double rd = U[uij];
+  const double dd = sqrt(rd * rd + h * h);
+  c[j] = rd / near0(dd);
+  s[j] = -h / near0(dd);
+  U[uij] = dd;
+  y[j + 1] = s[j] * y[j];
+  y[j] = c[j] * y[j];
+}
+
+// Solve the packed upper-triangular U y = y (column-major, first j columns)
+// unless U and y are both zero (src/beep/beep.cpp:1422-1426).
+__global__ void packed_back_substitution(const double* __restrict__ U, int j, double* __restrict__ y) {
+  double su = 0.0, sy = 0.0;
+  const int uij = j * (j + 1) / 2;
+  for (int k = 0; k < uij; ++k) su += fabs(U[k]);
+  for (int k = 0; k < j; ++k) sy += fabs(y[k]);
+  if (su == 0.0 && sy == 0.0) return;
+  for (int i = j - 1; i >= 0; --i) {
+    double t = y[i];
+    for (int k = i + 1; k < j; ++k) t -= U[k * (k + 1) / 2 + i] * y[k];
+    y[i] = t / U[i * (i + 1) / 2 + i];
+  }
+}
+
+__global__ void set_scalar(double* p, const double* src) { *p = *src; }
+
+inline int grid_for(int64_t len) {
+  int64_t g = (len + kThreads - 1) / kThreads;
+  if (g > 4 * 148) g = 4 * 148;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st) {
+  if (st) st->begin(0, P.ctx->stream);
+  nf_apply(P, x_dev, y_dev);  // writes every y entry
+  if (st) st->end(P.nf.n_items > 0 ? 1 : 0);
+  if (fmm_active(P)) fmm_apply(P, x_dev, y_dev, st);  // adds the far field
+}
+
+int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,
+                 double* rel_resid) {
+  Ctx* ctx = P.ctx;
+  cudaStream_t st = ctx->stream;
+  const int64_t len = 2 * (int64_t)P.n;
+  if (max_iters <= 0) throw std::invalid_argument("max_iters must be positive");
+  const int m = (restart > 0 && restart < max_iters) ? restart : max_iters;
+  if (P.krylov_m != m || !P.d_V.get()) {
+    P.d_V.alloc(ctx, sizeof(double) * (size_t)len * (m + 1));
+    // scalars: U (m(m+1)/2), c (m), s (m), y (m+1), norms (4), partials
+    size_t nscal = (size_t)m * (m + 1) / 2 + 2 * m + (m + 1) + 8 + (size_t)kDotBlocks * (m + 1);
+    P.d_scal.alloc(ctx, sizeof(double) * nscal);
+    P.krylov_m = m;
+  }
+  double* V = P.d_V.as<double>();
+  double* U = P.d_scal.as<double>();
+  double* c = U + (size_t)m * (m + 1) / 2;
+  double* s = c + m;
+  double* y = s + m;
+  double* norms = y + (m + 1);  // [0] = ||b||, [1] = scratch norm
+  double* partial = norms + 8;
+  auto dots = [&](const double* Vb, int ncols, const double* w, double* out, bool take_sqrt) {
+    dim3 g(kDotBlocks, ncols);
+    dot_partials<<<g, kThreads, 0, st>>>(Vb, len, w, len, partial);
+    reduce_partials<<<ncols, kThreads, 0, st>>>(partial, kDotBlocks, out, take_sqrt ? 1 : 0);
+  };
+  const int g = grid_for(len);
+  // ||b||
+  dots(b_dev, 1, b_dev, norms, true);
+  double nrm2b = 0.0;
+  BP_CUDA(cudaMemcpyAsync(&nrm2b, norms, sizeof(double), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  const double stop = tol * nrm2b;
+  int total = 0;
+  double last = 0.0;
+  while (true) {
+    BP_CUDA(cudaMemsetAsync(U, 0, sizeof(double) * ((size_t)m * (m + 1) / 2 + 2 * m + (m + 1)), st));
+    // r = A x - b into V[:,0], normalise, y[0] = beta
+    matvec_device(P, x_dev, V);
+    sub_inplace<<<g, kThreads, 0, st>>>(V, b_dev, len);
+    dots(V, 1, V, norms + 1, true);
+    set_scalar<<<1, 1, 0, st>>>(y, norms + 1);
+    scale_by_norm<<<g, kThreads, 0, st>>>(V, norms + 1, len);
+    BP_LAUNCH_CHECK();
+    int j = 0, uij = 0;
+    const int cycle = std::min(m, max_iters - total);
+    while (true) {
+      const int u0j = uij;
+      double* vj = V + len * j;
+      double* w = V + len * (j + 1);
+      matvec_device(P, vj, w);
+      dots(V, j + 1, w, U + u0j, false);
+      orth_update<<<g, kThreads, 0, st>>>(V, len, j + 1, U + u0j, w, len);
+      dots(w, 1, w, norms + 1, true);
+      scale_by_norm<<<g, kThreads, 0, st>>>(w, norms + 1, len);
+      givens_step<<<1, 1, 0, st>>>(U, u0j, j, norms + 1, c, s, y);
+      BP_LAUNCH_CHECK();
+      uij += j + 1;
+      ++j;
+      double yj = 0.0;
+      BP_CUDA(cudaMemcpyAsync(&yj, y + j, sizeof(double), cudaMemcpyDeviceToHost, st));
+      BP_CUDA(cudaStreamSynchronize(st));
+      last = std::fabs(yj);
+      if (!(j < cycle && last > stop)) break;
+    }
+    packed_back_substitution<<<1, 1, 0, st>>>(U, j, y);
+    update_x<<<g, kThreads, 0, st>>>(V, len, j, y, x_dev, len);
+    BP_LAUNCH_CHECK();
+    total += j;
+    if (last <= stop || total >= max_iters || restart <= 0) break;
+  }
+  BP_CUDA(cudaStreamSynchronize(st));
+  if (rel_resid) *rel_resid = nrm2b > 0 ? last / nrm2b : 0.0;
+  return total;
+}
+
+}  // namespace bp

@@ -1,0 +1,468 @@
+// Near field of the BEM matvec on sm_100a.
+//
+// What it computes (reference: src/bem/bem_kernels.h:18-251,
+// src/bem/local_integrations.h:98-130, src/beep/beep.cpp:768-1064):
+//   for every leaf L of the adaptive octree and every pair (i, j) with i a
+//   patch of L (collocation, "src" in the reference) and j a patch of the
+//   27-box neighbourhood of L (integration, "targ"), i != j:
+//     A_ij = sum_q w_q sum_p w_p (G - u)
+//     B_ij = sum_q w_q sum_p w_p n_p . (grad G / eps_j - grad u)
+//     C_ij = -sum_q w_q sum_p w_p n_q . (grad G - grad u / eps_j)
+//     D_ij = -(1/eps_j) sum_q w_q sum_p w_p n_q^T (Hess G - Hess u) n_p  (kappa != 0)
+//   with G = 1/(4 pi r), u = exp(-kappa r)/(4 pi r), r = x_p - x_q, q over
+//   the qualocation points of i, p over the quadrature points of j, and
+//   pairs with |r|^2 < 1e-9 skipped.  The diagonal (i, i) slot holds the
+//   singular self-patch integral plus the geometric corrections
+//   (src/bem/bem_kernels.cpp:123-136, src/beep/beep.cpp:829-843); it is
+//   computed and applied in FP64 in every precision mode.
+//   Per matvec: y_f[i] += B_ij f_j - A_ij h_j ; y_h[i] += D_ij f_j - C_ij h_j.
+//
+// Layout: one dense block of (A,B,C,D) per leaf, rows = the leaf's patches,
+// cols = the concatenated patches of its neighbours in neighbour order
+// 0..26.  The column list is stored once per leaf, so a pair costs 16 bytes
+// (FP32) or 32 bytes (FP64) of coefficients instead of the reference's
+// 24-byte (src, targ, A, B, C, D) record.  The apply kernel stages the
+// leaf's x values in shared memory once and streams each row's
+// coefficients with 16/32-byte vector loads, one warp per row, reduced with
+// warp shuffles: the per-iteration floor is the coefficient stream (HBM).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <stdexcept>
+
+#include "engine.h"
+
+namespace bp {
+
+namespace {
+
+constexpr int kAsmRows = 8;      // rows per assembly work item
+constexpr int kAsmThreads = 256;
+constexpr int kApplyRows = 64;   // rows per apply work item
+constexpr int kApplyThreads = 256;
+constexpr double kOneOver4Pi = 0.07957747154594767;  // 1/(4 pi)
+
+template <typename T>
+struct Vec4 {};
+template <>
+struct Vec4<float> {
+  using type = float4;
+};
+template <>
+struct Vec4<double> {
+  using type = double4;
+};
+
+// Streaming (evict-first) loads of one coefficient quadruple.
+__device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
+__device__ __forceinline__ double4 ld_stream(const double4* p) {
+  const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ float fast_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double fast_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float fexp(float x) { return expf(x); }
+__device__ __forceinline__ double fexp(double x) { return exp(x); }
+
+// One (collocation point, quadrature point) term of the four kernels,
+// accumulated into a, b, c, d (src/bem/bem_kernels.h:187-240).
+template <typename T>
+__device__ __forceinline__ void pair_term(T qx, T qy, T qz, T qnx, T qny, T qnz, T px, T py, T pz, T pnx, T pny,
+                                          T pnz, T pw, T kappa, T ie, bool with_d, T& a, T& b, T& c, T& d) {
+  const T dx = px - qx, dy = py - qy, dz = pz - qz;
+  const T r2 = dx * dx + dy * dy + dz * dz;
+  if (fabs(r2) < T(1e-9)) return;
+  const T ir = fast_rsqrt(r2);
+  const T r = r2 * ir;
+  const T ir2 = ir * ir;
+  const T ir3 = ir2 * ir;
+  const T gr0 = T(kOneOver4Pi);
+  const T gr1 = gr0 * ir;
+  const T gr3 = gr0 * ir3;
+  const T ur0 = fexp(-kappa * r) * gr0;
+  const T ur1 = ur0 * ir;
+  const T ur2 = ur0 * ir2;
+  const T ur3 = ur0 * ir3;
+  const T ur3ur2 = ur3 + kappa * ur2;
+  // gd = -dx*gr3 ; ud = -dx*ur3ur2
+  const T ndx = pnx * dx + pny * dy + pnz * dz;   // n_p . dx
+  const T n0dx = qnx * dx + qny * dy + qnz * dz;  // n_q . dx
+  a += pw * (gr1 - ur1);
+  b += pw * (-(ie * gr3) + ur3ur2) * ndx;
+  c += -pw * (-gr3 + ie * ur3ur2) * n0dx;
+  if (with_d) {
+    const T ir4 = ir2 * ir2;
+    const T ir5 = ir4 * ir;
+    const T gr5 = gr0 * ir5;
+    const T ur4 = ur0 * ir4;
+    const T ur5 = ur0 * ir5;
+    const T pur4ur3 = kappa * (T(3) * ur4 + kappa * ur3) + T(3) * ur5;
+    const T nn0 = pnx * qnx + pny * qny + pnz * qnz;
+    // sum_jk n0_k n_j (gdd_jk - udd_jk)
+    const T s = ndx * n0dx * (T(3) * gr5 - pur4ur3) - nn0 * (gr3 - ur3ur2);
+    d -= pw * s;
+  }
+}
+
+// Singular self-patch integrals in FP64, one warp per patch
+// (src/bem/bem_kernels.h:18-132): all ordered pairs of distinct galerkin
+// points of the patch, normalised by the sum of the outer weights; then the
+// geometric corrections B += (1-gc) + gc/eps, C -= gc + (1-gc)/eps.
+__global__ void singular_kernel(int n, const int32_t* __restrict__ off, const double* __restrict__ g, int ng,
+                                const double* __restrict__ eps, const double* __restrict__ gcv, double kappa,
+                                double* __restrict__ diag) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int s = off[warp], e = off[warp + 1];
+  const double* X = g;
+  const double* Y = g + ng;
+  const double* Z = g + 2 * (size_t)ng;
+  const double* NX = g + 3 * (size_t)ng;
+  const double* NY = g + 4 * (size_t)ng;
+  const double* NZ = g + 5 * (size_t)ng;
+  const double* W = g + 6 * (size_t)ng;
+  const double ie = 1.0 / eps[warp];
+  double A = 0, B = 0, C = 0, D = 0, wsum = 0;
+  for (int q = s + lane; q < e; q += 32) {
+    double a = 0, b = 0, c = 0, d = 0;
+    for (int p = s; p < e; ++p) {
+      pair_term<double>(X[q], Y[q], Z[q], NX[q], NY[q], NZ[q], X[p], Y[p], Z[p], NX[p], NY[p], NZ[p], W[p], kappa,
+                        ie, kappa != 0.0, a, b, c, d);
+    }
+    A += a * W[q];
+    B += b * W[q];
+    C += c * W[q];
+    D += d * W[q];
+    wsum += W[q];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    A += __shfl_xor_sync(0xffffffffu, A, o);
+    B += __shfl_xor_sync(0xffffffffu, B, o);
+    C += __shfl_xor_sync(0xffffffffu, C, o);
+    D += __shfl_xor_sync(0xffffffffu, D, o);
+    wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+  }
+  if (lane == 0) {
+    const double epsr = eps[warp];
+    const double gc = gcv[warp];
+    A /= wsum;
+    B /= wsum;
+    C /= wsum;
+    D *= ie / wsum;
+    const double fgc = (1.0 - gc) + gc / epsr;
+    const double hgc = gc + (1.0 - gc) / epsr;
+    diag[4 * warp + 0] = A;
+    diag[4 * warp + 1] = B + fgc;
+    diag[4 * warp + 2] = C - hgc;
+    diag[4 * warp + 3] = D;
+  }
+}
+
+// Coefficient assembly.  A work item is <= kAsmRows rows of one leaf; their
+// qualocation points are staged in shared memory; each thread walks the
+// leaf's columns and produces the (A,B,C,D) of every staged row for its
+// column, so one row's stores are contiguous across the block.
+template <typename T>
+__global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
+    const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
+    const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
+    const int32_t* __restrict__ qoff, const T* __restrict__ qual, int nq, const int32_t* __restrict__ poff,
+    const T* __restrict__ quad, int np, const double* __restrict__ eps, T kappa, const double* __restrict__ diag,
+    T* __restrict__ coef) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sq = reinterpret_cast<T*>(smem_raw);
+  __shared__ int s_start[kAsmRows + 1];
+  __shared__ int s_row[kAsmRows];
+  const NfItem it = items[blockIdx.x];
+  const int64_t r0 = row_off[it.leaf] + it.row_begin;
+  const int64_t c0 = col_off[it.leaf];
+  const int ncols = (int)(col_off[it.leaf + 1] - c0);
+  const int64_t nrows_leaf = row_off[it.leaf + 1] - row_off[it.leaf];
+  const int64_t block = coef_off[it.leaf];
+  const int tq = it.qual_total;
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int r = 0; r < it.row_count; ++r) {
+      const int i = rows[r0 + r];
+      s_row[r] = i;
+      s_start[r] = acc;
+      acc += qoff[i + 1] - qoff[i];
+    }
+    s_start[it.row_count] = acc;
+  }
+  __syncthreads();
+  for (int r = 0; r < it.row_count; ++r) {
+    const int i = s_row[r];
+    const int base = qoff[i];
+    const int cnt = s_start[r + 1] - s_start[r];
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      for (int f = 0; f < 7; ++f) sq[f * tq + s_start[r] + k] = qual[(size_t)f * nq + base + k];
+    }
+  }
+  __syncthreads();
+  const bool with_d = kappa != T(0);
+  using V4 = typename Vec4<T>::type;
+  V4* out = reinterpret_cast<V4*>(coef);
+  for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) {
+    const int j = cols[c0 + cc];
+    const T ie = T(1.0 / eps[j]);
+    const int ps = poff[j], pe = poff[j + 1];
+    for (int r = 0; r < it.row_count; ++r) {
+      const int i = s_row[r];
+      const int64_t o = block + (int64_t)(it.row_begin + r) * ncols + cc;
+      V4 v;
+      if (i == j) {  // self pair: applied in FP64 from the singular diagonal
+        v.x = T(0);
+        v.y = T(0);
+        v.z = T(0);
+        v.w = T(0);
+        out[o] = v;
+        continue;
+      }
+      T A = 0, B = 0, C = 0, D = 0;
+      const int qs = s_start[r], qe = s_start[r + 1];
+      for (int q = qs; q < qe; ++q) {
+        const T qx = sq[q], qy = sq[tq + q], qz = sq[2 * tq + q];
+        const T qnx = sq[3 * tq + q], qny = sq[4 * tq + q], qnz = sq[5 * tq + q];
+        T a = 0, b = 0, c = 0, d = 0;
+        for (int p = ps; p < pe; ++p) {
+          pair_term<T>(qx, qy, qz, qnx, qny, qnz, quad[p], quad[(size_t)np + p], quad[2 * (size_t)np + p],
+                       quad[3 * (size_t)np + p], quad[4 * (size_t)np + p], quad[5 * (size_t)np + p],
+                       quad[6 * (size_t)np + p], kappa, ie, with_d, a, b, c, d);
+        }
+        const T wq = sq[6 * tq + q];
+        A += a * wq;
+        B += b * wq;
+        C += c * wq;
+        D += d * wq;
+      }
+      v.x = A;
+      v.y = B;
+      v.z = C;
+      v.w = D * ie;
+      out[o] = v;
+    }
+  }
+  (void)nrows_leaf;
+}
+
+// y_f[i] = sum_j B_ij f_j - A_ij h_j ; y_h[i] = sum_j D_ij f_j - C_ij h_j
+// over the leaf's columns (the cached-coefficient stream of
+// src/beep/beep.cpp:1049-1062).  Accumulation type AccT.
+template <typename T>
+__global__ void __launch_bounds__(kApplyThreads) apply_kernel(
+    const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
+    const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
+    const T* __restrict__ coef, const double* __restrict__ diag, int n, const double* __restrict__ x,
+    double* __restrict__ y) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sf = reinterpret_cast<T*>(smem_raw);
+  const NfItem it = items[blockIdx.x];
+  const int64_t c0 = col_off[it.leaf];
+  const int ncols = (int)(col_off[it.leaf + 1] - c0);
+  T* sh = sf + ncols;
+  for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) {
+    const int j = cols[c0 + cc];
+    sf[cc] = T(x[j]);
+    sh[cc] = T(x[n + j]);
+  }
+  __syncthreads();
+  using V4 = typename Vec4<T>::type;
+  const V4* blk = reinterpret_cast<const V4*>(coef) + coef_off[it.leaf];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t r0 = row_off[it.leaf] + it.row_begin;
+  for (int r = warp; r < it.row_count; r += nwarps) {
+    const V4* rowp = blk + (int64_t)(it.row_begin + r) * ncols;
+    T accf = 0, acch = 0;
+    int cc = lane;
+    for (; cc + 96 < ncols; cc += 128) {
+      const V4 v0 = ld_stream(rowp + cc);
+      const V4 v1 = ld_stream(rowp + cc + 32);
+      const V4 v2 = ld_stream(rowp + cc + 64);
+      const V4 v3 = ld_stream(rowp + cc + 96);
+      accf += v0.y * sf[cc] - v0.x * sh[cc];
+      acch += v0.w * sf[cc] - v0.z * sh[cc];
+      accf += v1.y * sf[cc + 32] - v1.x * sh[cc + 32];
+      acch += v1.w * sf[cc + 32] - v1.z * sh[cc + 32];
+      accf += v2.y * sf[cc + 64] - v2.x * sh[cc + 64];
+      acch += v2.w * sf[cc + 64] - v2.z * sh[cc + 64];
+      accf += v3.y * sf[cc + 96] - v3.x * sh[cc + 96];
+      acch += v3.w * sf[cc + 96] - v3.z * sh[cc + 96];
+    }
+    for (; cc < ncols; cc += 32) {
+      const V4 v = ld_stream(rowp + cc);
+      accf += v.y * sf[cc] - v.x * sh[cc];
+      acch += v.w * sf[cc] - v.z * sh[cc];
+    }
+    double df = (double)accf, dh = (double)acch;
+    for (int o = 16; o > 0; o >>= 1) {
+      df += __shfl_xor_sync(0xffffffffu, df, o);
+      dh += __shfl_xor_sync(0xffffffffu, dh, o);
+    }
+    if (lane == 0) {
+      const int i = rows[r0 + r];
+      const double fi = x[i], hi = x[n + i];
+      y[i] = df + (diag[4 * i + 1] * fi - diag[4 * i + 0] * hi);
+      y[n + i] = dh + (diag[4 * i + 3] * fi - diag[4 * i + 2] * hi);
+    }
+  }
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+void nf_build_structure(Problem& P) {
+  const TreeInfo& T = P.tree;
+  NearField& nf = P.nf;
+  nf.h_row_off.assign(1, 0);
+  nf.h_col_off.assign(1, 0);
+  nf.h_coef_off.assign(1, 0);
+  nf.h_rows.clear();
+  nf.h_cols.clear();
+  std::vector<int> seen(P.n, 0);
+  std::vector<int> leaves;
+  for (size_t k = 0; k < T.nodes.size(); ++k) {
+    const TreeNode& nd = T.nodes[k];
+    if (!(nd.flags & TREE_LEAF) || nd.content_count == 0) continue;
+    leaves.push_back((int)k);
+  }
+  nf.max_cols = 0;
+  for (int leaf : leaves) {
+    const TreeNode& nd = T.nodes[leaf];
+    for (int c = 0; c < nd.content_count; ++c) {
+      int i = T.contents[nd.content_start + c];
+      nf.h_rows.push_back(i);
+      seen[i]++;
+    }
+    for (int nb = 0; nb < 27; ++nb) {
+      int m = nd.neighbours[nb];
+      if (m < 0) continue;
+      const TreeNode& mn = T.nodes[m];
+      for (int c = 0; c < mn.content_count; ++c) nf.h_cols.push_back(T.contents[mn.content_start + c]);
+    }
+    int64_t nrows = (int64_t)nf.h_rows.size() - nf.h_row_off.back();
+    int64_t ncols = (int64_t)nf.h_cols.size() - nf.h_col_off.back();
+    nf.max_cols = std::max<int>(nf.max_cols, (int)ncols);
+    nf.h_coef_off.push_back(nf.h_coef_off.back() + nrows * ncols);
+    nf.h_row_off.push_back((int64_t)nf.h_rows.size());
+    nf.h_col_off.push_back((int64_t)nf.h_cols.size());
+  }
+  for (int i = 0; i < P.n; ++i)
+    if (seen[i] != 1) throw std::runtime_error("octree leaves do not partition the patches");
+  nf.n_leaves = (int)leaves.size();
+  nf.n_pairs = nf.h_coef_off.back();
+  Ctx* ctx = P.ctx;
+  nf.rows = upload(ctx, nf.h_rows);
+  nf.cols = upload(ctx, nf.h_cols);
+  nf.row_off = upload(ctx, nf.h_row_off);
+  nf.col_off = upload(ctx, nf.h_col_off);
+  nf.coef_off = upload(ctx, nf.h_coef_off);
+}
+
+static std::vector<NfItem> make_items(const Problem& P, int chunk) {
+  const NearField& nf = P.nf;
+  std::vector<NfItem> items;
+  for (int l = 0; l < nf.n_leaves; ++l) {
+    int nrows = (int)(nf.h_row_off[l + 1] - nf.h_row_off[l]);
+    for (int r = 0; r < nrows; r += chunk) {
+      NfItem it;
+      it.leaf = l;
+      it.row_begin = r;
+      it.row_count = std::min(chunk, nrows - r);
+      int tq = 0;
+      for (int k = 0; k < it.row_count; ++k) {
+        int i = nf.h_rows[nf.h_row_off[l] + r + k];
+        tq += P.h_qual_off[i + 1] - P.h_qual_off[i];
+      }
+      it.qual_total = tq;
+      items.push_back(it);
+    }
+  }
+  return items;
+}
+
+void nf_assemble(Problem& P) {
+  auto t0 = std::chrono::steady_clock::now();
+  Ctx* ctx = P.ctx;
+  NearField& nf = P.nf;
+  // geometric correction per patch
+  DevBuf d_gc = upload(ctx, P.h_gc);
+  {
+    P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
+    const int ng = (int)(P.h_gal.size() / 7);
+    const int threads = 256;
+    const int blocks = (P.n * 32 + threads - 1) / threads;
+    singular_kernel<<<blocks, threads, 0, ctx->stream>>>(P.n, P.d_gal_off.as<int32_t>(), P.d_gal.as<double>(), ng,
+                                                        P.d_eps.as<double>(), d_gc.as<double>(), P.params.kappa,
+                                                        P.d_diag.as<double>());
+    BP_LAUNCH_CHECK();
+  }
+  std::vector<NfItem> asm_items = make_items(P, kAsmRows);
+  int max_tq = 0;
+  for (auto& it : asm_items) max_tq = std::max(max_tq, it.qual_total);
+  DevBuf d_asm_items = upload(ctx, asm_items);
+  const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
+  nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
+  const int nq = (int)(P.h_qual.size() / 7);
+  const int np = (int)(P.h_quad.size() / 7);
+  const size_t smem = elem * 7 * (size_t)max_tq;
+  if (smem > 200 * 1024) throw std::invalid_argument("too many qualocation points per patch");
+  if (!asm_items.empty()) {
+    if (P.fp64) {
+      BP_CUDA(cudaFuncSetAttribute(assemble_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      assemble_kernel<double><<<(int)asm_items.size(), kAsmThreads, smem, ctx->stream>>>(
+          d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+          nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual.as<double>(), nq,
+          P.d_quad_off.as<int32_t>(), P.d_quad.as<double>(), np, P.d_eps.as<double>(), P.params.kappa,
+          P.d_diag.as<double>(), nf.coef.as<double>());
+    } else {
+      BP_CUDA(cudaFuncSetAttribute(assemble_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      assemble_kernel<float><<<(int)asm_items.size(), kAsmThreads, smem, ctx->stream>>>(
+          d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+          nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(), nq,
+          P.d_quad_off.as<int32_t>(), P.d_quad_f.as<float>(), np, P.d_eps.as<double>(), (float)P.params.kappa,
+          P.d_diag.as<double>(), nf.coef.as<float>());
+    }
+    BP_LAUNCH_CHECK();
+  }
+  // apply work items
+  nf.h_items = make_items(P, kApplyRows);
+  nf.items = upload(ctx, nf.h_items);
+  nf.n_items = (int)nf.h_items.size();
+  BP_CUDA(cudaStreamSynchronize(ctx->stream));
+  P.assemble_ms = ms_since(t0);
+}
+
+void nf_apply(Problem& P, const double* x_dev, double* y_dev) {
+  Ctx* ctx = P.ctx;
+  NearField& nf = P.nf;
+  if (nf.n_items == 0) return;
+  const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
+  const size_t smem = 2 * elem * (size_t)nf.max_cols;
+  if (P.fp64) {
+    if (smem > 48 * 1024)
+      BP_CUDA(cudaFuncSetAttribute(apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    apply_kernel<double><<<nf.n_items, kApplyThreads, smem, ctx->stream>>>(
+        nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev, y_dev);
+  } else {
+    if (smem > 48 * 1024)
+      BP_CUDA(cudaFuncSetAttribute(apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    apply_kernel<float><<<nf.n_items, kApplyThreads, smem, ctx->stream>>>(
+        nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev, y_dev);
+  }
+  BP_LAUNCH_CHECK();
+}
+
+}  // namespace bp

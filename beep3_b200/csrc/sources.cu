@@ -1,0 +1,124 @@
+// Point-charge sources: right-hand side and energy coefficients.
+//
+// RHS (BEEP::set_rhs, src/beep/beep.cpp:1124-1260): at every qualocation
+// point q of patch i, phi(q) = sum_c q_c/|x_q - x_c| and grad phi;
+//   f_rhs[i] = sum_q w_q phi(q) / (4 pi eps_solvent)
+//   h_rhs[i] = sum_q w_q grad phi(q) . n_q / (4 pi eps_solvent).
+// The reference evaluates phi with its 6-figure vanilla FMM; here the sum is
+// direct (exact in FP64), tiled through shared memory.
+//
+// Energy coefficients (Mesh::init_energy_precalcs, src/bem/mesh.cpp:730-925):
+// at the galerkin points of each patch, from the charges of its own mesh,
+//   ec_f[i] = sum_g (grad phi . n_g) w_g / (4 pi),  ec_h[i] = sum_g phi w_g / (4 pi)
+// followed by the Gauss-law renormalisation of ec_f
+// (Mesh::renormalise_energy_precalcs, src/bem/mesh.cpp:905-925).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "engine.h"
+
+namespace bp {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr double kOneOver4Pi = 0.07957747154594767;
+
+// One thread per point; charges staged through shared memory in tiles.
+// out[2*p] = w * phi * scale, out[2*p+1] = w * (grad phi . n) * scale
+__global__ void point_potential_kernel(const double* __restrict__ pts, int npts, int first_pt, int count_pts,
+                                       const double* __restrict__ charges, int nc, double scale,
+                                       double* __restrict__ out) {
+  __shared__ double4 tile[kThreads];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = k < count_pts;
+  const int p = first_pt + k;
+  double x = 0, y = 0, z = 0;
+  if (active) {
+    x = pts[p];
+    y = pts[(size_t)npts + p];
+    z = pts[2 * (size_t)npts + p];
+  }
+  double phi = 0, gx = 0, gy = 0, gz = 0;
+  for (int base = 0; base < nc; base += kThreads) {
+    const int c = base + threadIdx.x;
+    if (c < nc) tile[threadIdx.x] = make_double4(charges[4 * c], charges[4 * c + 1], charges[4 * c + 2], charges[4 * c + 3]);
+    __syncthreads();
+    const int lim = min(kThreads, nc - base);
+    if (active) {
+      for (int t = 0; t < lim; ++t) {
+        const double4 ch = tile[t];
+        const double dx = x - ch.x, dy = y - ch.y, dz = z - ch.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 > 2.220446049250313e-16) {
+          const double id = rsqrt(d2);
+          const double pt = ch.w * id;
+          const double ft = -pt * id * id;
+          phi += pt;
+          gx += ft * dx;
+          gy += ft * dy;
+          gz += ft * dz;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    const double w = pts[6 * (size_t)npts + p];
+    const double nx = pts[3 * (size_t)npts + p], ny = pts[4 * (size_t)npts + p], nz = pts[5 * (size_t)npts + p];
+    out[2 * k] = w * phi * scale;
+    out[2 * k + 1] = w * (gx * nx + gy * ny + gz * nz) * scale;
+  }
+}
+
+// Per-patch sums of the per-point values (fixed order: deterministic).
+__global__ void sum_points_kernel(const int32_t* __restrict__ off, int first, int count, int pt_base,
+                                  const double* __restrict__ vals, double* __restrict__ a, double* __restrict__ b) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int i = first + k;
+  double s0 = 0, s1 = 0;
+  for (int p = off[i]; p < off[i + 1]; ++p) {
+    s0 += vals[2 * (p - pt_base)];
+    s1 += vals[2 * (p - pt_base) + 1];
+  }
+  a[k] = s0;
+  b[k] = s1;
+}
+
+}  // namespace
+
+void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev) {
+  Ctx* ctx = P.ctx;
+  const int nq = (int)(P.h_qual.size() / 7);
+  DevBuf vals(ctx, sizeof(double) * 2 * (size_t)nq);
+  const double scale = kOneOver4Pi / eps_solvent;
+  point_potential_kernel<<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+      P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
+  BP_LAUNCH_CHECK();
+  sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+      P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
+  BP_LAUNCH_CHECK();
+  BP_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void energy_coefficients_device(Problem& P, int first, int count, const double* charges_dev, int n_charges,
+                                double* cf_dev, double* ch_dev) {
+  Ctx* ctx = P.ctx;
+  const int ng = (int)(P.h_gal.size() / 7);
+  const int p0 = P.h_gal_off[first], p1 = P.h_gal_off[first + count];
+  DevBuf vals(ctx, sizeof(double) * 2 * (size_t)std::max(1, p1 - p0));
+  if (p1 > p0) {
+    point_potential_kernel<<<(p1 - p0 + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+        P.d_gal.as<double>(), ng, p0, p1 - p0, charges_dev, n_charges, kOneOver4Pi, vals.as<double>());
+    BP_LAUNCH_CHECK();
+  }
+  // vals[2p] -> ec_h (potential), vals[2p+1] -> ec_f (normal field)
+  sum_points_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+      P.d_gal_off.as<int32_t>(), first, count, p0, vals.as<double>(), ch_dev, cf_dev);
+  BP_LAUNCH_CHECK();
+  BP_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace bp

@@ -1,0 +1,376 @@
+"""Benchmark of the BEM matvec / GMRES solve (one JSON line on rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+  python bench.py --impl reference ...   # CPU restatement of the reference path
+
+A step is one matvec y = A x of the whole problem (near field + FMM) with x
+already in HBM; ``value`` is matvecs/s of the mixed-precision engine
+(whole job: sum over ranks / max time).  ``e2e`` is the same through the
+host-buffer C-ABI call (bp_matvec: H2D of x and D2H of y inside the timed
+region).  Extra keys report the FP64 engine, full solves/s, solve latency
+percentiles and the mixed-vs-FP64 energy error.  Multi-GPU runs are
+independent replicas (the path does not shard): scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BEM matvec/s & solves/s, mixed vs FP64 at <=1e-4 energy err; p50/p99 latency"
+L2_BYTES = 126 * 1024 * 1024
+
+
+# --------------------------------------------------------------------------- workloads
+def workload(name: str):
+    """Returns (description dict, list of (Mesh, offset, quaternion), kappa, nbsize)."""
+    import beep3_b200 as b
+    if name == "kirkwood":
+        V, T = b.icosphere(3, 10.0)
+        mesh = b.Mesh(V, T, b.charges_in_sphere(10, 7.0, seed=1234))
+        desc = dict(workload="kirkwood sphere r=10 A, icosphere k=3 (642 patches), 10 charges, eps 2/80, "
+                             "kappa 0.1, qual 4 / quad 0, reference tree nbsize 1500", patches=642)
+        return desc, [(mesh, None, (1, 0, 0, 0))], 0.1, 1500
+    if name == "star":
+        V, T, shape = b.star_surface(6, 20.0, seed=1235)
+        mesh = b.Mesh(V, T, b.charges_in_star(2000, shape, seed=1236))
+        desc = dict(workload="star-shaped molecule R=20 A (l<=6 harmonics, amp 0.15), icosphere k=6 "
+                             "(40962 patches), 2000 charges, eps 2/80, kappa 0.1, qual 4 / quad 0, "
+                             "FMM order 9, reference tree nbsize 1500", patches=40962)
+        return desc, [(mesh, None, (1, 0, 0, 0))], 0.1, 1500
+    raise ValueError(f"unknown workload {name}")
+
+
+def build_beep(meshes, kappa, nbsize, precision, device):
+    import beep3_b200 as b
+    bp = b.BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device)
+    for mesh, off, q in meshes:
+        bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
+    bp.build()
+    return bp
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- helpers
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def allreduce_max(dist, v: float, device) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_device_matvecs(bp, x, y, steps: int, flush) -> list[float]:
+    """Per-step device time (ms) of bp_matvec_device with CUDA events on the
+    engine's stream; L2 flushed between steps (outside the events) when the
+    working set fits in L2."""
+    import torch
+    from beep3_b200 import _native as N
+    L = N.lib()
+    p = bp.build()
+    stream = torch.cuda.current_stream()
+    N.check(L.bp_ctx_set_stream(bp.context(), C.c_void_p(stream.cuda_stream)))
+    out = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.add_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N.check(L.bp_matvec_device(p, x.data_ptr(), y.data_ptr()))
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def time_e2e(bp, xh, yh, steps: int) -> list[float]:
+    """Per-step time (ms) of the host-buffer ABI call bp_matvec, bracketed by
+    CUDA events on the engine's stream (the call copies x in and y out)."""
+    import torch
+    from beep3_b200 import _native as N
+    L = N.lib()
+    p = bp.build()
+    stream = torch.cuda.current_stream()
+    N.check(L.bp_ctx_set_stream(bp.context(), C.c_void_p(stream.cuda_stream)))
+    out = []
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N.check(L.bp_matvec(p, xh.data_ptr(), yh.data_ptr()))
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def stage_profile(bp, x, y, reps: int = 5):
+    from beep3_b200 import _native as N
+    ms = np.zeros(8)
+    launches = np.zeros(8, np.int32)
+    ns = C.c_int32()
+    N.check(N.lib().bp_matvec_profile(bp.build(), x.data_ptr(), y.data_ptr(), reps, N.ptr(ms), N.ptr(launches),
+                                      C.byref(ns)))
+    return ms, launches
+
+
+def cpu_baseline(bp, budget_s: float = 15.0) -> dict:
+    """The oracle (restated reference CPU matvec: cached near-field stream +
+    plane-wave FMM) timed on this host on a bounded sample."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    arr = bp.gathered()
+    centre, edge = bp.calculate_bounding_cube()
+    t0 = time.perf_counter()
+    pr = O.Problem(arr, bp.host_tree(), bp.kappa, fp32=True, cube_edge=edge, nterms=bp.nterms)
+    setup_s = time.perf_counter() - t0
+    x = np.random.default_rng(5).standard_normal(2 * pr.n)
+    reps, spent = 0, 0.0
+    while spent < budget_s and reps < 1000:
+        t = time.perf_counter()
+        pr.matvec(x)
+        spent += time.perf_counter() - t
+        reps += 1
+    pr.close()
+    return {"value": reps / spent, "unit": "matvec/s", "cores": threads, "kind": "port",
+            "sample": f"{reps} oracle matvecs of the full workload ({spent:.1f} s; near-field precalc "
+                      f"{setup_s:.1f} s excluded, as in BEEP::benchmark)"}
+
+
+# --------------------------------------------------------------------------- arms
+def run_reference(args):
+    world, rank, local, dist = dist_setup(args)
+    if rank != 0:
+        return
+    desc, meshes, kappa, nbsize = workload(args.workload)
+    import beep3_b200 as b  # geometry preparation (host) only
+    bp = b.BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision="mixed")
+    for mesh, off, q in meshes:
+        bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
+    import oracle as O
+    arr = bp.gathered()
+    centre, edge = bp.calculate_bounding_cube()
+    pr = O.Problem(arr, bp.host_tree(), kappa, fp32=True, cube_edge=edge, nterms=bp.nterms)
+    x = np.random.default_rng(5).standard_normal(2 * pr.n)
+    for _ in range(args.warmup):
+        pr.matvec(x)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        pr.matvec(x)
+        times.append(time.perf_counter() - t)
+    tot = sum(times)
+    val = args.steps / tot
+    threads = os.cpu_count() or 1
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "matvec/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32/fp64",
+            "data": "synthetic", "config": desc,
+            "cpu_baseline": {"value": val, "unit": "matvec/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} oracle matvecs of the full workload"},
+            "e2e": {"value": val, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local, dist = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    desc, meshes, kappa, nbsize = workload(args.workload)
+    bp = build_beep(meshes, kappa, nbsize, "mixed", local)
+    bp64 = build_beep(meshes, kappa, nbsize, "fp64", local)
+    n2 = 2 * bp.num_patches
+    inf = bp.info()
+    gen = torch.Generator(device="cpu").manual_seed(7)
+    x = torch.randn(n2, dtype=torch.float64, generator=gen).to(dev)
+    y = torch.empty_like(x)
+    working = inf.n_nearfield_pairs * 16 + n2 * 16
+    flush = torch.zeros(2 * L2_BYTES // 4, dtype=torch.float32, device=dev) if working < 2 * L2_BYTES else None
+    # warm-up
+    time_device_matvecs(bp, x, y, max(args.warmup, 3), flush)
+    time_device_matvecs(bp64, x, y, max(args.warmup, 3), flush)
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    steps_ms = time_device_matvecs(bp, x, y, args.steps, flush)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t_local = sum(steps_ms)
+    t_max = allreduce_max(dist, t_local, dev)
+    value = world * args.steps / (t_max / 1e3)
+    # FP64 engine, same steps
+    steps64 = time_device_matvecs(bp64, x, y, args.steps, flush)
+    t64 = allreduce_max(dist, sum(steps64), dev)
+    value64 = world * args.steps / (t64 / 1e3)
+    # end to end through the host-buffer ABI
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    time_e2e(bp, xh, yh, 3)
+    e2e_ms = time_e2e(bp, xh, yh, args.steps)
+    te = allreduce_max(dist, sum(e2e_ms), dev)
+    e2e_value = world * args.steps / (te / 1e3)
+    # stage profile -> roofline of the dominant kernel (near-field apply)
+    ms, launches = stage_profile(bp, x, y)
+    near_ms = ms[0]
+    alg_bytes = inf.n_nearfield_pairs * 16 + inf.n_nearfield_cols * 4 + n2 * 8 * 2 + bp.num_patches * 32
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg_bytes / (near_ms * 1e-3) / 1e9
+    # solves (RHS + GMRES) and energies, both precisions
+    solve_ms, solve64_ms = [], []
+    for _ in range(3):
+        bp.solve(1e-6, 100)
+        bp64.solve(1e-6, 100)
+    for _ in range(max(3, args.steps // 4)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        info = bp.solve(1e-6, 100)
+        solve_ms.append((time.perf_counter() - t) * 1e3)
+        t = time.perf_counter()
+        info64 = bp64.solve(1e-6, 100)
+        solve64_ms.append((time.perf_counter() - t) * 1e3)
+    e_mixed, _ = bp.calculate_energies()
+    e_fp64, _ = bp64.calculate_energies()
+    line = {
+        "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32 near field/FMM + fp64 singular/GMRES", "data": "synthetic",
+        "config": dict(desc, precision="mixed", parallelism=f"replicas x{world}",
+                       l2="flushed between steps" if flush is not None else "inputs larger than L2",
+                       nearfield_pairs=int(inf.n_nearfield_pairs), tree_levels=int(inf.n_levels),
+                       fmm=bool(inf.fmm_active)),
+        "e2e": {"value": e2e_value, "unit": "matvec/s", "h2d_bytes_per_step": n2 * 8, "d2h_bytes_per_step": n2 * 8},
+        "gpu_launches": int(launches.sum()) * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "nearfield apply_kernel<float>", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                     "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": near_ms},
+        "stage_ms": {k: round(float(v), 5) for k, v in zip(
+            ["near", "p2m", "m2m", "m2x", "x2x", "x2l", "l2l", "l2p"], ms)},
+        "fp64_matvec_per_s": value64,
+        "mixed_over_fp64": value / value64,
+        "solves_per_s": world * 1e3 / statistics.median(solve_ms),
+        "fp64_solves_per_s": world * 1e3 / statistics.median(solve64_ms),
+        "solve_latency_ms": {"p50": float(np.percentile(solve_ms, 50)), "p99": float(np.percentile(solve_ms, 99))},
+        "gmres_iterations": {"mixed": info.num_iterations, "fp64": info64.num_iterations},
+        "energy_kj_per_mol": {"mixed": e_mixed, "fp64": e_fp64,
+                              "rel_err_mixed_vs_fp64": abs(e_mixed - e_fp64) / abs(e_fp64)},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(bp)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bp.close()
+    bp64.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="kirkwood", choices=["kirkwood", "star"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,209 @@
+/*
+ * beep3_b200.h -- C ABI of the B200 (sm_100a) BEM matvec / GMRES engine.
+ *
+ * The engine replaces the accelerator boundary of libBEEP: the OpenCL handler
+ * and its work blobs (src/opencl/opencl_handler.h:87-229,
+ * src/opencl/opencl_workblob.h:20-52, src/bem/opencl_bem.h:37-295,
+ * src/fmm/opencl_fmm.h) and, behind it, the bodies of
+ * BEEP::init_fmm_octree, BEEP::precalc_neighbour_interactions,
+ * BEEP::do_bem_fmm_iteration and BEEP::gmres (src/beep/beep.cpp).
+ * BEEP's own public API (src/beep/beep.h:198-278) is unchanged: its methods
+ * call these entry points instead of the OpenCL queue.
+ *
+ * Conventions
+ *   - every function returns an int32_t status, BP_OK (0) on success; the
+ *     message of the last failure on the calling thread is bp_last_error();
+ *   - nothing throws across the ABI; all pointers are plain C pointers;
+ *   - the unknown vector is x = [f; h] of length 2N: the N surface potentials
+ *     followed by the N normal derivatives, in patch order
+ *     (src/beep/beep.cpp:1275-1283);
+ *   - "host" pointers are ordinary CPU memory (pinned or pageable);
+ *     "device" pointers are CUDA global memory on the context's device and
+ *     calls taking them are ordered on the context's stream without a host
+ *     synchronisation.
+ */
+#ifndef BEEP3_B200_H_
+#define BEEP3_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BP_ABI_VERSION 1
+
+enum bp_status {
+  BP_OK = 0,
+  BP_ERR_INVALID = 1,      /* bad argument */
+  BP_ERR_CUDA = 2,         /* CUDA runtime failure */
+  BP_ERR_NOMEM = 3,        /* host allocation failure */
+  BP_ERR_BUDGET = 4,       /* device allocation would exceed the context's HBM budget */
+  BP_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  BP_ERR_INTERNAL = 6,
+  BP_ERR_UNSUPPORTED = 7,  /* e.g. an FMM order without quadrature tables */
+  BP_ERR_NOT_CONVERGED = 8 /* GMRES stopped at its iteration limit (x is still written) */
+};
+
+enum bp_precision {
+  BP_PREC_FP64 = 0,  /* near field, FMM and Krylov solve in FP64 */
+  BP_PREC_MIXED = 1  /* FP32 near field and FMM, FP64 singular integrals, Krylov and energy */
+};
+
+typedef struct bp_ctx_s* bp_ctx;
+typedef struct bp_geom_s* bp_geom;
+typedef struct bp_problem_s* bp_problem;
+
+const char* bp_last_error(void);
+int32_t bp_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Context: one CUDA device, one stream, one HBM budget.
+ * Replaces OpenCL_Handler construction and its 512 MB/device admission
+ * budget (src/opencl/opencl_handler.cpp:19-147, :397-462).
+ */
+int32_t bp_ctx_create(int32_t device, uint64_t hbm_budget_bytes, bp_ctx* out);
+int32_t bp_ctx_destroy(bp_ctx ctx);
+int32_t bp_ctx_set_stream(bp_ctx ctx, void* cuda_stream); /* cudaStream_t; NULL = the context's own */
+int32_t bp_ctx_memory(bp_ctx ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
+int32_t bp_ctx_synchronize(bp_ctx ctx);
+
+/* ---------------------------------------------------------------------------
+ * Surface preparation (host only): vertex-centred node patches and their
+ * point lists from a closed triangulated surface, planar or PN-curved.
+ * Mirrors Mesh::create_bezier_triangles / create_node_patches and
+ * BasicNodePatch point generation (src/bem/mesh.cpp:1632-1652,
+ * src/bem/node_patch.cpp:55-130, :198-273).  Points are 7 doubles:
+ * x y z nx ny nz w.  qual_rule / quad_rule are the per-triangle rule orders
+ * (0 = one centroid point per patch, else 1, 4, 6 or 7); galerkin points use
+ * the 4-point rule.  totals[0] = curved surface area, totals[1] = planar.
+ */
+int32_t bp_geom_create(int32_t n_vertices, const double* vertices, const double* vertex_normals,
+                       int32_t n_triangles, const int32_t* triangles, int32_t planar, int32_t qual_rule,
+                       int32_t quad_rule, bp_geom* out);
+int32_t bp_geom_sizes(bp_geom g, int32_t* n_patches, int32_t* n_qual, int32_t* n_quad, int32_t* n_galerkin);
+int32_t bp_geom_copy(bp_geom g, double* centroid, double* normal, double* area, double* node,
+                     int32_t* qual_offsets, double* qual_points, int32_t* quad_offsets, double* quad_points,
+                     int32_t* galerkin_offsets, double* galerkin_points, double* totals);
+int32_t bp_geom_destroy(bp_geom g);
+
+/* ---------------------------------------------------------------------------
+ * Problem: all node patches of all mesh instances in universe coordinates
+ * (the contents BEEP inserts into its FMM octree, src/beep/beep.cpp:1618-1634).
+ */
+typedef struct {
+  int32_t n_patches;
+  const double* centroid;          /* [n][3] */
+  const double* normal;            /* [n][3] unit */
+  const double* area;              /* [n] curved patch area */
+  const double* dielectric_ratio;  /* [n] eps_solvent / eps_protein */
+  const double* gc;                /* [n] geometric correction, 0.5 */
+  const int32_t* qual_offsets;     /* [n+1] qualocation (collocation) points */
+  const double* qual_points;       /* [.][7], weights sum to 1 per patch */
+  const int32_t* quad_offsets;     /* [n+1] quadrature (integration) points */
+  const double* quad_points;       /* [.][7] */
+  const int32_t* galerkin_offsets; /* [n+1] points of the singular self-patch integral */
+  const double* galerkin_points;   /* [.][7] */
+} bp_patches;
+
+typedef struct {
+  double kappa;           /* inverse Debye length, 1/Angstrom */
+  double beta0;           /* screening standing in for the Laplace channels (1e-10) */
+  double cube_centre[3];  /* bounding cube (BEEP::calculate_bounding_cube) */
+  double cube_edge;
+  int32_t nbsize;         /* target mean neighbourhood size of the adaptive tree */
+  int32_t nterms;         /* FMM order; 9 (reference matvec order) or 18 */
+  int32_t precision;      /* enum bp_precision */
+  int32_t flags;          /* reserved, 0 */
+} bp_params;
+
+typedef struct {
+  int64_t n_patches;
+  int64_t n_levels;
+  int64_t n_nodes;
+  int64_t n_leaves;
+  int64_t n_nearfield_pairs; /* sum over leaves of |leaf| * |neighbourhood| */
+  int64_t n_nearfield_cols;  /* sum over leaves of |neighbourhood| (stored column ids) */
+  int64_t fmm_active;        /* 1 when the tree is deep enough for the far field */
+  uint64_t device_bytes;
+  double tree_ms;
+  double assemble_ms;        /* singular + near-field coefficient assembly */
+} bp_problem_info;
+
+/* Builds the adaptive octree, the singular self-patch integrals and the
+ * cached near-field coefficients (BEEP::init_fmm_octree +
+ * BEEP::precalc_neighbour_interactions, src/beep/beep.cpp:1585-1641,
+ * :768-956). */
+int32_t bp_problem_create(bp_ctx ctx, const bp_patches* patches, const bp_params* params, bp_problem* out);
+int32_t bp_problem_destroy(bp_problem p);
+int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info);
+
+/* Export of the adaptive octree (for inspection and cross-checks).
+ * node_info: [n_nodes][18] int32 = level, ix, iy, iz, flags (1 has children,
+ * 2 leaf, 4 shadow), parent, content_start, content_count, mp_idx, lc_idx,
+ * child node ids 1..8 (-1 absent); nodes are level by level in the
+ * reference's map order.  node_geom: [n_nodes][4] = centre xyz, edge.
+ * contents: [n_patches] patch ids, node by node in insertion order.
+ * Any output pointer may be NULL. */
+int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info, double* node_geom,
+                        int32_t* contents);
+
+/* The same adaptive octree built on the host alone (no device needed):
+ * BEEP::init_fmm_octree's insert + build_neighbourhoods +
+ * optimize_neighbourhoods + remove_empty_nodes (src/beep/beep.cpp:1585-1641).
+ * Export layout as bp_problem_tree. */
+typedef struct bp_tree_s* bp_tree;
+int32_t bp_tree_create(int32_t n_points, const double* points, const double cube_centre[3], double cube_edge,
+                       int32_t nbsize, bp_tree* out);
+int32_t bp_tree_export(bp_tree t, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info, double* node_geom,
+                       int32_t* contents);
+int32_t bp_tree_destroy(bp_tree t);
+
+/* y = A x, the BEM/FMM matvec (BEEP::do_bem_fmm_iteration,
+ * src/beep/beep.cpp:1485-1583).  Host arrays of 2N doubles; blocking. */
+int32_t bp_matvec(bp_problem p, const double* x, double* y);
+/* Same on device arrays, stream-ordered, no synchronisation. */
+int32_t bp_matvec_device(bp_problem p, const double* x_dev, double* y_dev);
+/* Per-stage device time of `reps` matvecs on device arrays, averaged, in ms,
+ * measured with CUDA events on the context stream.  stage_ms[0] = near field,
+ * [1] = P2M, [2] = M2M, [3] = multipole->exponential, [4] = exponential
+ * translations, [5] = exponential->local, [6] = L2L, [7] = L2P;
+ * *n_stages = 8.  stage_launches (may be NULL) receives kernel launches per
+ * stage per matvec. */
+int32_t bp_matvec_profile(bp_problem p, const double* x_dev, double* y_dev, int32_t reps, double* stage_ms,
+                          int32_t* stage_launches, int32_t* n_stages);
+
+/* GMRES(restart) solve of A x = rhs (BEEP::gmres, src/beep/beep.cpp:1262-1483):
+ * classical Gram-Schmidt Arnoldi and Givens rotations in FP64, stop when the
+ * residual estimate falls below tol * ||rhs||.  x holds the initial guess on
+ * entry and the solution on return.  restart <= 0 means one cycle of
+ * max_iters, as in the reference.  Host arrays of 2N doubles. */
+int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
+                 int32_t* iterations, double* rel_residual);
+/* Same on device arrays (still blocks: the Krylov loop reads its residual). */
+int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_dev, double tol, int32_t max_iters,
+                        int32_t restart, int32_t* iterations, double* rel_residual);
+
+/* Right-hand side from point charges (BEEP::set_rhs, src/beep/beep.cpp:1124-1260):
+ * Coulomb potential and field of all charges at every qualocation point,
+ * weighted and scaled by 1/(4 pi eps_solvent).  charges_xyzq: [n][4]. */
+int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charges, double eps_solvent, double* rhs);
+
+/* Energy coefficients of patches [first, first+count) from the charges of
+ * their own mesh (Mesh::init_energy_precalcs + renormalise_energy_precalcs,
+ * src/bem/mesh.cpp:730-925): Coulomb potential and normal field at the
+ * galerkin points, corrected so that the f-coefficients satisfy Gauss's law
+ * with total_area the curved area of the mesh. */
+int32_t bp_energy_coefficients(bp_problem p, int32_t first, int32_t count, const double* charges_xyzq,
+                               int32_t n_charges, double total_area, double* coef_f, double* coef_h);
+/* Solvation energy in kJ/mol of patches [first, first+count) from a solution
+ * x (host, 2N), compensated summation (Mesh::calculate_energy,
+ * src/bem/mesh.cpp:1373-1404). */
+int32_t bp_energy(bp_problem p, int32_t first, int32_t count, const double* coef_f, const double* coef_h,
+                  double eps_ratio, const double* x, double* energy_kj_per_mol);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEEP3_B200_H_ */

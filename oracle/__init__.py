@@ -1,0 +1,242 @@
+"""ORACLE -- test infrastructure only.
+
+CPU restatement of libBEEP's BEM matvec path (near field, singular
+integrals, plane-wave FMM, GMRES, right-hand side, energies) used as the
+checker in tests/, in ``__graft_entry__.smoke()`` and as the CPU baseline in
+``bench.py``.  Nothing in the ``beep3_b200`` package imports it.
+
+The C++ part is built by ``oracle/Makefile`` into ``oracle/_build/liboracle.so``
+(:func:`build` runs make when the library is missing or stale).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    srcs = list(HERE.glob("*.cpp")) + list(HERE.glob("*.h"))
+    if not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
+        res = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError("oracle build failed:\n" + res.stdout + res.stderr)
+    return LIB
+
+
+class OrPatches(C.Structure):
+    _fields_ = [("n", C.c_int32)] + [(k, C.c_void_p) for k in (
+        "centroid", "normal", "area", "eps", "gc", "qual_off", "qual", "quad_off", "quad", "gal_off", "gal")]
+
+
+class OrTree(C.Structure):
+    _fields_ = [("n_nodes", C.c_int32), ("n_levels", C.c_int32), ("info", C.c_void_p), ("geom", C.c_void_p),
+                ("neighbours", C.c_void_p), ("contents", C.c_void_p)]
+
+
+MATVEC_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double))
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB))
+        P = C.c_void_p
+        L.or_pair_coefficients.argtypes = [C.POINTER(OrPatches), C.c_int, P, P, C.c_double, C.c_int, P]
+        L.or_singular.argtypes = [C.POINTER(OrPatches), C.c_double, C.c_int, P]
+        L.or_near_create.argtypes = [C.POINTER(OrPatches), C.POINTER(OrTree), C.c_double, C.c_int]
+        L.or_near_create.restype = P
+        L.or_near_destroy.argtypes = [P]
+        L.or_near_count.argtypes = [P]
+        L.or_near_count.restype = C.c_int64
+        L.or_near_apply.argtypes = [P, P, P]
+        L.or_point_sums.argtypes = [C.c_int, P, P, P, C.c_int, C.c_double, P, P]
+        L.or_gmres.argtypes = [MATVEC_FN, P, C.c_int, P, P, C.c_double, C.c_int, C.c_int,
+                               C.POINTER(C.c_double)]
+        L.or_gmres.restype = C.c_int
+        if hasattr(L, "or_fmm_create"):
+            L.or_fmm_create.argtypes = [C.POINTER(OrPatches), C.POINTER(OrTree), C.c_double, C.c_double,
+                                        C.c_double, C.c_int]
+            L.or_fmm_create.restype = P
+            L.or_fmm_destroy.argtypes = [P]
+            L.or_fmm_apply.argtypes = [P, P, P]
+            L.or_fmm_direct.argtypes = [C.POINTER(OrPatches), C.c_double, C.c_double, C.c_int, P, P, P, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _c(a, dt=np.float64):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class Patches:
+    """Holds contiguous copies of the gathered patch arrays for the oracle."""
+
+    def __init__(self, a: dict):
+        self.a = {k: _c(a[k], np.int32 if k.endswith("_off") else np.float64)
+                  for k in ("centroid", "normal", "area", "eps", "gc", "qual_off", "qual", "quad_off", "quad",
+                            "gal_off", "gal")}
+        self.n = len(self.a["area"])
+        self.s = OrPatches(self.n, *(_p(self.a[k]) for k in (
+            "centroid", "normal", "area", "eps", "gc", "qual_off", "qual", "quad_off", "quad", "gal_off", "gal")))
+
+
+def neighbours_from_info(info: np.ndarray) -> np.ndarray:
+    """[n][27] same-level neighbour node ids (nb = 9(dz+1) + 3(dy+1) + dx+1)."""
+    key = {(int(r[0]), int(r[1]), int(r[2]), int(r[3])): k for k, r in enumerate(info)}
+    out = np.full((len(info), 27), -1, np.int32)
+    for k, r in enumerate(info):
+        L, x, y, z = (int(v) for v in r[:4])
+        for nb in range(27):
+            dz, dy, dx = nb // 9 - 1, (nb % 9) // 3 - 1, nb % 3 - 1
+            out[k, nb] = key.get((L, x + dx, y + dy, z + dz), -1)
+    return out
+
+
+class Tree:
+    def __init__(self, t: dict):
+        self.info = _c(t["info"], np.int32)
+        self.geom = _c(t["geom"])
+        self.contents = _c(t["contents"], np.int32)
+        self.neigh = neighbours_from_info(self.info)
+        self.n_levels = int(t["n_levels"])
+        self.s = OrTree(len(self.info), self.n_levels, _p(self.info), _p(self.geom), _p(self.neigh),
+                        _p(self.contents))
+
+
+def pair_coefficients(patches: Patches, I, J, kappa: float, fp32: bool) -> np.ndarray:
+    I = _c(I, np.int32)
+    J = _c(J, np.int32)
+    out = np.zeros((len(I), 4))
+    lib().or_pair_coefficients(C.byref(patches.s), len(I), _p(I), _p(J), kappa, int(fp32), _p(out))
+    return out
+
+
+def singular(patches: Patches, kappa: float, fp32: bool) -> np.ndarray:
+    out = np.zeros((patches.n, 4))
+    lib().or_singular(C.byref(patches.s), kappa, int(fp32), _p(out))
+    return out
+
+
+def point_sums(off, pts, charges, scale: float):
+    off = _c(off, np.int32)
+    pts = _c(pts)
+    ch = _c(charges)
+    n = len(off) - 1
+    a, b = np.zeros(n), np.zeros(n)
+    lib().or_point_sums(n, _p(off), _p(pts), _p(ch), len(ch), scale, _p(a), _p(b))
+    return a, b
+
+
+def rhs(patches: Patches, charges, eps_solvent: float) -> np.ndarray:
+    """BEEP::set_rhs restated with a direct sum (src/beep/beep.cpp:1124-1260)."""
+    ch = np.asarray(charges, float)
+    ch = ch[ch[:, 3] != 0]
+    a, b = point_sums(patches.a["qual_off"], patches.a["qual"], ch, 1.0 / (4 * np.pi * eps_solvent))
+    return np.concatenate([a, b])
+
+
+def energy_coefficients(gal_off, gal, area, charges, total_area: float):
+    """Mesh::init_energy_precalcs + renormalise_energy_precalcs (src/bem/mesh.cpp:730-925)."""
+    ch = np.asarray(charges, float)
+    ch = ch[ch[:, 3] != 0]
+    ech, ecf = point_sums(gal_off, gal, ch, 1.0 / (4 * np.pi))
+    total_f = -ecf.sum()
+    gauss_error = ch[:, 3].sum() - total_f
+    ecf = ecf - (np.asarray(area) / total_area) * gauss_error
+    return ecf, ech
+
+
+CONVERT_KJ_PER_MOL = 6.02214179e23 * 1.60217646e-19 ** 2 / (8.85418782e-12 * 1.0e-10 * 1000.0)
+
+
+def energy(f, h, ecf, ech, eps_ratio: float) -> float:
+    """Mesh::calculate_energy (src/bem/mesh.cpp:1373-1404), Kahan sum, kJ/mol."""
+    s = comp = 0.0
+    for fi, hi, cf, chh in zip(f, h, ecf, ech):
+        frag = hi * eps_ratio * chh - fi * cf
+        y = frag - comp
+        t = s + y
+        comp = (t - s) - y
+        s = t
+    return s * 0.5 * CONVERT_KJ_PER_MOL
+
+
+class Problem:
+    """Restated BEEP matvec over a given tree: cached near field (+ FMM)."""
+
+    def __init__(self, arrays: dict, tree: dict, kappa: float, fp32: bool, beta0: float = 1e-10,
+                 cube_edge: float | None = None, nterms: int = 9, far_field: bool = True):
+        self.patches = Patches(arrays)
+        self.tree = Tree(tree)
+        self.n = self.patches.n
+        self.kappa = kappa
+        L = lib()
+        self._near = L.or_near_create(C.byref(self.patches.s), C.byref(self.tree.s), kappa, int(fp32))
+        self._fmm = None
+        if far_field and self.tree.n_levels - 1 >= 2:
+            if not hasattr(L, "or_fmm_create"):
+                raise RuntimeError("the oracle has no far field")
+            self._fmm = L.or_fmm_create(C.byref(self.patches.s), C.byref(self.tree.s), kappa, beta0,
+                                        float(cube_edge), nterms)
+
+    @property
+    def n_records(self) -> int:
+        return int(lib().or_near_count(self._near))
+
+    def near(self, x) -> np.ndarray:
+        x = _c(x)
+        y = np.zeros(2 * self.n)
+        lib().or_near_apply(self._near, _p(x), _p(y))
+        return y
+
+    def far(self, x) -> np.ndarray:
+        y = np.zeros(2 * self.n)
+        if self._fmm is not None:
+            x = _c(x)
+            lib().or_fmm_apply(self._fmm, _p(x), _p(y))
+        return y
+
+    def matvec(self, x) -> np.ndarray:
+        return self.near(x) + self.far(x)
+
+    def solve(self, b, tol: float = 1e-6, max_iters: int = 100, restart: int = 0, x0=None):
+        b = _c(b)
+        x = np.zeros(2 * self.n) if x0 is None else _c(x0).copy()
+
+        @MATVEC_FN
+        def mv(_user, xp, yp):
+            xv = np.ctypeslib.as_array(xp, shape=(2 * self.n,))
+            yv = np.ctypeslib.as_array(yp, shape=(2 * self.n,))
+            yv[:] = self.matvec(xv.copy())
+
+        rr = C.c_double()
+        its = lib().or_gmres(mv, None, 2 * self.n, _p(b), _p(x), tol, max_iters, restart, C.byref(rr))
+        return x, its, rr.value
+
+    def close(self):
+        L = lib()
+        if self._near:
+            L.or_near_destroy(self._near)
+            self._near = None
+        if self._fmm:
+            L.or_fmm_destroy(self._fmm)
+            self._fmm = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
