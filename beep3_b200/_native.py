@@ -94,9 +94,9 @@ _SIGS = {
     "bp_problem_create": [_P, C.POINTER(bp_patches), C.POINTER(bp_params), _PP],
     "bp_problem_destroy": [_P],
     "bp_problem_info_get": [_P, C.POINTER(bp_problem_info)],
-    "bp_problem_tree": [_P, C.POINTER(_I), C.POINTER(_I), _P, _P, _P],
+    "bp_problem_tree": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_int64), _P, _P, _P],
     "bp_tree_create": [_I, _P, _P, _D, _I, _PP],
-    "bp_tree_export": [_P, C.POINTER(_I), C.POINTER(_I), _P, _P, _P],
+    "bp_tree_export": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_int64), _P, _P, _P],
     "bp_tree_destroy": [_P],
     "bp_matvec": [_P, _P, _P],
     "bp_matvec_device": [_P, _P, _P],

@@ -23,12 +23,12 @@ DEFAULT_NBSIZE = 1500  # DEFAULT_BEM_NEIGHBOURHOOD_SIZE, CPU build (src/beep/bee
 
 
 def _export_tree(export_fn, handle, n_points: int) -> dict:
-    nn, nl = C.c_int32(), C.c_int32()
-    N.check(export_fn(handle, C.byref(nn), C.byref(nl), None, None, None))
+    nn, nl, nc = C.c_int32(), C.c_int32(), C.c_int64()
+    N.check(export_fn(handle, C.byref(nn), C.byref(nl), C.byref(nc), None, None, None))
     info = np.zeros((nn.value, 18), np.int32)
     geom = np.zeros((nn.value, 4))
-    contents = np.zeros(n_points, np.int32)
-    N.check(export_fn(handle, None, None, N.ptr(info), N.ptr(geom), N.ptr(contents)))
+    contents = np.zeros(nc.value, np.int32)
+    N.check(export_fn(handle, None, None, None, N.ptr(info), N.ptr(geom), N.ptr(contents)))
     return dict(n_levels=nl.value, info=info, geom=geom, contents=contents)
 
 

@@ -210,9 +210,10 @@ BP_API int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info) {
   return BP_OK;
 }
 
-static int32_t export_tree(const TreeInfo& T, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info,
+static int32_t export_tree(const TreeInfo& T, int32_t* n_nodes, int32_t* n_levels, int64_t* n_contents, int32_t* node_info,
                            double* node_geom, int32_t* contents) {
   if (n_nodes) *n_nodes = (int32_t)T.nodes.size();
+  if (n_contents) *n_contents = (int64_t)T.contents.size();
   if (n_levels) *n_levels = T.n_levels;
   for (size_t k = 0; k < T.nodes.size(); ++k) {
     const TreeNode& nd = T.nodes[k];
@@ -239,11 +240,11 @@ static int32_t export_tree(const TreeInfo& T, int32_t* n_nodes, int32_t* n_level
   return BP_OK;
 }
 
-BP_API int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info,
+BP_API int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int64_t* n_contents, int32_t* node_info,
                                double* node_geom, int32_t* contents) {
   Problem* P = as_problem(p);
   if (!P) return fail(BP_ERR_INVALID, "bp_problem_tree: null problem");
-  return export_tree(P->tree, n_nodes, n_levels, node_info, node_geom, contents);
+  return export_tree(P->tree, n_nodes, n_levels, n_contents, node_info, node_geom, contents);
 }
 
 BP_API int32_t bp_tree_create(int32_t n, const double* points, const double cube_centre[3], double cube_edge,
@@ -257,10 +258,10 @@ BP_API int32_t bp_tree_create(int32_t n, const double* points, const double cube
   });
 }
 
-BP_API int32_t bp_tree_export(bp_tree t, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info, double* node_geom,
+BP_API int32_t bp_tree_export(bp_tree t, int32_t* n_nodes, int32_t* n_levels, int64_t* n_contents, int32_t* node_info, double* node_geom,
                               int32_t* contents) {
   if (!t) return fail(BP_ERR_INVALID, "bp_tree_export: null tree");
-  return export_tree(*reinterpret_cast<TreeInfo*>(t), n_nodes, n_levels, node_info, node_geom, contents);
+  return export_tree(*reinterpret_cast<TreeInfo*>(t), n_nodes, n_levels, n_contents, node_info, node_geom, contents);
 }
 
 BP_API int32_t bp_tree_destroy(bp_tree t) {

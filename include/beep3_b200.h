@@ -143,9 +143,10 @@ int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info);
  * 2 leaf, 4 shadow), parent, content_start, content_count, mp_idx, lc_idx,
  * child node ids 1..8 (-1 absent); nodes are level by level in the
  * reference's map order.  node_geom: [n_nodes][4] = centre xyz, edge.
- * contents: [n_patches] patch ids, node by node in insertion order.
+ * contents: [n_contents] patch ids of every node, node after node, each in
+ * insertion order (a patch appears once per level it is stored on).
  * Any output pointer may be NULL. */
-int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info, double* node_geom,
+int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int64_t* n_contents, int32_t* node_info, double* node_geom,
                         int32_t* contents);
 
 /* The same adaptive octree built on the host alone (no device needed):
@@ -155,7 +156,7 @@ int32_t bp_problem_tree(bp_problem p, int32_t* n_nodes, int32_t* n_levels, int32
 typedef struct bp_tree_s* bp_tree;
 int32_t bp_tree_create(int32_t n_points, const double* points, const double cube_centre[3], double cube_edge,
                        int32_t nbsize, bp_tree* out);
-int32_t bp_tree_export(bp_tree t, int32_t* n_nodes, int32_t* n_levels, int32_t* node_info, double* node_geom,
+int32_t bp_tree_export(bp_tree t, int32_t* n_nodes, int32_t* n_levels, int64_t* n_contents, int32_t* node_info, double* node_geom,
                        int32_t* contents);
 int32_t bp_tree_destroy(bp_tree t);
 

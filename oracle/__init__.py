@@ -38,7 +38,7 @@ class OrPatches(C.Structure):
 
 class OrTree(C.Structure):
     _fields_ = [("n_nodes", C.c_int32), ("n_levels", C.c_int32), ("info", C.c_void_p), ("geom", C.c_void_p),
-                ("neighbours", C.c_void_p), ("contents", C.c_void_p)]
+                ("neighbours", C.c_void_p), ("contents", C.c_void_p), ("n_contents", C.c_int64)]
 
 
 MATVEC_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double))
@@ -113,7 +113,7 @@ class Tree:
         self.neigh = neighbours_from_info(self.info)
         self.n_levels = int(t["n_levels"])
         self.s = OrTree(len(self.info), self.n_levels, _p(self.info), _p(self.geom), _p(self.neigh),
-                        _p(self.contents))
+                        _p(self.contents), len(self.contents))
 
 
 def pair_coefficients(patches: Patches, I, J, kappa: float, fp32: bool) -> np.ndarray:
