@@ -182,6 +182,7 @@ struct Problem {
   DevBuf d_diag;                                            // 4n double (singular + corrections)
   NearField nf;
   std::unique_ptr<FmmState, void (*)(FmmState*)> fmm{nullptr, fmm_destroy};
+  DevBuf fmm_contents;  // node-major patch lists of the tree (int32)
   // matvec scratch
   DevBuf d_x, d_y;  // 2n double each
   // Krylov workspace
@@ -201,20 +202,21 @@ struct StageTimes {
   int launches[kStages] = {0, 0, 0, 0, 0, 0, 0, 0};
   cudaStream_t stream = nullptr;
   int open_stage = -1;
-  cudaEvent_t open_ev = nullptr;
+  cudaEvent_t open_ev = nullptr, close_ev = nullptr;
+  // both events are created before the first is recorded, so no host-side
+  // event creation falls inside the measured interval
   void begin(int s, cudaStream_t st) {
     stream = st;
     open_stage = s;
     BP_CUDA(cudaEventCreate(&open_ev));
+    BP_CUDA(cudaEventCreate(&close_ev));
     BP_CUDA(cudaEventRecord(open_ev, st));
   }
   void end(int launches_in_stage) {
-    cudaEvent_t e;
-    BP_CUDA(cudaEventCreate(&e));
-    BP_CUDA(cudaEventRecord(e, stream));
-    recs.push_back({open_stage, open_ev, e});
+    BP_CUDA(cudaEventRecord(close_ev, stream));
+    recs.push_back({open_stage, open_ev, close_ev});
     launches[open_stage] += launches_in_stage;
-    open_ev = nullptr;
+    open_ev = close_ev = nullptr;
   }
   double ms(int s) const {
     double t = 0;
