@@ -50,6 +50,13 @@ def workload(name: str):
                              "(40962 patches), 2000 charges, eps 2/80, kappa 0.1, qual 4 / quad 0, "
                              "FMM order 9, reference tree nbsize 1500", patches=40962)
         return desc, [(mesh, None, (1, 0, 0, 0))], 0.1, 1500
+    if name == "star-small":
+        V, T, shape = b.star_surface(5, 20.0, seed=1235)
+        mesh = b.Mesh(V, T, b.charges_in_star(500, shape, seed=1236))
+        desc = dict(workload="star-shaped molecule R=20 A, icosphere k=5 (10242 patches), 500 charges, eps 2/80, "
+                             "kappa 0.1, qual 4 / quad 0, FMM order 9, reference tree nbsize 1500 "
+                             "(profiling case)", patches=10242)
+        return desc, [(mesh, None, (1, 0, 0, 0))], 0.1, 1500
     raise ValueError(f"unknown workload {name}")
 
 
@@ -152,6 +159,7 @@ def time_device_matvecs(bp, x, y, steps: int, flush) -> list[float]:
     L = N.lib()
     p = bp.build()
     stream = torch.cuda.current_stream()
+    assert stream.cuda_stream != 0, "time on a non-default stream"
     N.check(L.bp_ctx_set_stream(bp.context(), C.c_void_p(stream.cuda_stream)))
     out = []
     for _ in range(steps):
@@ -260,6 +268,32 @@ def run_ours(args):
     import torch
     world, rank, local, dist = dist_setup(args)
     torch.cuda.set_device(local)
+    # a dedicated (non-default) stream: the engine and the CUDA events of the
+    # timing run on it (the legacy default stream has handle 0, which the
+    # engine's bp_ctx_set_stream reads as "its own stream")
+    with torch.cuda.stream(torch.cuda.Stream()):
+        _run_ours(args, world, rank, local, dist)
+
+
+def _only_matvec(args, local):
+    """Profiling mode: the mixed engine only, W warm-up + K timed matvecs."""
+    import torch
+    desc, meshes, kappa, nbsize = workload(args.workload)
+    bp = build_beep(meshes, kappa, nbsize, "mixed", local)
+    dev = torch.device("cuda", local)
+    x = torch.randn(2 * bp.num_patches, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    time_device_matvecs(bp, x, y, args.warmup, None)
+    ms = time_device_matvecs(bp, x, y, args.steps, None)
+    print(json.dumps({"mode": "only-matvec", "config": desc, "ms_per_step": sum(ms) / len(ms)}), flush=True)
+    bp.close()
+
+
+def _run_ours(args, world, rank, local, dist):
+    import torch
+    if args.only_matvec:
+        _only_matvec(args, local)
+        return
     dev = torch.device("cuda", local)
     desc, meshes, kappa, nbsize = workload(args.workload)
     bp = build_beep(meshes, kappa, nbsize, "mixed", local)
@@ -361,7 +395,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="star", choices=["kirkwood", "star"])
+    ap.add_argument("--workload", default="star", choices=["kirkwood", "star", "star-small"])
+    ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

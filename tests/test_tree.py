@@ -1,0 +1,67 @@
+"""The engine's adaptive octree (host, C++) against the pure-Python
+restatement of the reference rules, plus structural invariants."""
+import numpy as np
+import pytest
+
+import beep3_b200 as b
+from beep3_b200.beep import build_tree
+from conftest import make_beep
+from oracle import tree as OT
+
+
+def scenario(k, nbsize, star=False, seed=3):
+    if star:
+        V, T, shape = b.star_surface(k, 20.0, seed=seed)
+        ch = b.charges_in_star(20, shape, seed=seed)
+    else:
+        V, T = b.icosphere(k, 10.0)
+        ch = b.charges_in_sphere(10, 7.0, seed=seed)
+    bp = make_beep(b.Mesh(V, T, ch), nbsize=nbsize)
+    pts = bp.gathered()["centroid"]
+    centre, edge = bp.calculate_bounding_cube()
+    return pts, centre, edge
+
+
+@pytest.mark.parametrize("k,nbsize,star", [(3, 60, False), (3, 200, False), (4, 100, False), (4, 300, True),
+                                           (3, 1500, False)])
+def test_tree_matches_python_restatement(k, nbsize, star):
+    pts, centre, edge = scenario(k, nbsize, star)
+    t = build_tree(pts, centre, edge, nbsize)
+    r = OT.build(pts, centre, edge, nbsize)
+    assert t["n_levels"] == r["n_levels"]
+    np.testing.assert_array_equal(t["info"], r["info"])
+    np.testing.assert_allclose(t["geom"], r["geom"], rtol=0, atol=1e-12)
+    np.testing.assert_array_equal(t["contents"], r["contents"])
+
+
+@pytest.mark.parametrize("k,nbsize", [(4, 100), (5, 400)])
+def test_tree_invariants(k, nbsize):
+    pts, centre, edge = scenario(k, nbsize)
+    t = build_tree(pts, centre, edge, nbsize)
+    info, contents = t["info"], t["contents"]
+    n = len(pts)
+    leaf = (info[:, 4] & 2) > 0
+    shadow = (info[:, 4] & 4) > 0
+    assert not np.any(leaf & shadow)
+    # leaves partition the patches
+    seen = np.zeros(n, int)
+    for r in info[leaf]:
+        seen[contents[r[6]:r[6] + r[7]]] += 1
+    assert np.all(seen == 1)
+    # every patch lies in its node's cube
+    for k_, r in enumerate(info):
+        c, e = t["geom"][k_, :3], t["geom"][k_, 3]
+        p = pts[contents[r[6]:r[6] + r[7]]]
+        if len(p):
+            assert np.all(np.abs(p - c) <= e / 2 * (1 + 1e-9))
+    # mean explicit work per item within the target (BEEP's nbsize rule)
+    key = {(int(r[0]), int(r[1]), int(r[2]), int(r[3])): int(r[7]) for r in info}
+    work = 0
+    for r in info[leaf]:
+        L, x, y, z = (int(v) for v in r[:4])
+        nb = sum(key.get((L, x + dx, y + dy, z + dz), 0) for dx in (-1, 0, 1) for dy in (-1, 0, 1)
+                 for dz in (-1, 0, 1))
+        work += nb * int(r[7])
+    assert work / n <= nbsize * 1.05
+    # children of split non-shadow nodes' neighbours exist (full neighbourhoods)
+    assert t["n_levels"] >= 3
