@@ -177,6 +177,7 @@ BP_API int32_t bp_problem_create(bp_ctx ctx, const bp_patches* pp, const bp_para
     nf_build_structure(*P);
     nf_assemble(*P);
     if (fmm_active(*P)) fmm_setup(*P);
+    matvec_setup(*P);
     BP_CUDA(cudaStreamSynchronize(c->stream));
     *out = reinterpret_cast<bp_problem>(P.release());
     return BP_OK;

@@ -185,10 +185,24 @@ struct Problem {
   DevBuf fmm_contents;  // node-major patch lists of the tree (int32)
   // matvec scratch
   DevBuf d_x, d_y;  // 2n double each
+  DevBuf d_yfar;    // 2n double: far field, added to the near field at the end
+  // graph of one matvec (d_gx -> d_gy): near field on the main stream and the
+  // FMM on a side stream, joined before the final add
+  DevBuf d_gx, d_gy;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool graph_failed = false;
   // Krylov workspace
   DevBuf d_V, d_w, d_scal;
   int krylov_m = 0;
   double tree_ms = 0, assemble_ms = 0;
+  ~Problem() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+  }
 };
 
 // Optional per-stage timing of a matvec with CUDA events on the stream.
@@ -239,11 +253,12 @@ struct StageTimes {
 // nearfield.cu
 void nf_build_structure(Problem& P);
 void nf_assemble(Problem& P);
-void nf_apply(Problem& P, const double* x_dev, double* y_dev);
+void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t stream);
 // fmm.cu
 bool fmm_active(const Problem& P);
 void fmm_setup(Problem& P);
-void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st);
+void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st, cudaStream_t stream);
+void matvec_setup(Problem& P);
 // krylov.cu
 void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st = nullptr);
 int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,

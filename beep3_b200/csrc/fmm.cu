@@ -42,7 +42,6 @@ namespace bp {
 namespace {
 
 constexpr int kCh = 12;
-constexpr int kXlCh = 2;  // channels per X2L block
 constexpr int kMaxNT = 18;
 
 template <typename T>
@@ -299,9 +298,9 @@ __global__ void __launch_bounds__(256) p2m_kernel(const __grid_constant__ Tables
 template <typename T>
 __device__ void shift_block(const Tables<T>& tb, int ifl, bool multipole, int level, const typename C2T<T>::type* in,
                             typename C2T<T>::type* w1, typename C2T<T>::type* w2, typename C2T<T>::type* out,
-                            const T* rd) {
+                            const T* rd, int c0, int nc) {
   using C = typename C2T<T>::type;
-  const int E = tb.E, NT = tb.nt, nout = kCh * E;
+  const int E = tb.E, NT = tb.nt, nout = nc * E;
   const T arg = T(0.70710678118654752440);
   C e1;
   if (multipole) {
@@ -348,7 +347,7 @@ __device__ void shift_block(const Tables<T>& tb, int ifl, bool multipole, int le
     int nn = 0;
     while (tri(nn + 1, 0) <= e) ++nn;
     const int m = e - tri(nn, 0);
-    const int lg = 2 * level + (ch >= 8 ? 1 : 0);
+    const int lg = 2 * level + (c0 + ch >= 8 ? 1 : 0);
     const T* dc = (multipole ? tb.mpshift : tb.lcshift) + (size_t)lg * (NT + 1) * (NT + 1) * (NT + 1);
     const C* src = w2 + ch * E;
     C v = cmk<C>(0, 0);
@@ -386,53 +385,56 @@ struct ShiftChild {
   int node, octant;
 };
 
+// M2M: one block per (parent, channel) gathering its children in order
 template <typename T>
-__global__ void __launch_bounds__(256) m2m_kernel(const __grid_constant__ Tables<T> tb, const ShiftItem* __restrict__ items,
-                                                  const ShiftChild* __restrict__ children, int child_level,
-                                                  typename C2T<T>::type* __restrict__ M) {
+__global__ void __launch_bounds__(64) m2m_kernel(const __grid_constant__ Tables<T> tb, const ShiftItem* __restrict__ items,
+                                                 const ShiftChild* __restrict__ children, int child_level,
+                                                 typename C2T<T>::type* __restrict__ M) {
   using C = typename C2T<T>::type;
   extern __shared__ unsigned char smem_raw[];
-  const int nout = kCh * tb.E;
+  const int E = tb.E;
   C* w1 = reinterpret_cast<C*>(smem_raw);
-  C* w2 = w1 + nout;
-  C* acc = w2 + nout;
-  C* in = acc + nout;
-  const ShiftItem it = items[blockIdx.x];
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) acc[o] = cmk<C>(0, 0);
+  C* w2 = w1 + E;
+  C* acc = w2 + E;
+  C* in = acc + E;
+  const ShiftItem it = items[blockIdx.x / kCh];
+  const int ch = blockIdx.x % kCh;
+  for (int o = threadIdx.x; o < E; o += blockDim.x) acc[o] = cmk<C>(0, 0);
   for (int c = 0; c < it.n_children; ++c) {
-    const ShiftChild ch = children[it.first_child + c];
+    const ShiftChild sc = children[it.first_child + c];
     __syncthreads();
-    for (int o = threadIdx.x; o < nout; o += blockDim.x) in[o] = M[(size_t)ch.node * nout + o];
+    for (int o = threadIdx.x; o < E; o += blockDim.x) in[o] = M[((size_t)sc.node * kCh + ch) * E + o];
     __syncthreads();
-    const T* rd = tb.R(ch.octant > 4 ? ROT_MSQ3 : ROT_SQ3);
-    shift_block<T>(tb, ch.octant, true, child_level, in, w1, w2, acc, rd);
+    const T* rd = tb.R(sc.octant > 4 ? ROT_MSQ3 : ROT_SQ3);
+    shift_block<T>(tb, sc.octant, true, child_level, in, w1, w2, acc, rd, ch, 1);
   }
   __syncthreads();
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) M[(size_t)it.parent * nout + o] = acc[o];
+  for (int o = threadIdx.x; o < E; o += blockDim.x) M[((size_t)it.parent * kCh + ch) * E + o] = acc[o];
 }
 
-// L2L: one block per child, local_child += shift(local_parent)
+// L2L: one block per (child, channel), local_child += shift(local_parent)
 template <typename T>
-__global__ void __launch_bounds__(256) l2l_kernel(const __grid_constant__ Tables<T> tb, const ShiftItem* __restrict__ items,
-                                                  const ShiftChild* __restrict__ children, int parent_level,
-                                                  typename C2T<T>::type* __restrict__ L) {
+__global__ void __launch_bounds__(64) l2l_kernel(const __grid_constant__ Tables<T> tb, const ShiftItem* __restrict__ items,
+                                                 const ShiftChild* __restrict__ children, int parent_level,
+                                                 typename C2T<T>::type* __restrict__ L) {
   using C = typename C2T<T>::type;
   extern __shared__ unsigned char smem_raw[];
-  const int nout = kCh * tb.E;
+  const int E = tb.E;
   C* w1 = reinterpret_cast<C*>(smem_raw);
-  C* w2 = w1 + nout;
-  C* acc = w2 + nout;
-  C* in = acc + nout;
-  const ShiftItem it = items[blockIdx.x];
-  const ShiftChild ch = children[it.first_child];
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
-    in[o] = L[(size_t)it.parent * nout + o];
-    acc[o] = L[(size_t)ch.node * nout + o];
+  C* w2 = w1 + E;
+  C* acc = w2 + E;
+  C* in = acc + E;
+  const ShiftItem it = items[blockIdx.x / kCh];
+  const int ch = blockIdx.x % kCh;
+  const ShiftChild sc = children[it.first_child];
+  for (int o = threadIdx.x; o < E; o += blockDim.x) {
+    in[o] = L[((size_t)it.parent * kCh + ch) * E + o];
+    acc[o] = L[((size_t)sc.node * kCh + ch) * E + o];
   }
   __syncthreads();
-  const T* rd = tb.R(ch.octant > 4 ? ROT_SQ3 : ROT_MSQ3);
-  shift_block<T>(tb, ch.octant, false, parent_level, in, w1, w2, acc, rd);
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) L[(size_t)ch.node * nout + o] = acc[o];
+  const T* rd = tb.R(sc.octant > 4 ? ROT_SQ3 : ROT_MSQ3);
+  shift_block<T>(tb, sc.octant, false, parent_level, in, w1, w2, acc, rd, ch, 1);
+  for (int o = threadIdx.x; o < E; o += blockDim.x) L[((size_t)sc.node * kCh + ch) * E + o] = acc[o];
 }
 
 // ---------------------------------------------------------------- M2X
@@ -563,16 +565,22 @@ __global__ void __launch_bounds__(kM2xThreads) m2x_kernel(const __grid_constant_
 
 // ---------------------------------------------------------------- X2L
 struct XlItem {
-  int parent_level, first_entry, n_entries;
-  int targets[8];  // target child node ids (-1 absent or shadow)
+  int parent_level;
+  int first_entry[3], n_entries[3];  // entries of each direction pair (UP/DOWN, N/S, E/W)
+  int targets[8];                    // target child node ids (-1 absent or shadow)
 };
 struct XlEntry {
   int src;          // source node id
   signed char dir, targ, a, b, c, up;
 };
 
-constexpr int kXlThreads = 256;
+constexpr int kXlGroup = 96;  // threads per direction pair (>= nexptotp)
+constexpr int kXlThreads = 3 * kXlGroup;
 
+// One block per (parent, channel); thread group g handles direction pair g:
+// its diagonal translations accumulated in shared memory per (direction,
+// target child), then yphystof + yexptolocal + rotation back per target;
+// the three pairs' local expansions are summed in a fixed order.
 template <typename T>
 __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__ Tables<T> tb,
                                                          const XlItem* __restrict__ items,
@@ -581,25 +589,27 @@ __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__
                                                          typename C2T<T>::type* __restrict__ L) {
   using C = typename C2T<T>::type;
   extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E, NT = tb.nt, nl = tb.nl, NPM = tb.np_max;
-  C* acc = reinterpret_cast<C*>(smem_raw);  // [6][8][kXlCh][NPM]
-  const XlItem it = items[blockIdx.x / (kCh / kXlCh)];
-  const int ch0 = (blockIdx.x % (kCh / kXlCh)) * kXlCh;
-  const int total = 6 * 8 * kXlCh * NPM;
-  for (int o = threadIdx.x; o < total; o += blockDim.x) acc[o] = cmk<C>(0, 0);
+  const int E = tb.E, nl = tb.nl, NPM = tb.np_max;
+  C* acc = reinterpret_cast<C*>(smem_raw);  // [6 dirs][8 targets][NPM]
+  C* mf = acc + 6 * 8 * NPM;                 // [3 pairs][2][64]
+  C* loc = mf + 3 * 2 * 64;                  // [3][E]
+  C* out = loc + 3 * E;                      // [3][E]
+  const XlItem it = items[blockIdx.x / kCh];
+  const int ch = blockIdx.x % kCh;
+  const int lg = 2 * it.parent_level + (ch >= 8 ? 1 : 0);
+  const int np = tb.nexptotp[lg], nexptot = tb.nexptot[lg];
+  const int g = threadIdx.x / kXlGroup, lt = threadIdx.x - g * kXlGroup;
+  for (int o = threadIdx.x; o < 6 * 8 * NPM; o += blockDim.x) acc[o] = cmk<C>(0, 0);
   __syncthreads();
-  // translations: thread owns (channel, i) pairs
-  for (int o = threadIdx.x; o < kXlCh * NPM; o += blockDim.x) {
-    const int cl = o / NPM, i = o - cl * NPM;
-    const int ch = ch0 + cl;
-    const int lg = 2 * it.parent_level + (ch >= 8 ? 1 : 0);
-    const int np = tb.nexptotp[lg];
-    if (i >= np) continue;
+  // translations of pair g
+  if (lt < np) {
+    const int i = lt;
     const C* xs = tb.xs + (size_t)lg * 3 * NPM;
     const C* ys = tb.ys + (size_t)lg * 3 * NPM;
     const T* zs = tb.zs + (size_t)lg * 3 * NPM;
-    for (int k = 0; k < it.n_entries; ++k) {
-      const XlEntry en = entries[it.first_entry + k];
+    const int e0 = it.first_entry[g], ne = it.n_entries[g];
+    for (int k = 0; k < ne; ++k) {
+      const XlEntry en = entries[e0 + k];
       const C w = W[(((size_t)en.src * 6 + en.dir) * kCh + ch) * NPM + i];
       C t;
       if (en.up) {
@@ -619,316 +629,322 @@ __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__
         if (en.a > 0) t = cmul(t, cconj(xs[(en.a - 1) * NPM + i]));
         else if (en.a < 0) t = cmul(t, xs[(-en.a - 1) * NPM + i]);
       }
-      C& a = acc[(((size_t)en.dir * 8 + en.targ) * kXlCh + cl) * NPM + i];
+      C& a = acc[((size_t)en.dir * 8 + en.targ) * NPM + i];
       a = cadd(a, cmul(w, t));
     }
   }
-  __syncthreads();
-  // conversion of the accumulated waves of each target to its local expansion
-  C* mf = acc + total;          // [kXlCh][2][64]
-  C* loc = mf + kXlCh * 2 * 64;  // [kXlCh][E]
-  C* out = loc + kXlCh * E;      // [kXlCh][E]
+  const int* numphys = tb.numphys + (size_t)lg * nl;
+  const C* fb = tb.fexpback + tb.fexpback_off[lg];
+  const T* rl = tb.rlsc + (size_t)lg * E * nl;
   for (int t = 0; t < 8; ++t) {
     const int tn = it.targets[t];
     if (tn < 0) continue;
-    for (int o = threadIdx.x; o < kXlCh * E; o += blockDim.x) out[o] = cmk<C>(0, 0);
-    for (int pair = 0; pair < 3; ++pair) {
-      __syncthreads();
-      // yphystof (up = dir 2*pair, down = 2*pair+1)
-      for (int o = threadIdx.x; o < kXlCh * 2 * 64; o += blockDim.x) {
-        const int cl = o / 128, rem = o - cl * 128, which = rem / 64, j = rem - which * 64;
-        const int ch = ch0 + cl;
-        const int lg = 2 * it.parent_level + (ch >= 8 ? 1 : 0);
-        if (j >= tb.nexptot[lg]) continue;
-        const int* numphys = tb.numphys + (size_t)lg * nl;
-        const C* fb = tb.fexpback + tb.fexpback_off[lg];
-        int l = 0, nftot = 0, nptot = 0, bb = 0;
-        while (nftot + tb.numfour[l] <= j) {
-          nftot += tb.numfour[l];
-          nptot += numphys[l] / 2;
-          bb += (tb.numfour[l] - 1) * (numphys[l] / 2);
-          ++l;
-        }
-        const int mm = j - nftot + 1;  // mode number 1..numfour
-        const int na = numphys[l], na2 = na / 2;
-        const C* ph = acc + (((size_t)(2 * pair + which) * 8 + t) * kXlCh + cl) * NPM + nptot;
-        C s = cmk<C>(0, 0);
-        if (mm == 1) {
-          for (int iv = 0; iv < na2; ++iv) s.x += T(2) * ph[iv].x;
-        } else if (mm & 1) {  // odd mm >= 3
-          const C* f = fb + bb + ((mm - 3) / 2) * na2;
-          for (int iv = 0; iv < na2; ++iv) s = cadd(s, cscale(f[iv], T(2) * ph[iv].x));
-        } else {  // even mm
-          const int nodd = (tb.numfour[l] - 1) / 2;
-          const C* f = fb + bb + nodd * na2 + ((mm - 2) / 2) * na2;
-          for (int iv = 0; iv < na2; ++iv) s = cadd(s, cmul(f[iv], cmk<C>(0, T(2) * ph[iv].y)));
-        }
-        mf[(cl * 2 + which) * 64 + j] = cscale(s, T(1) / T(na));
+    __syncthreads();
+    // yphystof of the pair's up (2g) and down (2g+1) waves
+    for (int o = lt; o < 2 * 64; o += kXlGroup) {
+      const int which = o / 64, j = o - which * 64;
+      if (j >= nexptot) continue;
+      int l = 0, nftot = 0, nptot = 0, bb = 0;
+      while (nftot + tb.numfour[l] <= j) {
+        nftot += tb.numfour[l];
+        nptot += numphys[l] / 2;
+        bb += (tb.numfour[l] - 1) * (numphys[l] / 2);
+        ++l;
       }
-      __syncthreads();
-      // yexptolocal
-      for (int o = threadIdx.x; o < kXlCh * E; o += blockDim.x) {
-        const int cl = o / E, e = o - cl * E;
-        const int ch = ch0 + cl;
-        const int lg = 2 * it.parent_level + (ch >= 8 ? 1 : 0);
-        const T* rl = tb.rlsc + (size_t)lg * E * nl;
-        int nm = 0;
-        while (tri(nm + 1, 0) <= e) ++nm;
-        const int mth = e - tri(nm, 0);
-        const C* fu = mf + (cl * 2 + 0) * 64;
-        const C* fd = mf + (cl * 2 + 1) * 64;
-        C v = cmk<C>(0, 0);
-        int ntot = 0;
-        for (int l = 0; l < nl; ++l) {
-          const int mmax = tb.numfour[l] - 1 > nm ? nm : tb.numfour[l] - 1;
-          if (mth <= mmax) {
-            const C pm = (nm & 1) ? csub(fd[ntot + mth], fu[ntot + mth]) : cadd(fd[ntot + mth], fu[ntot + mth]);
-            v = cadd(v, cscale(pm, rl[(size_t)e * nl + l] * tb.weights[l]));
-          }
-          ntot += tb.numfour[l];
+      const int mm = j - nftot + 1;
+      const int na = numphys[l], na2 = na / 2;
+      const C* ph = acc + ((size_t)(2 * g + which) * 8 + t) * NPM + nptot;
+      C sum = cmk<C>(0, 0);
+      if (mm == 1) {
+        for (int iv = 0; iv < na2; ++iv) sum.x += T(2) * ph[iv].x;
+      } else if (mm & 1) {
+        const C* f = fb + bb + ((mm - 3) / 2) * na2;
+        for (int iv = 0; iv < na2; ++iv) sum = cadd(sum, cscale(f[iv], T(2) * ph[iv].x));
+      } else {
+        const int nodd = (tb.numfour[l] - 1) / 2;
+        const C* f = fb + bb + nodd * na2 + ((mm - 2) / 2) * na2;
+        for (int iv = 0; iv < na2; ++iv) sum = cadd(sum, cmul(f[iv], cmk<C>(0, T(2) * ph[iv].y)));
+      }
+      mf[(g * 2 + which) * 64 + j] = cscale(sum, T(1) / T(na));
+    }
+    __syncthreads();
+    // yexptolocal
+    for (int e = lt; e < E; e += kXlGroup) {
+      int nm = 0;
+      while (tri(nm + 1, 0) <= e) ++nm;
+      const int mth = e - tri(nm, 0);
+      const C* fu = mf + (g * 2 + 0) * 64;
+      const C* fd = mf + (g * 2 + 1) * 64;
+      C v = cmk<C>(0, 0);
+      int ntot = 0;
+      for (int l = 0; l < nl; ++l) {
+        const int mmax = tb.numfour[l] - 1 > nm ? nm : tb.numfour[l] - 1;
+        if (mth <= mmax) {
+          const C pm = (nm & 1) ? csub(fd[ntot + mth], fu[ntot + mth]) : cadd(fd[ntot + mth], fu[ntot + mth]);
+          v = cadd(v, cscale(pm, rl[(size_t)e * nl + l] * tb.weights[l]));
         }
-        const T rs = T(3.14159265358979323846) / (tb.betascal[lg] * T(2)) * tb.sfac[e];
-        v = cscale(v, rs);
-        switch (mth & 3) {  // * i^m
+        ntot += tb.numfour[l];
+      }
+      const T rs = T(3.14159265358979323846) / (tb.betascal[lg] * T(2)) * tb.sfac[e];
+      v = cscale(v, rs);
+      switch (mth & 3) {  // * i^m
+        case 1: v = cmk<C>(-v.y, v.x); break;
+        case 2: v = cmk<C>(-v.x, -v.y); break;
+        case 3: v = cmk<C>(v.y, -v.x); break;
+        default: break;
+      }
+      loc[g * E + e] = v;
+    }
+    __syncthreads();
+    // rotate back
+    for (int e = lt; e < E; e += kXlGroup) {
+      if (g == 0) {
+        out[e] = loc[e];
+        continue;
+      }
+      int l = 0;
+      while (tri(l + 1, 0) <= e) ++l;
+      const int m = e - tri(l, 0);
+      if (g == 1) {  // rotate_ytoz(rdpi2): rotate then * i^m
+        C v = rotate_one<T>(tb, loc + E, tb.R(ROT_PI2), l, m);
+        switch (m & 3) {
           case 1: v = cmk<C>(-v.y, v.x); break;
           case 2: v = cmk<C>(-v.x, -v.y); break;
           case 3: v = cmk<C>(v.y, -v.x); break;
           default: break;
         }
-        loc[o] = v;
-      }
-      __syncthreads();
-      // rotate back and accumulate
-      for (int o = threadIdx.x; o < kXlCh * E; o += blockDim.x) {
-        const int cl = o / E, e = o - cl * E;
-        if (pair == 0) {
-          out[o] = cadd(out[o], loc[o]);
-          continue;
-        }
-        int l = 0;
-        while (tri(l + 1, 0) <= e) ++l;
-        const int m = e - tri(l, 0);
-        if (pair == 1) {  // rotate_ytoz(rdpi2): rotate then * i^m
-          C v = rotate_one<T>(tb, loc + cl * E, tb.R(ROT_PI2), l, m);
-          switch (m & 3) {
-            case 1: v = cmk<C>(-v.y, v.x); break;
-            case 2: v = cmk<C>(-v.x, -v.y); break;
-            case 3: v = cmk<C>(v.y, -v.x); break;
-            default: break;
-          }
-          out[o] = cadd(out[o], v);
-        } else {  // rotate_ztox(rdmpi2)
-          out[o] = cadd(out[o], rotate_one<T>(tb, loc + cl * E, tb.R(ROT_MPI2), l, m));
-        }
+        out[E + e] = v;
+      } else {  // rotate_ztox(rdmpi2)
+        out[2 * E + e] = rotate_one<T>(tb, loc + 2 * E, tb.R(ROT_MPI2), l, m);
       }
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < kXlCh * E; o += blockDim.x) {
-      const int cl = o / E, e = o - cl * E;
-      L[((size_t)tn * kCh + ch0 + cl) * E + e] = out[o];
-    }
+    for (int e = threadIdx.x; e < E; e += blockDim.x)
+      L[((size_t)tn * kCh + ch) * E + e] = cadd(cadd(out[e], out[E + e]), out[2 * E + e]);
   }
-  (void)NT;
 }
 
 // ---------------------------------------------------------------- L2P
+// evaluate_local_expansion_at_xyz computes, per target point, q(n,m) =
+// i_n P_n^m e^{im phi}, its gradient gq and Hessian g2q through the ladder
+// relations of grad_q / grad2_q (src/fmm/fmm.h:128-415), and contracts them
+// with the local coefficients.  Every quantity FMM_results_to_BEM needs is
+// linear in q, so the ladders are transposed onto the coefficients once per
+// leaf (l2p_prep_kernel): per screening group one expansion F for f and three
+// H_j for h, and a target only evaluates q and four dot products per group
+// (l2p_eval_kernel).  Same mathematics, summed in a different order.
 struct LeafItem {
   int node, level, start, count;
+  int leaf;  // index of the leaf's derivative expansions (eval chunks of a leaf share it)
   double c[3];
 };
 
-constexpr int kL2pWarps = 4;
-
-// per-warp evaluation of the channel sums of FMM_results_to_BEM for one
-// screening group; lanes over coefficients; returns (f, h) partial sums
+// One term of a ladder output: coef * S(a, b) or coef * conj(S(a, b)).
 template <typename T>
-__device__ void l2p_group(const Tables<T>& tb, int g, int level, double d, double ctheta,
-                          const typename C2T<T>::type& e1, const double nrm[3], const typename C2T<T>::type* Lc,
-                          typename C2T<T>::type* q, typename C2T<T>::type* gq, typename C2T<T>::type* g2,
-                          T* bi, T* p, double& f_acc, double& h_acc) {
-  using C = typename C2T<T>::type;
-  const int lane = threadIdx.x & 31;
-  const int NT = tb.nt, N2 = NT + 2, E = tb.E;
-  const int EQ = (N2 + 1) * (N2 + 2) / 2;      // q: n <= NT+2
-  const int EG = (NT + 2) * (NT + 3) / 2;      // gq: n <= NT+1
-  const int lg = 2 * level + g;
-  const T beta = tb.beta[g], scale = tb.scale[lg], isc = T(1) / scale;
-  if (lane == 0) bessel_in_dev<T>(scale, (T)(d * (double)beta), N2, bi);
-  // Legendre: lane m computes column m
-  {
-    const T x = (T)ctheta;
-    const T u = -sqrt(T(1) - x * x);
-    if (lane <= N2) {
-      const int m = lane;
-      T pmm = 1;
-      for (int k = 1; k <= m; ++k) pmm = pmm * u * T(2 * k - 1);
-      p[tri(m, m)] = pmm;
-      if (m < N2) {
-        T p1 = T(2 * m + 1) * x * pmm;
-        p[tri(m + 1, m)] = p1;
-        T p0 = pmm;
-        for (int n = m + 2; n <= N2; ++n) {
-          const T pn = ((T(2) * n - T(1)) * x * p1 - T(n + m - 1) * p0) / T(n - m);
-          p[tri(n, m)] = pn;
-          p0 = p1;
-          p1 = pn;
-        }
-      }
-    }
+struct LTerm {
+  int a, b;
+  T re, im;
+  bool conj;
+};
+
+// Terms of component d of the ladder at output (n, m) (grad_q, src/fmm/fmm.h:128-208).
+template <typename T>
+__device__ int ladder_terms(int n, int m, int d, T sc, T isc, T beta, LTerm<T> out[4]) {
+  // l0, l1, l2, r0, r1, r2 as (scale, a, b, conj, valid)
+  struct P {
+    T s;
+    int a, b;
+    bool c, v;
+  } l[3] = {{0, 0, 0, false, false}, {0, 0, 0, false, false}, {0, 0, 0, false, false}},
+    r[3] = {{0, 0, 0, false, false}, {0, 0, 0, false, false}, {0, 0, 0, false, false}};
+  if (n == 0 && m == 0) {
+    r[0] = {-sc, 1, 1, true, true};
+    r[1] = {-sc, 1, 0, false, true};
+    r[2] = {sc, 1, 1, false, true};
+  } else if (n == 1 && m == 0) {
+    l[1] = {isc, 0, 0, false, true};
+    r[0] = {-sc, 2, 1, true, true};
+    r[1] = {-T(2) * sc, 2, 0, false, true};
+    r[2] = {sc, 2, 1, false, true};
+  } else if (m == 0) {
+    l[0] = {-isc, n - 1, 1, true, true};
+    l[1] = {T(n) * isc, n - 1, 0, false, true};
+    l[2] = {isc, n - 1, 1, false, true};
+    r[0] = {-sc, n + 1, 1, true, true};
+    r[1] = {-T(n + 1) * sc, n + 1, 0, false, true};
+    r[2] = {sc, n + 1, 1, false, true};
+  } else if (n == 1 && m == 1) {
+    l[0] = {T(2) * isc, 0, 0, false, true};
+    r[0] = {T(2) * sc, 2, 0, false, true};
+    r[1] = {-sc, 2, 1, false, true};
+    r[2] = {sc, 2, 2, false, true};
+  } else if (m == n) {
+    l[0] = {T((n + n - 1) * (n + n)) * isc, n - 1, n - 1, false, true};
+    r[0] = {T(2) * sc, n + 1, n - 1, false, true};
+    r[1] = {-sc, n + 1, n, false, true};
+    r[2] = {sc, n + 1, n + 1, false, true};
+  } else if (m == n - 1) {
+    l[0] = {T((n + m - 1) * (n + m)) * isc, n - 1, n - 2, false, true};
+    l[1] = {T(n + m) * isc, n - 1, n - 1, false, true};
+    r[0] = {T(6) * sc, n + 1, m - 1, false, true};
+    r[1] = {-T(2) * sc, n + 1, m, false, true};
+    r[2] = {sc, n + 1, m + 1, false, true};
+  } else {
+    l[0] = {T((n + m - 1) * (n + m)) * isc, n - 1, m - 1, false, true};
+    l[1] = {T(n + m) * isc, n - 1, m, false, true};
+    l[2] = {isc, n - 1, m + 1, false, true};
+    r[0] = {T((n - m + 1) * (n - m + 2)) * sc, n + 1, m - 1, false, true};
+    r[1] = {-T(n - m + 1) * sc, n + 1, m, false, true};
+    r[2] = {sc, n + 1, m + 1, false, true};
   }
-  __syncwarp();
-  for (int e = lane; e < EQ; e += 32) {
-    int n = 0;
-    while (tri(n + 1, 0) <= e) ++n;
-    const int m = e - tri(n, 0);
-    if (n == 0) {
-      q[e] = cmk<C>(bi[0], 0);
-    } else {
-      C ph = cmk<C>(1, 0);
-      for (int k = 0; k < m; ++k) ph = cmul(ph, e1);
-      q[e] = cscale(ph, bi[n] * p[e]);
-    }
-  }
-  __syncwarp();
-  // ladder (grad_q) from a source array src(n, m) with triangle width
-  auto ladder = [&](const C* src, int n, int m, C out[3]) {
-    C left[3], right[3];
-    auto S = [&](int a, int b) { return src[tri(a, b)]; };
-    const T sc = scale;
-    if (n == 0 && m == 0) {
-      left[0] = left[1] = left[2] = cmk<C>(0, 0);
-      right[0] = cscale(cconj(S(1, 1)), -sc);
-      right[1] = cscale(S(1, 0), -sc);
-      right[2] = cscale(S(1, 1), sc);
-    } else if (n == 1 && m == 0) {
-      left[0] = cmk<C>(0, 0);
-      left[1] = cscale(S(0, 0), isc);
-      left[2] = cmk<C>(0, 0);
-      right[0] = cscale(cconj(S(2, 1)), -sc);
-      right[1] = cscale(S(2, 0), -T(2) * sc);
-      right[2] = cscale(S(2, 1), sc);
-    } else if (m == 0) {
-      left[0] = cscale(cconj(S(n - 1, 1)), -isc);
-      left[1] = cscale(S(n - 1, 0), T(n) * isc);
-      left[2] = cscale(S(n - 1, 1), isc);
-      right[0] = cscale(cconj(S(n + 1, 1)), -sc);
-      right[1] = cscale(S(n + 1, 0), -T(n + 1) * sc);
-      right[2] = cscale(S(n + 1, 1), sc);
-    } else if (n == 1 && m == 1) {
-      left[0] = cscale(S(0, 0), T(2) * isc);
-      left[1] = left[2] = cmk<C>(0, 0);
-      right[0] = cscale(S(2, 0), T(2) * sc);
-      right[1] = cscale(S(2, 1), -sc);
-      right[2] = cscale(S(2, 2), sc);
-    } else if (m == n) {
-      left[0] = cscale(S(n - 1, n - 1), T((n + n - 1) * (n + n)) * isc);
-      left[1] = left[2] = cmk<C>(0, 0);
-      right[0] = cscale(S(n + 1, n - 1), T(2) * sc);
-      right[1] = cscale(S(n + 1, n), -sc);
-      right[2] = cscale(S(n + 1, n + 1), sc);
-    } else if (m == n - 1) {
-      left[0] = cscale(S(n - 1, n - 2), T((n + m - 1) * (n + m)) * isc);
-      left[1] = cscale(S(n - 1, n - 1), T(n + m) * isc);
-      left[2] = cmk<C>(0, 0);
-      right[0] = cscale(S(n + 1, m - 1), T(6) * sc);
-      right[1] = cscale(S(n + 1, m), -T(2) * sc);
-      right[2] = cscale(S(n + 1, m + 1), sc);
-    } else {
-      left[0] = cscale(S(n - 1, m - 1), T((n + m - 1) * (n + m)) * isc);
-      left[1] = cscale(S(n - 1, m), T(n + m) * isc);
-      left[2] = cscale(S(n - 1, m + 1), isc);
-      right[0] = cscale(S(n + 1, m - 1), T((n - m + 1) * (n - m + 2)) * sc);
-      right[1] = cscale(S(n + 1, m), -T(n - m + 1) * sc);
-      right[2] = cscale(S(n + 1, m + 1), sc);
-    }
-    const T pre = T(-0.5) / T(2 * n + 1);
-    const C a0 = csub(left[0], right[0]), a2 = csub(left[2], right[2]), a1 = csub(left[1], right[1]);
-    out[0] = cscale(csub(a0, a2), pre * beta);
-    const C s = cadd(a0, a2);
-    out[1] = cmk<C>(-s.y * pre * beta, s.x * pre * beta);
-    out[2] = cscale(a1, pre * beta * T(-2));
+  const T pb = T(-0.5) / T(2 * n + 1) * beta;
+  int k = 0;
+  auto add = [&](const P& p, T fr, T fi) {
+    if (!p.v) return;
+    out[k++] = {p.a, p.b, p.s * fr, p.s * fi, p.c};
   };
-  for (int e = lane; e < EG; e += 32) {
-    int n = 0;
-    while (tri(n + 1, 0) <= e) ++n;
-    const int m = e - tri(n, 0);
-    C o[3];
-    ladder(q, n, m, o);
-    gq[e] = o[0];
-    gq[EG + e] = o[1];
-    gq[2 * EG + e] = o[2];
+  if (d == 0) {  // pb ((l0 - r0) - (l2 - r2))
+    add(l[0], pb, 0);
+    add(r[0], -pb, 0);
+    add(l[2], -pb, 0);
+    add(r[2], pb, 0);
+  } else if (d == 1) {  // i pb ((l0 - r0) + (l2 - r2))
+    add(l[0], 0, pb);
+    add(r[0], 0, -pb);
+    add(l[2], 0, pb);
+    add(r[2], 0, -pb);
+  } else {  // -2 pb (l1 - r1)
+    add(l[1], -T(2) * pb, 0);
+    add(r[1], T(2) * pb, 0);
   }
-  __syncwarp();
-  for (int e = lane; e < E; e += 32) {
-    int n = 0;
-    while (tri(n + 1, 0) <= e) ++n;
-    const int m = e - tri(n, 0);
-    for (int i = 0; i < 3; ++i) {
-      C o[3];
-      ladder(gq + i * EG, n, m, o);
-      for (int c = 0; c < 3; ++c) g2[(c * 3 + i) * E + e] = o[c];  // g2q(c, i)
-    }
-  }
-  __syncwarp();
-  // channel sums of FMM_results_to_BEM (per group)
-  const int c0 = g ? 8 : 0;
-  double fp = 0, hp = 0;
-  for (int e = lane; e < E; e += 32) {
-    int n = 0;
-    while (tri(n + 1, 0) <= e) ++n;
-    const int m = e - tri(n, 0);
-    const double w = m ? 2.0 : 1.0;
-    auto re = [&](C a, C b) { return (double)a.x * (double)b.x - (double)a.y * (double)b.y; };
-    const C* Lg = Lc;  // [12][E]
-    // f: d/dx of ch0 + d/dy of ch1 + d/dz of ch2 + pot of ch3 (group 0); channels 8-11 for group 1
-    double f = re(gq[e], Lg[(c0 + 0) * E + e]) + re(gq[EG + e], Lg[(c0 + 1) * E + e]) +
-               re(gq[2 * EG + e], Lg[(c0 + 2) * E + e]) + re(q[e], Lg[(c0 + 3) * E + e]);
-    // h: sum_j n_j (H_jk + H_kj)/2 on channels c0h+k, plus n . grad on the last channel
-    const int c0h = g ? 8 : 4, clast = g ? 11 : 7;
-    double h = 0;
-    for (int k = 0; k < 3; ++k) {
-      for (int j = 0; j < 3; ++j) {
-        const C hjk = g2[(j * 3 + k) * E + e], hkj = g2[(k * 3 + j) * E + e];
-        h += 0.5 * nrm[j] * (re(hjk, Lg[(c0h + k) * E + e]) + re(hkj, Lg[(c0h + k) * E + e]));
-      }
-    }
-    h += nrm[0] * re(gq[e], Lg[clast * E + e]) + nrm[1] * re(gq[EG + e], Lg[clast * E + e]) +
-         nrm[2] * re(gq[2 * EG + e], Lg[clast * E + e]);
-    fp += w * f;
-    hp += w * h;
-  }
-  const double tbp = (double)beta * (2.0 / 3.14159265358979323846);
-  f_acc += (g ? -1.0 : 1.0) * fp * tbp;
-  h_acc += (g ? -1.0 : 1.0) * hp * tbp;
-  __syncwarp();
+  return k;
 }
 
+// D += adjoint of ladder component d applied to W (outputs n <= nin):
+// sum_{n,m} Re[ladder_d(S)(n,m) W(n,m)] = sum Re[S(a,b) D(a,b)].
+// Sequential scatter by the calling thread (deterministic).
 template <typename T>
-__global__ void __launch_bounds__(32 * kL2pWarps) l2p_kernel(const __grid_constant__ Tables<T> tb,
-                                                             const LeafItem* __restrict__ items,
-                                                             const int32_t* __restrict__ contents,
-                                                             const double* __restrict__ centroid,
-                                                             const double* __restrict__ normal,
-                                                             const typename C2T<T>::type* __restrict__ L, int n,
-                                                             double* __restrict__ y) {
+__device__ void adjoint_ladder(const typename C2T<T>::type* W, int nin, int d, T sc, T isc, T beta,
+                               typename C2T<T>::type* D) {
+  using C = typename C2T<T>::type;
+  LTerm<T> t[4];
+  for (int n = 0; n <= nin; ++n)
+    for (int m = 0; m <= n; ++m) {
+      const C w = W[tri(n, m)];
+      const int k = ladder_terms<T>(n, m, d, sc, isc, beta, t);
+      for (int j = 0; j < k; ++j) {
+        // kappa * w, conjugated for conj terms
+        const T re = t[j].re * w.x - t[j].im * w.y;
+        const T im = t[j].re * w.y + t[j].im * w.x;
+        C& dst = D[tri(t[j].a, t[j].b)];
+        dst.x += re;
+        dst.y += t[j].conj ? -im : im;
+      }
+    }
+}
+
+// Per leaf and screening group g: F = A_x[V_a] + A_y[V_a+1] + A_z[V_a+2] + V_a+3
+// and H_j = 1/2 sum_k (A_k[A_j[V_b+k]] + A_j[A_k[V_b+k]]) + A_j[V_last], with
+// V_c = w_m L_c (w_0 = 1, w_m>0 = 2), all scaled by sign_g * 2 beta_g / pi.
+// Output [leaf][g][4][EQ]: F then H_0, H_1, H_2.
+template <typename T>
+__global__ void __launch_bounds__(64) l2p_prep_kernel(const __grid_constant__ Tables<T> tb,
+                                                      const LeafItem* __restrict__ items,
+                                                      const typename C2T<T>::type* __restrict__ L,
+                                                      typename C2T<T>::type* __restrict__ D) {
   using C = typename C2T<T>::type;
   extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E, NT = tb.nt;
-  const int EQ = (NT + 3) * (NT + 4) / 2, EG = (NT + 2) * (NT + 3) / 2;
-  C* Lc = reinterpret_cast<C*>(smem_raw);  // [12][E]
-  const int per_warp = EQ + 3 * EG + 9 * E;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* ws = Lc + kCh * E + (size_t)warp * per_warp;
-  C* q = ws;
-  C* gq = q + EQ;
-  C* g2 = gq + 3 * EG;
-  T* scal = reinterpret_cast<T*>(Lc + kCh * E + (size_t)kL2pWarps * per_warp) + (size_t)warp * (EQ + NT + 4);
-  T* p = scal;
-  T* bi = p + EQ;
+  const int NT = tb.nt, E = tb.E;
+  const int EQ = (NT + 3) * (NT + 4) / 2;
   const LeafItem it = items[blockIdx.x];
-  for (int o = threadIdx.x; o < kCh * E; o += blockDim.x) Lc[o] = L[(size_t)it.node * kCh * E + o];
+  // per group: V (6 channels used: a..a+3 for f, b..b+2 and last for h) [8][EQ],
+  // first level buffers F-part [3][EQ] and U[3][3][EQ], result [4][EQ]
+  C* base = reinterpret_cast<C*>(smem_raw);
+  const int per_group = (8 + 3 + 9 + 4) * EQ;
+  for (int o = threadIdx.x; o < 2 * per_group; o += blockDim.x) base[o] = cmk<C>(0, 0);
   __syncthreads();
-  for (int k = warp; k < it.count; k += kL2pWarps) {
+  for (int o = threadIdx.x; o < 2 * 8 * E; o += blockDim.x) {
+    const int g = o / (8 * E), rem = o - g * 8 * E, slot = rem / E, e = rem - slot * E;
+    // slots: 0..3 -> f channels, 4..6 -> h channels, 7 -> last
+    const int ch = g == 0 ? (slot < 4 ? slot : (slot < 7 ? 4 + (slot - 4) : 7))
+                          : (slot < 4 ? 8 + slot : (slot < 7 ? 8 + (slot - 4) : 11));
+    int n = 0;
+    while (tri(n + 1, 0) <= e) ++n;
+    const int m = e - tri(n, 0);
+    const C v = L[((size_t)it.node * kCh + ch) * E + e];
+    base[(size_t)g * per_group + slot * EQ + e] = cscale(v, m ? T(2) : T(1));
+  }
+  __syncthreads();
+  // first level: 3 F parts + 9 U per group = 24 passes
+  if (threadIdx.x < 24) {
+    const int g = threadIdx.x / 12, p = threadIdx.x % 12;
+    C* G = base + (size_t)g * per_group;
+    const int lg = 2 * it.level + g;
+    const T beta = tb.beta[g], sc = tb.scale[lg], isc = T(1) / sc;
+    if (p < 3) {
+      adjoint_ladder<T>(G + p * EQ, NT, p, sc, isc, beta, G + (8 + p) * EQ);
+    } else {
+      const int j = (p - 3) / 3, k = (p - 3) % 3;  // U_{j,k} = A_j[V_{b+k}]
+      adjoint_ladder<T>(G + (4 + k) * EQ, NT, j, sc, isc, beta, G + (11 + 3 * j + k) * EQ);
+    }
+  }
+  __syncthreads();
+  // second level: F sum (1 thread) and H_j (3 threads) per group
+  if (threadIdx.x < 8) {
+    const int g = threadIdx.x / 4, p = threadIdx.x % 4;
+    C* G = base + (size_t)g * per_group;
+    C* R = G + 20 * EQ;
+    const int lg = 2 * it.level + g;
+    const T beta = tb.beta[g], sc = tb.scale[lg], isc = T(1) / sc;
+    if (p == 0) {
+      for (int e = 0; e < EQ; ++e) {
+        C v = cadd(cadd(G[8 * EQ + e], G[9 * EQ + e]), G[10 * EQ + e]);
+        if (e < E) v = cadd(v, G[3 * EQ + e]);
+        R[e] = v;
+      }
+    } else {
+      const int j = p - 1;
+      C* H = R + p * EQ;
+      // A_k[U_{j,k}] and A_j[U_{k,k}] at weight 1/2 each: accumulate into H
+      // with a scratch buffer of the same size
+      for (int k = 0; k < 3; ++k) {
+        adjoint_ladder<T>(G + (11 + 3 * j + k) * EQ, NT + 1, k, sc * T(1), isc, beta * T(0.5), H);
+        adjoint_ladder<T>(G + (11 + 3 * k + k) * EQ, NT + 1, j, sc, isc, beta * T(0.5), H);
+      }
+      adjoint_ladder<T>(G + 7 * EQ, NT, j, sc, isc, beta, H);
+    }
+  }
+  __syncthreads();
+  // scale by sign_g * 2 beta_g / pi and store
+  for (int o = threadIdx.x; o < 2 * 4 * EQ; o += blockDim.x) {
+    const int g = o / (4 * EQ), rem = o - g * 4 * EQ;
+    const T f = (g ? T(-1) : T(1)) * tb.beta[g] * T(0.63661977236758134308);
+    D[((size_t)blockIdx.x * 2 + g) * 4 * EQ + rem] = cscale(base[(size_t)g * per_group + 20 * EQ + rem], f);
+  }
+}
+
+// One thread per target patch: q(n, m) generated on the fly (Bessel,
+// Legendre recurrence in n for each m, e^{i m phi}) and contracted with the
+// leaf's F and H_j; y_f += f / 4 pi, y_h += n . h / 4 pi.
+constexpr int kEvalChunk = 64;  // targets per l2p_eval block
+
+template <typename T>
+__global__ void __launch_bounds__(kEvalChunk) l2p_eval_kernel(const __grid_constant__ Tables<T> tb,
+                                                       const LeafItem* __restrict__ items,
+                                                       const int32_t* __restrict__ contents,
+                                                       const double* __restrict__ centroid,
+                                                       const double* __restrict__ normal,
+                                                       const typename C2T<T>::type* __restrict__ D, int n,
+                                                       double* __restrict__ y) {
+  using C = typename C2T<T>::type;
+  extern __shared__ unsigned char smem_raw[];
+  const int NT = tb.nt, N2 = NT + 2;
+  const int EQ = (NT + 3) * (NT + 4) / 2;
+  C* Ds = reinterpret_cast<C*>(smem_raw);  // [2][4][EQ]
+  const LeafItem it = items[blockIdx.x];
+  for (int o = threadIdx.x; o < 8 * EQ; o += blockDim.x) Ds[o] = D[(size_t)it.leaf * 8 * EQ + o];
+  __syncthreads();
+  for (int k = threadIdx.x; k < it.count; k += blockDim.x) {
     const int i = contents[it.start + k];
     const double rx = centroid[3 * i] - it.c[0], ry = centroid[3 * i + 1] - it.c[1], rz = centroid[3 * i + 2] - it.c[2];
     double proj = rx * rx + ry * ry;
@@ -936,21 +952,53 @@ __global__ void __launch_bounds__(32 * kL2pWarps) l2p_kernel(const __grid_consta
     proj = sqrt(proj);
     const double d = sqrt(rr);
     const double PREC = 2.220446049250313e-16;
-    const double ct = (d <= PREC) ? 0.0 : rz / d;
+    const T x = (T)((d <= PREC) ? 0.0 : rz / d);
     const C e1 = (proj <= PREC * d) ? cmk<C>(1, 0) : cmk<C>((T)(rx / proj), (T)(ry / proj));
-    const double nrm[3] = {normal[3 * i], normal[3 * i + 1], normal[3 * i + 2]};
-    double f = 0, h = 0;
-    l2p_group<T>(tb, 0, it.level, d, ct, e1, nrm, Lc, q, gq, g2, bi, p, f, h);
-    l2p_group<T>(tb, 1, it.level, d, ct, e1, nrm, Lc, q, gq, g2, bi, p, f, h);
-    for (int o = 16; o > 0; o >>= 1) {
-      f += __shfl_xor_sync(0xffffffffu, f, o);
-      h += __shfl_xor_sync(0xffffffffu, h, o);
+    const T u = -sqrt(T(1) - x * x);
+    T f = 0, h0 = 0, h1 = 0, h2 = 0;
+    T bi[kMaxNT + 4];
+    for (int g = 0; g < 2; ++g) {
+      const int lg = 2 * it.level + g;
+      bessel_in_dev<T>(tb.scale[lg], (T)(d * (double)tb.beta[g]), N2, bi);
+      const C* F = Ds + g * 4 * EQ;
+      const C* H0 = F + EQ;
+      const C* H1 = F + 2 * EQ;
+      const C* H2 = F + 3 * EQ;
+      C em = cmk<C>(1, 0);  // e^{i m phi}
+      T pmm = 1;            // P_m^m
+      for (int m = 0; m <= N2; ++m) {
+        if (m > 0) {
+          pmm = pmm * u * T(2 * m - 1);
+          em = cmul(em, e1);
+        }
+        T p0 = 0, p1 = pmm;  // P_{n-1}^m, P_n^m at n = m
+        for (int nn = m; nn <= N2; ++nn) {
+          T pn;
+          if (nn == m) {
+            pn = pmm;
+          } else if (nn == m + 1) {
+            pn = T(2 * m + 1) * x * pmm;
+          } else {
+            pn = ((T(2) * nn - T(1)) * x * p1 - T(nn + m - 1) * p0) / T(nn - m);
+          }
+          if (nn > m) {
+            p0 = p1;
+            p1 = pn;
+          }
+          const T amp = (nn == 0) ? bi[0] : bi[nn] * pn;
+          const C q = cscale(em, amp);
+          const int e = tri(nn, m);
+          if (nn <= NT + 1) f += q.x * F[e].x - q.y * F[e].y;
+          h0 += q.x * H0[e].x - q.y * H0[e].y;
+          h1 += q.x * H1[e].x - q.y * H1[e].y;
+          h2 += q.x * H2[e].x - q.y * H2[e].y;
+        }
+      }
     }
-    if (lane == 0) {
-      const double k4 = 0.07957747154594767;
-      y[i] += f * k4;
-      y[n + i] += h * k4;
-    }
+    const double k4 = 0.07957747154594767;
+    const double h = normal[3 * i] * (double)h0 + normal[3 * i + 1] * (double)h1 + normal[3 * i + 2] * (double)h2;
+    y[i] = (double)f * k4;  // far-field buffer: every patch is in exactly one leaf
+    y[n + i] = h * k4;
   }
 }
 
@@ -977,7 +1025,10 @@ struct FmmState {
   int n_p2m = 0, n_m2x = 0, n_xl = 0, n_leaf = 0;
   std::vector<int> m2m_first, m2m_count;  // per child level
   std::vector<int> l2l_first, l2l_count;  // per parent level
-  size_t smem_p2m = 0, smem_shift = 0, smem_m2x = 0, smem_xl = 0, smem_l2p = 0;
+  size_t smem_p2m = 0, smem_shift = 0, smem_m2x = 0, smem_xl = 0, smem_prep = 0, smem_eval = 0;
+  DevBuf leaf_exp;  // per leaf: [2 groups][F, H0, H1, H2][EQ]
+  DevBuf eval_items;
+  int n_eval = 0;
 };
 
 void fmm_destroy(FmmState* s) { delete s; }
@@ -1191,7 +1242,6 @@ void fmm_setup(Problem& P) {
     if ((nd.flags & TREE_LEAF) || (nd.flags & TREE_SHADOW)) continue;
     XlItem it;
     it.parent_level = nd.level;
-    it.first_entry = (int)xle.size();
     bool any_target = false;
     for (int c = 0; c < 8; ++c) {
       const int ck = nd.children[c];
@@ -1199,29 +1249,33 @@ void fmm_setup(Problem& P) {
       any_target |= it.targets[c] >= 0;
     }
     if (!any_target) continue;
-    for (const RawInteraction& r : table) {
-      if (it.targets[r.targ] < 0) continue;
-      const int nbk = nd.neighbours[r.nb];
-      if (nbk < 0 || cnt(nbk) == 0) continue;
-      const int sk = T.nodes[nbk].children[r.src];
-      if (sk < 0 || cnt(sk) == 0) continue;
-      XlEntry e;
-      e.src = sk;
-      e.dir = (signed char)r.dir;
-      e.targ = (signed char)r.targ;
-      int a, b, c;
-      switch (r.dir) {
-        case 0: case 1: a = r.dx; b = r.dy; c = r.dz; break;
-        case 2: case 3: a = r.dz; b = r.dx; c = r.dy; break;
-        default: a = -r.dz; b = r.dy; c = r.dx; break;
+    for (int pair = 0; pair < 3; ++pair) {
+      it.first_entry[pair] = (int)xle.size();
+      for (const RawInteraction& r : table) {
+        if (r.dir / 2 != pair) continue;
+        if (it.targets[r.targ] < 0) continue;
+        const int nbk = nd.neighbours[r.nb];
+        if (nbk < 0 || cnt(nbk) == 0) continue;
+        const int sk = T.nodes[nbk].children[r.src];
+        if (sk < 0 || cnt(sk) == 0) continue;
+        XlEntry e;
+        e.src = sk;
+        e.dir = (signed char)r.dir;
+        e.targ = (signed char)r.targ;
+        int a, b, c;
+        switch (r.dir) {
+          case 0: case 1: a = r.dx; b = r.dy; c = r.dz; break;
+          case 2: case 3: a = r.dz; b = r.dx; c = r.dy; break;
+          default: a = -r.dz; b = r.dy; c = r.dx; break;
+        }
+        e.a = (signed char)a;
+        e.b = (signed char)b;
+        e.c = (signed char)c;
+        e.up = (r.dir % 2 == 0) ? 1 : 0;
+        xle.push_back(e);
       }
-      e.a = (signed char)a;
-      e.b = (signed char)b;
-      e.c = (signed char)c;
-      e.up = (r.dir % 2 == 0) ? 1 : 0;
-      xle.push_back(e);
+      it.n_entries[pair] = (int)xle.size() - it.first_entry[pair];
     }
-    it.n_entries = (int)xle.size() - it.first_entry;
     xl.push_back(it);
   }
   // L2L per parent level: one item per (parent, child)
@@ -1243,12 +1297,18 @@ void fmm_setup(Problem& P) {
     S->l2l_count[lev] = (int)l2l.size() - S->l2l_first[lev];
   }
   // leaves
-  std::vector<LeafItem> leaves;
+  std::vector<LeafItem> leaves, evals;
   for (int k = 0; k < nn; ++k) {
     if (!(flags(k) & TREE_LEAF) || cnt(k) == 0) continue;
-    LeafItem it{k, T.nodes[k].level, (int)T.nodes[k].content_start, cnt(k), {0, 0, 0}};
+    LeafItem it{k, T.nodes[k].level, (int)T.nodes[k].content_start, cnt(k), (int)leaves.size(), {0, 0, 0}};
     for (int d = 0; d < 3; ++d) it.c[d] = T.nodes[k].centre[d];
     leaves.push_back(it);
+    for (int off = 0; off < it.count; off += kEvalChunk) {
+      LeafItem ev = it;
+      ev.start = it.start + off;
+      ev.count = std::min(kEvalChunk, it.count - off);
+      evals.push_back(ev);
+    }
   }
   Ctx* c = P.ctx;
   S->p2m_items = upload(c, p2m);
@@ -1264,15 +1324,20 @@ void fmm_setup(Problem& P) {
   S->l2l_children = upload(c, l2l_ch);
   S->leaf_items = upload(c, leaves);
   S->n_leaf = (int)leaves.size();
+  S->eval_items = upload(c, evals);
+  S->n_eval = (int)evals.size();
   // contents on the device (node-major patch lists)
   const int E = S->E, NT = S->nt;
   S->smem_p2m = celem * 2 * kP2mChunk * E + (S->fp64 ? 8 : 4) * kP2mChunk * kCh;
-  S->smem_shift = 4 * celem * kCh * E;
+  S->smem_shift = 4 * celem * E;
   S->smem_m2x = celem * (2 * E + 128);
-  S->smem_xl = celem * (6 * 8 * kXlCh * (size_t)S->np_max + kXlCh * 2 * 64 + 2 * kXlCh * E);
+  S->smem_xl = celem * (6 * 8 * (size_t)S->np_max + 3 * 2 * 64 + 6 * E);
+  if (S->np_max > kXlGroup) throw std::invalid_argument("FMM order too large for the X2L thread layout");
   const int EQ = (NT + 3) * (NT + 4) / 2, EG = (NT + 2) * (NT + 3) / 2;
-  S->smem_l2p = celem * (kCh * E + (size_t)kL2pWarps * (EQ + 3 * EG + 9 * E)) +
-                (S->fp64 ? 8 : 4) * (size_t)kL2pWarps * (EQ + NT + 4);
+  S->smem_prep = celem * 2 * 24 * (size_t)EQ;
+  S->smem_eval = celem * 8 * (size_t)EQ;
+  S->leaf_exp.alloc(P.ctx, celem * 8 * (size_t)EQ * std::max(1, S->n_leaf));
+  (void)EG;
   auto attr = [&](const void* fn, size_t bytes) {
     if (bytes > 48 * 1024) BP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   };
@@ -1282,16 +1347,18 @@ void fmm_setup(Problem& P) {
     attr((const void*)l2l_kernel<double>, S->smem_shift);
     attr((const void*)m2x_kernel<double>, S->smem_m2x);
     attr((const void*)x2l_kernel<double>, S->smem_xl);
-    attr((const void*)l2p_kernel<double>, S->smem_l2p);
+    attr((const void*)l2p_prep_kernel<double>, S->smem_prep);
+    attr((const void*)l2p_eval_kernel<double>, S->smem_eval);
   } else {
     attr((const void*)p2m_kernel<float>, S->smem_p2m);
     attr((const void*)m2m_kernel<float>, S->smem_shift);
     attr((const void*)l2l_kernel<float>, S->smem_shift);
     attr((const void*)m2x_kernel<float>, S->smem_m2x);
     attr((const void*)x2l_kernel<float>, S->smem_xl);
-    attr((const void*)l2p_kernel<float>, S->smem_l2p);
+    attr((const void*)l2p_prep_kernel<float>, S->smem_prep);
+    attr((const void*)l2p_eval_kernel<float>, S->smem_eval);
   }
-  if (S->smem_xl > 227 * 1024 || S->smem_l2p > 227 * 1024)
+  if (S->smem_xl > 227 * 1024 || S->smem_prep > 227 * 1024)
     throw std::invalid_argument("FMM order too large for the shared-memory layout");
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
@@ -1299,9 +1366,9 @@ void fmm_setup(Problem& P) {
 }
 
 template <typename T>
-static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* x, double* y, StageTimes* st) {
+static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* x, double* y, StageTimes* st,
+                    cudaStream_t s) {
   using C = typename C2T<T>::type;
-  cudaStream_t s = P.ctx->stream;
   C* M = S.M.as<C>();
   C* Lx = S.L.as<C>();
   C* W = S.W.as<C>();
@@ -1324,7 +1391,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   int l_m2m = 0;
   for (int lev = S.nlev - 1; lev >= 1; --lev) {
     if (!S.m2m_count[lev]) continue;
-    m2m_kernel<T><<<S.m2m_count[lev], 256, S.smem_shift, s>>>(
+    m2m_kernel<T><<<S.m2m_count[lev] * kCh, 64, S.smem_shift, s>>>(
         tb, S.m2m_items.as<ShiftItem>() + S.m2m_first[lev], S.m2m_children.as<ShiftChild>(), lev, M);
     BP_LAUNCH_CHECK();
     ++l_m2m;
@@ -1335,7 +1402,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   BP_LAUNCH_CHECK();
   end(1);
   begin(4);
-  x2l_kernel<T><<<S.n_xl * (kCh / kXlCh), kXlThreads, S.smem_xl, s>>>(tb, S.xl_items.as<XlItem>(),
+  x2l_kernel<T><<<S.n_xl * kCh, kXlThreads, S.smem_xl, s>>>(tb, S.xl_items.as<XlItem>(),
                                                                      S.xl_entries.as<XlEntry>(), W, Lx);
   BP_LAUNCH_CHECK();
   end(1);
@@ -1343,27 +1410,29 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   int l_l2l = 0;
   for (int lev = 0; lev < S.nlev - 1; ++lev) {
     if (!S.l2l_count[lev]) continue;
-    l2l_kernel<T><<<S.l2l_count[lev], 256, S.smem_shift, s>>>(
+    l2l_kernel<T><<<S.l2l_count[lev] * kCh, 64, S.smem_shift, s>>>(
         tb, S.l2l_items.as<ShiftItem>() + S.l2l_first[lev], S.l2l_children.as<ShiftChild>(), lev, Lx);
     BP_LAUNCH_CHECK();
     ++l_l2l;
   }
   end(l_l2l);
   begin(7);
-  l2p_kernel<T><<<S.n_leaf, 32 * kL2pWarps, S.smem_l2p, s>>>(tb, S.leaf_items.as<LeafItem>(), contents,
-                                                             P.d_centroid.as<double>(), P.d_normal.as<double>(), Lx,
-                                                             P.n, y);
+  l2p_prep_kernel<T><<<S.n_leaf, 64, S.smem_prep, s>>>(tb, S.leaf_items.as<LeafItem>(), Lx, S.leaf_exp.as<C>());
   BP_LAUNCH_CHECK();
-  end(1);
+  l2p_eval_kernel<T><<<S.n_eval, kEvalChunk, S.smem_eval, s>>>(tb, S.eval_items.as<LeafItem>(), contents,
+                                                        P.d_centroid.as<double>(), P.d_normal.as<double>(),
+                                                        S.leaf_exp.as<C>(), P.n, y);
+  BP_LAUNCH_CHECK();
+  end(2);
 }
 
-void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st) {
+void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st, cudaStream_t stream) {
   FmmState* S = P.fmm.get();
   if (!S) return;
   if (S->fp64)
-    run_fmm<double>(P, *S, S->tb_d, x_dev, y_dev, st);
+    run_fmm<double>(P, *S, S->tb_d, x_dev, y_dev, st, stream);
   else
-    run_fmm<float>(P, *S, S->tb_f, x_dev, y_dev, st);
+    run_fmm<float>(P, *S, S->tb_f, x_dev, y_dev, st, stream);
 }
 
 }  // namespace bp

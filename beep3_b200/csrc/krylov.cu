@@ -142,11 +142,99 @@ inline int grid_for(int64_t len) {
 
 }  // namespace
 
-void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st) {
-  if (st) st->begin(0, P.ctx->stream);
-  nf_apply(P, x_dev, y_dev);  // writes every y entry
+__global__ void add_inplace(double* __restrict__ y, const double* __restrict__ a, int64_t len) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += a[i];
+}
+
+void matvec_setup(Problem& P) {
+  Ctx* c = P.ctx;
+  const size_t bytes = sizeof(double) * 2 * (size_t)P.n;
+  P.d_yfar.alloc(c, bytes);
+  P.d_gx.alloc(c, bytes);
+  P.d_gy.alloc(c, bytes);
+  BP_CUDA(cudaStreamCreateWithFlags(&P.side, cudaStreamNonBlocking));
+  BP_CUDA(cudaEventCreateWithFlags(&P.ev_fork, cudaEventDisableTiming));
+  BP_CUDA(cudaEventCreateWithFlags(&P.ev_join, cudaEventDisableTiming));
+}
+
+// One matvec as kernel launches: the near field on `main` (writes y), the
+// FMM on `side` into the far-field buffer, joined and added on `main`.  With
+// side == main everything is serial (the profiling path).
+static void matvec_launches(Problem& P, const double* x, double* y, cudaStream_t main, cudaStream_t side,
+                            StageTimes* st) {
+  const bool far = fmm_active(P);
+  const int64_t len = 2 * (int64_t)P.n;
+  if (far && side != main) {
+    BP_CUDA(cudaEventRecord(P.ev_fork, main));
+    BP_CUDA(cudaStreamWaitEvent(side, P.ev_fork, 0));
+  }
+  if (st) st->begin(0, main);
+  nf_apply(P, x, y, main);  // writes every y entry
   if (st) st->end(P.nf.n_items > 0 ? 1 : 0);
-  if (fmm_active(P)) fmm_apply(P, x_dev, y_dev, st);  // adds the far field
+  if (!far) return;
+  fmm_apply(P, x, P.d_yfar.as<double>(), st, side);  // assigns every far-field entry
+  if (side != main) {
+    BP_CUDA(cudaEventRecord(P.ev_join, side));
+    BP_CUDA(cudaStreamWaitEvent(main, P.ev_join, 0));
+  }
+  if (st) st->begin(0, main);
+  add_inplace<<<grid_for(len), kThreads, 0, main>>>(y, P.d_yfar.as<double>(), len);
+  BP_LAUNCH_CHECK();
+  if (st) st->end(1);
+}
+
+// Captures matvec_launches(d_gx -> d_gy) as a CUDA graph on first use.
+static bool ensure_graph(Problem& P) {
+  if (P.graph) return true;
+  if (P.graph_failed) return false;
+  cudaStream_t s = P.ctx->stream;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    P.graph_failed = true;
+    return false;
+  }
+  bool ok = true;
+  try {
+    matvec_launches(P, P.d_gx.as<double>(), P.d_gy.as<double>(), s, P.side, nullptr);
+  } catch (const CudaError&) {
+    ok = false;
+  }
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (!ok || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    P.graph_failed = true;
+    return false;
+  }
+  e = cudaGraphInstantiate(&P.graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    P.graph = nullptr;
+    P.graph_failed = true;
+    return false;
+  }
+  return true;
+}
+
+void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st) {
+  cudaStream_t s = P.ctx->stream;
+  if (st) {  // profiling: serial launches with per-stage events
+    matvec_launches(P, x_dev, y_dev, s, s, st);
+    return;
+  }
+  if (ensure_graph(P)) {
+    const size_t bytes = sizeof(double) * 2 * (size_t)P.n;
+    if (x_dev != P.d_gx.as<double>())
+      BP_CUDA(cudaMemcpyAsync(P.d_gx.get(), x_dev, bytes, cudaMemcpyDeviceToDevice, s));
+    BP_CUDA(cudaGraphLaunch(P.graph, s));
+    if (y_dev != P.d_gy.as<double>())
+      BP_CUDA(cudaMemcpyAsync(y_dev, P.d_gy.get(), bytes, cudaMemcpyDeviceToDevice, s));
+    return;
+  }
+  matvec_launches(P, x_dev, y_dev, s, P.side, nullptr);
 }
 
 int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,

@@ -435,7 +435,14 @@ void nf_assemble(Problem& P) {
     }
     BP_LAUNCH_CHECK();
   }
-  // apply work items
+  // apply work items; the apply kernel's shared memory holds the x values of
+  // a leaf's columns
+  const size_t apply_smem = 2 * elem * (size_t)nf.max_cols;
+  if (apply_smem > 227 * 1024) throw std::invalid_argument("neighbourhood too large for the near-field apply");
+  if (P.fp64)
+    BP_CUDA(cudaFuncSetAttribute(apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+  else
+    BP_CUDA(cudaFuncSetAttribute(apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
   nf.h_items = make_items(P, kApplyRows);
   nf.items = upload(ctx, nf.h_items);
   nf.n_items = (int)nf.h_items.size();
@@ -443,24 +450,21 @@ void nf_assemble(Problem& P) {
   P.assemble_ms = ms_since(t0);
 }
 
-void nf_apply(Problem& P, const double* x_dev, double* y_dev) {
-  Ctx* ctx = P.ctx;
+void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t stream) {
   NearField& nf = P.nf;
   if (nf.n_items == 0) return;
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
   const size_t smem = 2 * elem * (size_t)nf.max_cols;
   if (P.fp64) {
-    if (smem > 48 * 1024)
-      BP_CUDA(cudaFuncSetAttribute(apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    apply_kernel<double><<<nf.n_items, kApplyThreads, smem, ctx->stream>>>(
+    apply_kernel<double><<<nf.n_items, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
-        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev, y_dev);
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev,
+        y_dev);
   } else {
-    if (smem > 48 * 1024)
-      BP_CUDA(cudaFuncSetAttribute(apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    apply_kernel<float><<<nf.n_items, kApplyThreads, smem, ctx->stream>>>(
+    apply_kernel<float><<<nf.n_items, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
-        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev, y_dev);
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev,
+        y_dev);
   }
   BP_LAUNCH_CHECK();
 }
