@@ -206,7 +206,7 @@ struct Problem {
 };
 
 // Optional per-stage timing of a matvec with CUDA events on the stream.
-constexpr int kStages = 8;  // near, P2M, M2M, M->X, X->X, X->L, L2L, L2P
+constexpr int kStages = 8;  // near(+add), P2M, M2M, M->X, X->L (translations + conversion), L2P prep, L2L, L2P eval
 struct StageTimes {
   struct Rec {
     int stage;

@@ -1416,14 +1416,16 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
     ++l_l2l;
   }
   end(l_l2l);
-  begin(7);
+  begin(5);
   l2p_prep_kernel<T><<<S.n_leaf, 64, S.smem_prep, s>>>(tb, S.leaf_items.as<LeafItem>(), Lx, S.leaf_exp.as<C>());
   BP_LAUNCH_CHECK();
+  end(1);
+  begin(7);
   l2p_eval_kernel<T><<<S.n_eval, kEvalChunk, S.smem_eval, s>>>(tb, S.eval_items.as<LeafItem>(), contents,
                                                         P.d_centroid.as<double>(), P.d_normal.as<double>(),
                                                         S.leaf_exp.as<C>(), P.n, y);
   BP_LAUNCH_CHECK();
-  end(2);
+  end(1);
 }
 
 void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st, cudaStream_t stream) {

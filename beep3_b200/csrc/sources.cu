@@ -122,3 +122,4 @@ void energy_coefficients_device(Problem& P, int first, int count, const double* 
 }
 
 }  // namespace bp
+

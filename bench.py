@@ -367,7 +367,7 @@ def _run_ours(args, world, rank, local, dist):
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                      "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": near_ms},
         "stage_ms": {k: round(float(v), 5) for k, v in zip(
-            ["near", "p2m", "m2m", "m2x", "x2x", "x2l", "l2l", "l2p"], ms)},
+            ["near+add", "p2m", "m2m", "m2x", "x2l", "l2p_prep", "l2l", "l2p_eval"], ms)},
         "fp64_matvec_per_s": value64,
         "mixed_over_fp64": value / value64,
         "solves_per_s": world * 1e3 / statistics.median(solve_ms),

@@ -166,11 +166,13 @@ int32_t bp_matvec(bp_problem p, const double* x, double* y);
 /* Same on device arrays, stream-ordered, no synchronisation. */
 int32_t bp_matvec_device(bp_problem p, const double* x_dev, double* y_dev);
 /* Per-stage device time of `reps` matvecs on device arrays, averaged, in ms,
- * measured with CUDA events on the context stream.  stage_ms[0] = near field,
+ * measured with CUDA events on the context stream, all stages serialised on
+ * that stream.  stage_ms[0] = near field (+ the final near/far add),
  * [1] = P2M, [2] = M2M, [3] = multipole->exponential, [4] = exponential
- * translations, [5] = exponential->local, [6] = L2L, [7] = L2P;
- * *n_stages = 8.  stage_launches (may be NULL) receives kernel launches per
- * stage per matvec. */
+ * translations fused with exponential->local, [5] = L2P per-leaf
+ * preparation, [6] = L2L, [7] = L2P evaluation; *n_stages = 8.
+ * stage_launches (may be NULL) receives kernel launches per stage per
+ * matvec. */
 int32_t bp_matvec_profile(bp_problem p, const double* x_dev, double* y_dev, int32_t reps, double* stage_ms,
                           int32_t* stage_launches, int32_t* n_stages);
 
