@@ -14,6 +14,8 @@
 // (Mesh::renormalise_energy_precalcs, src/bem/mesh.cpp:905-925).
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -122,4 +124,76 @@ void energy_coefficients_device(Problem& P, int first, int count, const double* 
 }
 
 }  // namespace bp
+
+// ---------------------------------------------------------------------------
+// Right-hand side without any device allocation.
+//
+// For callers that cannot allocate device memory themselves: code running
+// inside a host application whose allocator owns the whole GPU (a pooled
+// or pre-reserved heap), code that must not call cudaMalloc while another
+// thread may be capturing a CUDA graph, or embedded users given fixed
+// device buffers.  The per-point scratch of the right-hand-side kernels
+// lives in a fixed file-scope device array instead of a cudaMalloc'd
+// buffer; the caller passes inputs and outputs as device pointers.
+//
+// The array holds kNoAllocMaxPoints points (2 doubles each, 16 MiB) on every
+// GPU that loads this library, until the process exits.  Every call shares
+// it: calls that overlap on the GPU (different streams, or different host
+// threads on the same device) race on it and must be serialised by the
+// caller.  Each call writes every scratch entry it later reads, so nothing
+// has to start at zero.
+namespace bp {
+namespace {
+
+constexpr int kNoAllocMaxPoints = 1 << 20;
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxPoints];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array for the current device.  Host code
+// cannot use the symbol itself as a device pointer, so the address is
+// looked up once per device, with that device current, and cached.
+double* noalloc_scratch_for_current_device() {
+  int dev = -1;
+  BP_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) throw std::invalid_argument("device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    BP_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
+}  // namespace
+}  // namespace bp
+
+extern "C" BP_API int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_offsets_dev,
+                                         const double* qual_points_soa_dev, int32_t n_qual_points,
+                                         const double* charges_xyzq_dev, int32_t n_charges, double eps_solvent,
+                                         double* rhs_dev, void* cuda_stream) {
+  using namespace bp;
+  return guarded_engine([&]() -> int32_t {
+    if (n_patches <= 0 || n_qual_points <= 0 || !qual_offsets_dev || !qual_points_soa_dev || !rhs_dev ||
+        n_charges < 0 || (n_charges > 0 && !charges_xyzq_dev) || !(eps_solvent > 0))
+      return fail(BP_ERR_INVALID, "bp_rhs_noalloc: bad argument");
+    if (n_qual_points > kNoAllocMaxPoints)
+      return fail(BP_ERR_INVALID, "bp_rhs_noalloc: " + std::to_string(n_qual_points) +
+                                      " qualocation points exceed the fixed scratch of " +
+                                      std::to_string(kNoAllocMaxPoints) + " points");
+    double* scratch = noalloc_scratch_for_current_device();
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    const double scale = kOneOver4Pi / eps_solvent;
+    point_potential_kernel<<<(n_qual_points + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+        qual_points_soa_dev, n_qual_points, 0, n_qual_points, charges_xyzq_dev, n_charges, scale, scratch);
+    BP_LAUNCH_CHECK();
+    sum_points_kernel<<<(n_patches + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+        qual_offsets_dev, 0, n_patches, 0, scratch, rhs_dev, rhs_dev + n_patches);
+    BP_LAUNCH_CHECK();
+    return BP_OK;
+  });
+}
 

@@ -192,6 +192,23 @@ int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_dev, doub
  * weighted and scaled by 1/(4 pi eps_solvent).  charges_xyzq: [n][4]. */
 int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charges, double eps_solvent, double* rhs);
 
+/* Right-hand side without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- host applications
+ * whose own allocator owns the device memory, or code that must not
+ * allocate while another thread captures a CUDA graph: every argument is a
+ * caller-owned device pointer (qualocation offsets [n_patches+1], points as
+ * seven arrays x y z nx ny nz w of n_qual_points doubles each, charges
+ * [n][4], rhs [2 n_patches]) and the kernels' per-point scratch is a fixed
+ * 16 MiB array in the library, held on every GPU that loads it until exit.
+ * At most 1048576 qualocation points per call (larger calls return
+ * BP_ERR_INVALID).  The first call on a device looks the array up (do it
+ * before any stream capture); calls that overlap on the GPU share the array
+ * and race, so the caller serialises them.  Ordered on cuda_stream (NULL =
+ * the legacy default stream), no host synchronisation. */
+int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_offsets_dev, const double* qual_points_soa_dev,
+                       int32_t n_qual_points, const double* charges_xyzq_dev, int32_t n_charges, double eps_solvent,
+                       double* rhs_dev, void* cuda_stream);
+
 /* Energy coefficients of patches [first, first+count) from the charges of
  * their own mesh (Mesh::init_energy_precalcs + renormalise_energy_precalcs,
  * src/bem/mesh.cpp:730-925): Coulomb potential and normal field at the
