@@ -32,6 +32,13 @@ struct BudgetError : std::runtime_error {
 
 #define BP_LAUNCH_CHECK() BP_CUDA(cudaGetLastError())
 
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`.  The attribute is process-wide per (device, kernel) while
+// problems are created and launched from several threads at once, so the
+// limit only ever grows: a problem with a smaller neighbourhood must not
+// lower it under another problem's launch.
+void ensure_dynamic_smem(const void* kernel, size_t bytes);
+
 template <typename F>
 int32_t guarded_engine(F&& f) {
   try {

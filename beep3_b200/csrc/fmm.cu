@@ -1014,6 +1014,115 @@ void to_dev_c(std::vector<C>& out, const std::vector<S>& in) {
 }  // namespace
 
 // ---------------------------------------------------------------- host state
+// ---------------------------------------------------------------- operator form
+// The M2M and L2L shifts of one channel are R-linear maps of the 2E reals of
+// an expansion, fixed per (level, screening group, child octant); the L2P
+// preparation is an R-linear map from the 12 x 2E reals of a leaf's locals to
+// its 8 x 2EQ derivative-expansion reals, fixed per (level).  They are
+// tabulated once per problem by applying the kernels above to unit vectors
+// (same arithmetic, so the same operators), then applied as dense (shifts)
+// or sparse (preparation) matrix-vector products: no shared-memory phases
+// and no serial chains per output.
+template <typename T>
+__global__ void __launch_bounds__(64) shift_basis_kernel(const __grid_constant__ Tables<T> tb, int nlev,
+                                                         T* __restrict__ ops) {
+  using C = typename C2T<T>::type;
+  extern __shared__ unsigned char smem_raw[];
+  const int E = tb.E, R = 2 * E;
+  C* w1 = reinterpret_cast<C*>(smem_raw);
+  C* w2 = w1 + E;
+  C* acc = w2 + E;
+  C* in = acc + E;
+  const int k = blockIdx.x % R;
+  const int op = blockIdx.x / R;  // ((kind * nlev + level) * 2 + group) * 8 + octant-1
+  const int oct = op % 8 + 1, g = (op / 8) % 2, level = (op / 16) % nlev, kind = op / (16 * nlev);
+  for (int o = threadIdx.x; o < E; o += blockDim.x) {
+    in[o] = cmk<C>(2 * o == k ? T(1) : T(0), 2 * o + 1 == k ? T(1) : T(0));
+    acc[o] = cmk<C>(0, 0);
+  }
+  __syncthreads();
+  const bool multipole = kind == 0;
+  const T* rd = multipole ? tb.R(oct > 4 ? ROT_MSQ3 : ROT_SQ3) : tb.R(oct > 4 ? ROT_SQ3 : ROT_MSQ3);
+  shift_block<T>(tb, oct, multipole, level, in, w1, w2, acc, rd, g ? 8 : 0, 1);
+  T* col = ops + ((size_t)op * R + k) * R;  // column k: [op][k][r]
+  for (int o = threadIdx.x; o < E; o += blockDim.x) {
+    col[2 * o] = acc[o].x;
+    col[2 * o + 1] = acc[o].y;
+  }
+}
+
+struct DenseShift {
+  int target, first_src, n_src;  // sources listed in DenseSrc
+};
+struct DenseSrc {
+  int node, op;  // source expansion node and operator index
+};
+
+// y[target][ch] (=, or += for L2L) sum over sources of A_op x[source][ch];
+// one block per (target, channel), thread per output real
+template <typename T>
+__global__ void __launch_bounds__(128) dense_shift_kernel(int E, const DenseShift* __restrict__ items,
+                                                          const DenseSrc* __restrict__ srcs,
+                                                          const T* __restrict__ ops, const T* __restrict__ X,
+                                                          T* __restrict__ Y, int accumulate) {
+  extern __shared__ unsigned char smem_raw[];
+  const int R = 2 * E;
+  T* xs = reinterpret_cast<T*>(smem_raw);  // [8][R]
+  const DenseShift it = items[blockIdx.x / kCh];
+  const int ch = blockIdx.x % kCh;
+  for (int o = threadIdx.x; o < it.n_src * R; o += blockDim.x) {
+    const DenseSrc sc = srcs[it.first_src + o / R];
+    xs[o] = X[((size_t)sc.node * kCh + ch) * R + o % R];
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    T acc = accumulate ? Y[((size_t)it.target * kCh + ch) * R + r] : T(0);
+    for (int c = 0; c < it.n_src; ++c) {
+      const T* A = ops + (size_t)(srcs[it.first_src + c].op + (ch >= 8 ? 8 : 0)) * R * R;  // group offset
+      const T* x = xs + c * R;
+      for (int k = 0; k < R; ++k) acc += A[(size_t)k * R + r] * x[k];
+    }
+    Y[((size_t)it.target * kCh + ch) * R + r] = acc;
+  }
+}
+
+// Unit-vector inputs for tabulating the L2P preparation: item b of level l
+// has local expansions zero except real component k of channel c
+// (b = c * 2E + k).
+template <typename T>
+__global__ void prep_basis_inputs(int E, int nb, typename C2T<T>::type* __restrict__ Lb) {
+  const int b = blockIdx.x;
+  const int R = 2 * E;
+  const int c = b / R, k = b % R;
+  for (int o = threadIdx.x; o < kCh * E; o += blockDim.x) {
+    const int ch = o / E, e = o % E;
+    T re = (ch == c && 2 * e == k) ? T(1) : T(0);
+    T im = (ch == c && 2 * e + 1 == k) ? T(1) : T(0);
+    Lb[(size_t)b * kCh * E + o] = cmk<typename C2T<T>::type>(re, im);
+  }
+  (void)nb;
+}
+
+// D[leaf][row] = sum over the row's nonzeros of val * Lreal[leaf][col]
+template <typename T>
+__global__ void __launch_bounds__(256) prep_csr_kernel(int E, int EQ, const LeafItem* __restrict__ items,
+                                                       const int* __restrict__ rowptr, const int* __restrict__ cols,
+                                                       const T* __restrict__ vals, const T* __restrict__ Lr,
+                                                       T* __restrict__ D) {
+  extern __shared__ unsigned char smem_raw[];
+  const int R = 2 * E, rows = 8 * 2 * EQ;
+  T* x = reinterpret_cast<T*>(smem_raw);  // [12 * R]
+  const LeafItem it = items[blockIdx.x];
+  for (int o = threadIdx.x; o < kCh * R; o += blockDim.x) x[o] = Lr[(size_t)it.node * kCh * R + o];
+  __syncthreads();
+  const int* rp = rowptr + (size_t)it.level * (rows + 1);
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    T acc = 0;
+    for (int z = rp[r]; z < rp[r + 1]; ++z) acc += vals[z] * x[cols[z]];
+    D[(size_t)blockIdx.x * rows + r] = acc;
+  }
+}
+
 struct FmmState {
   int nt = 9, E = 55, nlev = 0, np_max = 0, nl = 0;
   bool fp64 = true;
@@ -1029,6 +1138,13 @@ struct FmmState {
   DevBuf leaf_exp;  // per leaf: [2 groups][F, H0, H1, H2][EQ]
   DevBuf eval_items;
   int n_eval = 0;
+  // operator form of M2M / L2L and of the L2P preparation
+  DevBuf shift_ops;                       // [op][k][r], op = ((kind*nlev + level)*2 + group)*8 + octant-1
+  DevBuf m2m_dense, m2m_src, l2l_dense, l2l_src;
+  std::vector<int> m2m_dfirst, m2m_dcount, l2l_dfirst, l2l_dcount;
+  DevBuf prep_rowptr, prep_cols, prep_vals;
+  size_t smem_dense = 0, smem_csr = 0;
+  bool use_operators = true;
 };
 
 void fmm_destroy(FmmState* s) { delete s; }
@@ -1176,6 +1292,103 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
 }
 
 }  // namespace
+
+
+template <typename T>
+static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const std::vector<ShiftItem>& m2m,
+                            const std::vector<ShiftChild>& m2m_ch, const std::vector<ShiftItem>& l2l,
+                            const std::vector<ShiftChild>& l2l_ch, const std::vector<LeafItem>& leaves) {
+  using C = typename C2T<T>::type;
+  Ctx* c = P.ctx;
+  cudaStream_t st = c->stream;
+  const int E = S.E, R = 2 * E, nlev = S.nlev, NT = S.nt;
+  const int EQ = (NT + 3) * (NT + 4) / 2;
+  // shifts: kind 0 = M2M (level = child level), kind 1 = L2L (level = parent level)
+  const int n_ops = 2 * nlev * 2 * 8;
+  S.shift_ops.alloc(c, sizeof(T) * (size_t)n_ops * R * R);
+  shift_basis_kernel<T><<<n_ops * R, 64, S.smem_shift, st>>>(tb, nlev, S.shift_ops.as<T>());
+  BP_LAUNCH_CHECK();
+  auto op_base = [&](int kind, int level, int oct) { return ((kind * nlev + level) * 2) * 8 + oct - 1; };
+  std::vector<DenseShift> md, ld;
+  std::vector<DenseSrc> ms, ls;
+  S.m2m_dfirst.assign(nlev, 0);
+  S.m2m_dcount.assign(nlev, 0);
+  for (int lev = nlev - 1; lev >= 1; --lev) {
+    S.m2m_dfirst[lev] = (int)md.size();
+    for (int q = S.m2m_first[lev]; q < S.m2m_first[lev] + S.m2m_count[lev]; ++q) {
+      const ShiftItem& it = m2m[q];
+      DenseShift d{it.parent, (int)ms.size(), it.n_children};
+      for (int k = 0; k < it.n_children; ++k) {
+        const ShiftChild& ch = m2m_ch[it.first_child + k];
+        ms.push_back({ch.node, op_base(0, lev, ch.octant)});
+      }
+      md.push_back(d);
+    }
+    S.m2m_dcount[lev] = (int)md.size() - S.m2m_dfirst[lev];
+  }
+  S.l2l_dfirst.assign(nlev, 0);
+  S.l2l_dcount.assign(nlev, 0);
+  for (int lev = 0; lev < nlev - 1; ++lev) {
+    S.l2l_dfirst[lev] = (int)ld.size();
+    for (int q = S.l2l_first[lev]; q < S.l2l_first[lev] + S.l2l_count[lev]; ++q) {
+      const ShiftItem& it = l2l[q];
+      const ShiftChild& ch = l2l_ch[it.first_child];
+      ld.push_back({ch.node, (int)ls.size(), 1});
+      ls.push_back({it.parent, op_base(1, lev, ch.octant)});
+    }
+    S.l2l_dcount[lev] = (int)ld.size() - S.l2l_dfirst[lev];
+  }
+  S.m2m_dense = upload(c, md);
+  S.m2m_src = upload(c, ms);
+  S.l2l_dense = upload(c, ld);
+  S.l2l_src = upload(c, ls);
+  S.smem_dense = sizeof(T) * 8 * (size_t)R;
+  // L2P preparation operator per level that holds leaves
+  const int nb = kCh * R, rows = 8 * 2 * EQ;
+  std::vector<int> levels_with_leaves(nlev, 0);
+  for (const LeafItem& lf : leaves) levels_with_leaves[lf.level] = 1;
+  DevBuf Lb(c, sizeof(C) * (size_t)nb * kCh * E);
+  DevBuf Db(c, sizeof(C) * (size_t)nb * 8 * EQ);
+  prep_basis_inputs<T><<<nb, 128, 0, st>>>(E, nb, Lb.as<C>());
+  BP_LAUNCH_CHECK();
+  std::vector<int> rowptr((size_t)nlev * (rows + 1), 0), cols;
+  std::vector<T> vals;
+  std::vector<T> host((size_t)nb * rows);
+  for (int lev = 0; lev < nlev; ++lev) {
+    int* rp = rowptr.data() + (size_t)lev * (rows + 1);
+    if (!levels_with_leaves[lev]) {
+      for (int r = 0; r <= rows; ++r) rp[r] = (int)vals.size();
+      continue;
+    }
+    std::vector<LeafItem> bi(nb);
+    for (int b = 0; b < nb; ++b) bi[b] = LeafItem{b, lev, 0, 0, b, {0, 0, 0}};
+    DevBuf d_bi = upload(c, bi);
+    l2p_prep_kernel<T><<<nb, 64, S.smem_prep, st>>>(tb, d_bi.as<LeafItem>(), Lb.as<C>(), Db.as<C>());
+    BP_LAUNCH_CHECK();
+    BP_CUDA(cudaMemcpyAsync(host.data(), Db.get(), sizeof(T) * host.size(), cudaMemcpyDeviceToHost, st));
+    BP_CUDA(cudaStreamSynchronize(st));
+    for (int r = 0; r < rows; ++r) {
+      rp[r] = (int)vals.size();
+      for (int b = 0; b < nb; ++b) {
+        const T v = host[(size_t)b * rows + r];
+        if (v != T(0)) {
+          cols.push_back(b);
+          vals.push_back(v);
+        }
+      }
+    }
+    rp[rows] = (int)vals.size();
+  }
+  if (vals.empty()) {
+    vals.push_back(0);
+    cols.push_back(0);
+  }
+  S.prep_rowptr = upload(c, rowptr);
+  S.prep_cols = upload(c, cols);
+  S.prep_vals = upload(c, vals);
+  S.smem_csr = sizeof(T) * (size_t)kCh * R;
+  BP_CUDA(cudaStreamSynchronize(st));
+}
 
 void fmm_setup(Problem& P) {
   auto S = new FmmState();
@@ -1339,7 +1552,7 @@ void fmm_setup(Problem& P) {
   S->leaf_exp.alloc(P.ctx, celem * 8 * (size_t)EQ * std::max(1, S->n_leaf));
   (void)EG;
   auto attr = [&](const void* fn, size_t bytes) {
-    if (bytes > 48 * 1024) BP_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    ensure_dynamic_smem(fn, bytes);
   };
   if (S->fp64) {
     attr((const void*)p2m_kernel<double>, S->smem_p2m);
@@ -1363,6 +1576,10 @@ void fmm_setup(Problem& P) {
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
   BP_CUDA(cudaStreamSynchronize(c->stream));
+  if (S->fp64)
+    build_operators<double>(P, *S, S->tb_d, m2m, m2m_ch, l2l, l2l_ch, leaves);
+  else
+    build_operators<float>(P, *S, S->tb_f, m2m, m2m_ch, l2l, l2l_ch, leaves);
 }
 
 template <typename T>
@@ -1390,9 +1607,16 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   begin(2);
   int l_m2m = 0;
   for (int lev = S.nlev - 1; lev >= 1; --lev) {
-    if (!S.m2m_count[lev]) continue;
-    m2m_kernel<T><<<S.m2m_count[lev] * kCh, 64, S.smem_shift, s>>>(
-        tb, S.m2m_items.as<ShiftItem>() + S.m2m_first[lev], S.m2m_children.as<ShiftChild>(), lev, M);
+    if (S.use_operators) {
+      if (!S.m2m_dcount[lev]) continue;
+      dense_shift_kernel<T><<<S.m2m_dcount[lev] * kCh, 128, S.smem_dense, s>>>(
+          S.E, S.m2m_dense.as<DenseShift>() + S.m2m_dfirst[lev], S.m2m_src.as<DenseSrc>(), S.shift_ops.as<T>(),
+          reinterpret_cast<const T*>(M), reinterpret_cast<T*>(M), 0);
+    } else {
+      if (!S.m2m_count[lev]) continue;
+      m2m_kernel<T><<<S.m2m_count[lev] * kCh, 64, S.smem_shift, s>>>(
+          tb, S.m2m_items.as<ShiftItem>() + S.m2m_first[lev], S.m2m_children.as<ShiftChild>(), lev, M);
+    }
     BP_LAUNCH_CHECK();
     ++l_m2m;
   }
@@ -1409,15 +1633,30 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   begin(6);
   int l_l2l = 0;
   for (int lev = 0; lev < S.nlev - 1; ++lev) {
-    if (!S.l2l_count[lev]) continue;
-    l2l_kernel<T><<<S.l2l_count[lev] * kCh, 64, S.smem_shift, s>>>(
-        tb, S.l2l_items.as<ShiftItem>() + S.l2l_first[lev], S.l2l_children.as<ShiftChild>(), lev, Lx);
+    if (S.use_operators) {
+      if (!S.l2l_dcount[lev]) continue;
+      dense_shift_kernel<T><<<S.l2l_dcount[lev] * kCh, 128, S.smem_dense, s>>>(
+          S.E, S.l2l_dense.as<DenseShift>() + S.l2l_dfirst[lev], S.l2l_src.as<DenseSrc>(), S.shift_ops.as<T>(),
+          reinterpret_cast<const T*>(Lx), reinterpret_cast<T*>(Lx), 1);
+    } else {
+      if (!S.l2l_count[lev]) continue;
+      l2l_kernel<T><<<S.l2l_count[lev] * kCh, 64, S.smem_shift, s>>>(
+          tb, S.l2l_items.as<ShiftItem>() + S.l2l_first[lev], S.l2l_children.as<ShiftChild>(), lev, Lx);
+    }
     BP_LAUNCH_CHECK();
     ++l_l2l;
   }
   end(l_l2l);
   begin(5);
-  l2p_prep_kernel<T><<<S.n_leaf, 64, S.smem_prep, s>>>(tb, S.leaf_items.as<LeafItem>(), Lx, S.leaf_exp.as<C>());
+  if (S.use_operators) {
+    const int NT = S.nt, EQ = (NT + 3) * (NT + 4) / 2;
+    prep_csr_kernel<T><<<S.n_leaf, 256, S.smem_csr, s>>>(S.E, EQ, S.leaf_items.as<LeafItem>(), S.prep_rowptr.as<int>(),
+                                                          S.prep_cols.as<int>(), S.prep_vals.as<T>(),
+                                                          reinterpret_cast<const T*>(Lx),
+                                                          reinterpret_cast<T*>(S.leaf_exp.as<C>()));
+  } else {
+    l2p_prep_kernel<T><<<S.n_leaf, 64, S.smem_prep, s>>>(tb, S.leaf_items.as<LeafItem>(), Lx, S.leaf_exp.as<C>());
+  }
   BP_LAUNCH_CHECK();
   end(1);
   begin(7);

@@ -15,6 +15,9 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "engine.h"
@@ -141,6 +144,19 @@ inline int grid_for(int64_t len) {
 }
 
 }  // namespace
+
+void ensure_dynamic_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> granted;
+  if (bytes <= 48 * 1024) return;  // the default limit
+  int dev = 0;
+  BP_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = granted[{dev, kernel}];
+  if (bytes <= cur) return;
+  BP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+}
 
 __global__ void add_inplace(double* __restrict__ y, const double* __restrict__ a, int64_t len) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)

@@ -419,14 +419,14 @@ void nf_assemble(Problem& P) {
   if (smem > 200 * 1024) throw std::invalid_argument("too many qualocation points per patch");
   if (!asm_items.empty()) {
     if (P.fp64) {
-      BP_CUDA(cudaFuncSetAttribute(assemble_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      ensure_dynamic_smem((const void*)assemble_kernel<double>, smem);
       assemble_kernel<double><<<(int)asm_items.size(), kAsmThreads, smem, ctx->stream>>>(
           d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual.as<double>(), nq,
           P.d_quad_off.as<int32_t>(), P.d_quad.as<double>(), np, P.d_eps.as<double>(), P.params.kappa,
           P.d_diag.as<double>(), nf.coef.as<double>());
     } else {
-      BP_CUDA(cudaFuncSetAttribute(assemble_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      ensure_dynamic_smem((const void*)assemble_kernel<float>, smem);
       assemble_kernel<float><<<(int)asm_items.size(), kAsmThreads, smem, ctx->stream>>>(
           d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(), nq,
@@ -440,9 +440,9 @@ void nf_assemble(Problem& P) {
   const size_t apply_smem = 2 * elem * (size_t)nf.max_cols;
   if (apply_smem > 227 * 1024) throw std::invalid_argument("neighbourhood too large for the near-field apply");
   if (P.fp64)
-    BP_CUDA(cudaFuncSetAttribute(apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+    ensure_dynamic_smem((const void*)apply_kernel<double>, apply_smem);
   else
-    BP_CUDA(cudaFuncSetAttribute(apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+    ensure_dynamic_smem((const void*)apply_kernel<float>, apply_smem);
   nf.h_items = make_items(P, kApplyRows);
   nf.items = upload(ctx, nf.h_items);
   nf.n_items = (int)nf.h_items.size();
