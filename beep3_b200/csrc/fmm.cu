@@ -113,6 +113,7 @@ struct Tables {
   const T* zs;
   const T* mpshift;      // [lg][(nt+1)^3]
   const T* lcshift;
+  const C* tcomb;        // [lg][686 combos][np_max] plane-wave translation factors
   __device__ const T* R(int which) const { return rot + (size_t)which * (nt + 1) * (nt + 1) * (2 * nt + 1); }
   __device__ T rd(const T* r, int l, int mp, int m) const {
     return r[((size_t)l * (nt + 1) + mp) * (2 * nt + 1) + m + nt];
@@ -205,89 +206,107 @@ __device__ __forceinline__ void patch_charges(const double* area, const double* 
 }
 
 // ---------------------------------------------------------------- P2M
+// The multipole basis of a patch in its childless node (yformmp without the
+// charge: i_l(beta r) P_l^m(cos theta) e^{-i m phi} * scale factors, per
+// screening group) depends on geometry alone, so it is tabulated once per
+// problem (p2m_basis_kernel) and every matvec only contracts it with the
+// patches' 12 charges (p2m_kernel).
 struct P2mItem {
   int node, level, start, count;
+  int pos;  // first row of the node's patches in the basis table
   double c[3];
 };
 
 constexpr int kP2mChunk = 32;
 
+// basis[(pos + p) * 2 + g][e] for patch p of the item, group g
 template <typename T>
-__global__ void __launch_bounds__(256) p2m_kernel(const __grid_constant__ Tables<T> tb, const P2mItem* __restrict__ items,
+__global__ void __launch_bounds__(64) p2m_basis_kernel(const __grid_constant__ Tables<T> tb,
+                                                       const P2mItem* __restrict__ items,
+                                                       const int32_t* __restrict__ contents,
+                                                       const double* __restrict__ centroid,
+                                                       typename C2T<T>::type* __restrict__ basis) {
+  using C = typename C2T<T>::type;
+  const int E = tb.E, NT = tb.nt;
+  const P2mItem it = items[blockIdx.x];
+  for (int t = threadIdx.x; t < 2 * it.count; t += blockDim.x) {
+    const int pl = t >> 1, g = t & 1;
+    const int i = contents[it.start + pl];
+    const double rx = centroid[3 * i] - it.c[0], ry = centroid[3 * i + 1] - it.c[1], rz = centroid[3 * i + 2] - it.c[2];
+    double proj = rx * rx + ry * ry;
+    const double rr = proj + rz * rz;
+    proj = sqrt(proj);
+    const double d = sqrt(rr);
+    const double PREC = 2.220446049250313e-16;
+    const T ct = (T)((d <= PREC) ? 1.0 : rz / d);
+    C e1 = (proj <= PREC * d) ? cmk<C>(1, 0) : cmk<C>((T)(rx / proj), (T)(-ry / proj));
+    const int lg = 2 * it.level + g;
+    T bi[kMaxNT + 2];
+    bessel_in_dev<T>(tb.scale[lg], (T)(d * (double)tb.beta[g]), NT, bi);
+    T p[(kMaxNT + 1) * (kMaxNT + 2) / 2];
+    legendre_dev<T>(NT, ct, p);
+    C* bs = basis + ((size_t)(it.pos + pl) * 2 + g) * E;
+    bs[0] = cmk<C>(bi[0], 0);
+    C ephi = e1;  // e^{-i m phi} for m = 1
+    for (int m = 1; m <= NT; ++m) {
+      for (int l = m; l <= NT; ++l) {
+        const T cp = bi[l] * tb.sfac[tri(l, m)] * p[tri(l, m)];
+        bs[tri(l, m)] = cscale(ephi, cp);
+      }
+      ephi = cmul(ephi, e1);
+    }
+    for (int l = 1; l <= NT; ++l) bs[tri(l, 0)] = cmk<C>(p[tri(l, 0)] * bi[l] * tb.sfac[tri(l, 0)], 0);
+  }
+}
+
+// One block per childless node; thread (g, e) accumulates coefficient e of
+// the group's channels (8 for group 0, 4 for group 1) over the node's
+// patches, charges staged per chunk in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(128) p2m_kernel(const P2mItem* __restrict__ items, int E,
                                                   const int32_t* __restrict__ contents,
-                                                  const double* __restrict__ centroid, const double* __restrict__ area,
+                                                  const double* __restrict__ area,
                                                   const double* __restrict__ normal, const double* __restrict__ eps,
                                                   const double* __restrict__ x, int n,
+                                                  const typename C2T<T>::type* __restrict__ basis,
                                                   typename C2T<T>::type* __restrict__ M) {
   using C = typename C2T<T>::type;
-  extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E, NT = tb.nt;
-  C* basis = reinterpret_cast<C*>(smem_raw);                       // [chunk][2][E]
-  T* q = reinterpret_cast<T*>(basis + 2 * kP2mChunk * E);          // [chunk][12]
+  __shared__ T q[kP2mChunk][kCh];
   const P2mItem it = items[blockIdx.x];
-  C acc[(kCh * ((kMaxNT + 1) * (kMaxNT + 2) / 2) + 255) / 256];
-  const int nout = kCh * E;
-  for (int k = 0; k < (nout + 255) / 256; ++k) acc[k] = cmk<C>(0, 0);
+  const int g = threadIdx.x >= 64 ? 1 : 0, e = threadIdx.x - 64 * g;
+  const int c0 = g ? 8 : 0, nc = g ? 4 : 8;
+  C acc[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) acc[c] = cmk<C>(0, 0);
   for (int base = 0; base < it.count; base += kP2mChunk) {
     const int cnt = min(kP2mChunk, it.count - base);
-    const int t = threadIdx.x;
-    if (t < 2 * cnt) {
-      const int pl = t >> 1, g = t & 1;
-      const int i = contents[it.start + base + pl];
-      const double rx = centroid[3 * i] - it.c[0], ry = centroid[3 * i + 1] - it.c[1],
-                   rz = centroid[3 * i + 2] - it.c[2];
-      double proj = rx * rx + ry * ry;
-      const double rr = proj + rz * rz;
-      proj = sqrt(proj);
-      const double d = sqrt(rr);
-      const double PREC = 2.220446049250313e-16;
-      const T ct = (T)((d <= PREC) ? 1.0 : rz / d);
-      C e1 = (proj <= PREC * d) ? cmk<C>(1, 0) : cmk<C>((T)(rx / proj), (T)(-ry / proj));
-      const int lg = 2 * it.level + g;
-      T bi[kMaxNT + 2];
-      bessel_in_dev<T>(tb.scale[lg], (T)(d * (double)tb.beta[g]), NT, bi);
-      T p[(kMaxNT + 1) * (kMaxNT + 2) / 2];
-      legendre_dev<T>(NT, ct, p);
-      C* bs = basis + ((size_t)pl * 2 + g) * E;
-      bs[0] = cmk<C>(bi[0], 0);
-      C ephi = e1;  // e^{-i m phi} for m = 1
-      for (int m = 1; m <= NT; ++m) {
-        for (int l = m; l <= NT; ++l) {
-          const T cp = bi[l] * tb.sfac[tri(l, m)] * p[tri(l, m)];
-          bs[tri(l, m)] = cscale(ephi, cp);
-        }
-        ephi = cmul(ephi, e1);
-      }
-      for (int l = 1; l <= NT; ++l) bs[tri(l, 0)] = cmk<C>(p[tri(l, 0)] * bi[l] * tb.sfac[tri(l, 0)], 0);
-    } else if (t >= 64 && t < 64 + cnt) {
-      const int pl = t - 64;
-      const int i = contents[it.start + base + pl];
+    __syncthreads();
+    if (threadIdx.x < cnt) {
       T qq[kCh];
-      patch_charges<T>(area, normal, eps, x, n, i, qq);
-      for (int c = 0; c < kCh; ++c) q[pl * kCh + c] = qq[c];
+      patch_charges<T>(area, normal, eps, x, n, contents[it.start + base + threadIdx.x], qq);
+#pragma unroll
+      for (int c = 0; c < kCh; ++c) q[threadIdx.x][c] = qq[c];
     }
     __syncthreads();
-    for (int k = 0; k < (nout + 255) / 256; ++k) {
-      const int o = threadIdx.x + 256 * k;
-      if (o < nout) {
-        const int ch = o / E, e = o - ch * E;
-        const int g = ch >= 8 ? 1 : 0;
-        C a = acc[k];
-        for (int pl = 0; pl < cnt; ++pl) {
-          const C b = basis[((size_t)pl * 2 + g) * E + e];
-          const T qc = q[pl * kCh + ch];
-          a.x += b.x * qc;
-          a.y += b.y * qc;
-        }
-        acc[k] = a;
+    if (e < E) {
+      const C* b = basis + ((size_t)(it.pos + base) * 2 + g) * E + e;
+#pragma unroll 4
+      for (int p = 0; p < cnt; ++p) {
+        const C v = b[(size_t)p * 2 * E];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < nc) {
+            const T qc = q[p][c0 + c];
+            acc[c].x += v.x * qc;
+            acc[c].y += v.y * qc;
+          }
       }
     }
-    __syncthreads();
   }
-  for (int k = 0; k < (nout + 255) / 256; ++k) {
-    const int o = threadIdx.x + 256 * k;
-    if (o < nout) M[(size_t)it.node * nout + o] = acc[k];
-  }
+  if (e < E)
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      if (c < nc) M[((size_t)it.node * kCh + c0 + c) * E + e] = acc[c];
 }
 
 // ---------------------------------------------------------------- M2M / L2L
@@ -378,65 +397,6 @@ __device__ void shift_block(const Tables<T>& tb, int ifl, bool multipole, int le
   __syncthreads();
 }
 
-struct ShiftItem {
-  int parent, first_child, n_children;  // children listed in shift_children
-};
-struct ShiftChild {
-  int node, octant;
-};
-
-// M2M: one block per (parent, channel) gathering its children in order
-template <typename T>
-__global__ void __launch_bounds__(64) m2m_kernel(const __grid_constant__ Tables<T> tb, const ShiftItem* __restrict__ items,
-                                                 const ShiftChild* __restrict__ children, int child_level,
-                                                 typename C2T<T>::type* __restrict__ M) {
-  using C = typename C2T<T>::type;
-  extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E;
-  C* w1 = reinterpret_cast<C*>(smem_raw);
-  C* w2 = w1 + E;
-  C* acc = w2 + E;
-  C* in = acc + E;
-  const ShiftItem it = items[blockIdx.x / kCh];
-  const int ch = blockIdx.x % kCh;
-  for (int o = threadIdx.x; o < E; o += blockDim.x) acc[o] = cmk<C>(0, 0);
-  for (int c = 0; c < it.n_children; ++c) {
-    const ShiftChild sc = children[it.first_child + c];
-    __syncthreads();
-    for (int o = threadIdx.x; o < E; o += blockDim.x) in[o] = M[((size_t)sc.node * kCh + ch) * E + o];
-    __syncthreads();
-    const T* rd = tb.R(sc.octant > 4 ? ROT_MSQ3 : ROT_SQ3);
-    shift_block<T>(tb, sc.octant, true, child_level, in, w1, w2, acc, rd, ch, 1);
-  }
-  __syncthreads();
-  for (int o = threadIdx.x; o < E; o += blockDim.x) M[((size_t)it.parent * kCh + ch) * E + o] = acc[o];
-}
-
-// L2L: one block per (child, channel), local_child += shift(local_parent)
-template <typename T>
-__global__ void __launch_bounds__(64) l2l_kernel(const __grid_constant__ Tables<T> tb, const ShiftItem* __restrict__ items,
-                                                 const ShiftChild* __restrict__ children, int parent_level,
-                                                 typename C2T<T>::type* __restrict__ L) {
-  using C = typename C2T<T>::type;
-  extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E;
-  C* w1 = reinterpret_cast<C*>(smem_raw);
-  C* w2 = w1 + E;
-  C* acc = w2 + E;
-  C* in = acc + E;
-  const ShiftItem it = items[blockIdx.x / kCh];
-  const int ch = blockIdx.x % kCh;
-  const ShiftChild sc = children[it.first_child];
-  for (int o = threadIdx.x; o < E; o += blockDim.x) {
-    in[o] = L[((size_t)it.parent * kCh + ch) * E + o];
-    acc[o] = L[((size_t)sc.node * kCh + ch) * E + o];
-  }
-  __syncthreads();
-  const T* rd = tb.R(sc.octant > 4 ? ROT_SQ3 : ROT_MSQ3);
-  shift_block<T>(tb, sc.octant, false, parent_level, in, w1, w2, acc, rd, ch, 1);
-  for (int o = threadIdx.x; o < E; o += blockDim.x) L[((size_t)sc.node * kCh + ch) * E + o] = acc[o];
-}
-
 // ---------------------------------------------------------------- M2X
 // rotation application out(l,m) = in(l,0) d(l,0,m) + sum_mp in(l,mp) d(l,mp,m) + conj(in(l,mp)) d(l,mp,-m)
 template <typename T>
@@ -455,132 +415,168 @@ struct M2xItem {
   int node, level;  // level of the node; tables of level-1
 };
 
-constexpr int kM2xThreads = 128;
+constexpr int kPairLanes = 64;  // lanes per direction pair / per target (>= nexptotp, nexptot and E)
+constexpr int kM2xThreads = 3 * kPairLanes;
+constexpr int kM2xChannels = 4;  // channels per M2X block (never straddles the screening groups)
 
-// one block per (node, channel): three multipole -> (Fourier -> physical)
-// conversions, one per direction pair
+// One block per (node, 4 channels); thread group g = direction pair
+// (0 up/down, 1 north/south, 2 east/west) runs the pair's rotation,
+// ympoletoexp and yftophys for the block's channels, the three pairs in
+// parallel.  Tables are those of the node's parent level.
 template <typename T>
 __global__ void __launch_bounds__(kM2xThreads) m2x_kernel(const __grid_constant__ Tables<T> tb,
                                                           const M2xItem* __restrict__ items,
                                                           const typename C2T<T>::type* __restrict__ M,
                                                           typename C2T<T>::type* __restrict__ W) {
   using C = typename C2T<T>::type;
+  constexpr int CB = kM2xChannels;
   extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E, NT = tb.nt, nl = tb.nl;
-  C* mp = reinterpret_cast<C*>(smem_raw);  // [E]
-  C* rot = mp + E;                          // [E]
-  C* fu = rot + E;                          // [nexptot]
-  C* fd = fu + 64;                          // [nexptot]
-  const M2xItem it = items[blockIdx.x / kCh];
-  const int ch = blockIdx.x % kCh;
-  const int lg = 2 * (it.level - 1) + (ch >= 8 ? 1 : 0);
+  const int E = tb.E, NT = tb.nt, nl = tb.nl, NPM = tb.np_max;
+  C* mp = reinterpret_cast<C*>(smem_raw);  // [CB][E]
+  C* rot = mp + CB * E;                     // [3][CB][E]
+  C* fr = rot + 3 * CB * E;                 // [3][2][CB][64]
+  const M2xItem it = items[blockIdx.x / (kCh / CB)];
+  const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
+  const int lg = 2 * (it.level - 1) + (ch0 >= 8 ? 1 : 0);
   const int nexptot = tb.nexptot[lg], np = tb.nexptotp[lg];
   const int* numphys = tb.numphys + (size_t)lg * nl;
   const T* rl = tb.rlsc + (size_t)lg * E * nl;
   const C* fexpe = tb.fexpe + tb.fexpe_off[lg];
   const C* fexpo = tb.fexpo + tb.fexpo_off[lg];
-  for (int e = threadIdx.x; e < E; e += blockDim.x) mp[e] = M[((size_t)it.node * kCh + ch) * E + e];
+  const int g = threadIdx.x / kPairLanes, lane = threadIdx.x - g * kPairLanes;
+  // after the shared multipole load the three pairs are independent: each
+  // pair's 64 threads synchronise on their own named barrier
+  auto pair_sync = [&]() { asm volatile("bar.sync %0, %1;\n" ::"r"(g + 1), "n"(kPairLanes) : "memory"); };
+  for (int o = threadIdx.x; o < CB * E; o += blockDim.x) mp[o] = M[((size_t)it.node * kCh + ch0) * E + o];
   __syncthreads();
-  for (int pair = 0; pair < 3; ++pair) {
-    // rotated multipole: pair 0 none, 1 rotate_ztoy(rdmpi2), 2 rotate_ztox(rdpi2)
-    for (int e = threadIdx.x; e < E; e += blockDim.x) {
-      if (pair == 0) {
-        rot[e] = mp[e];
-      } else {
-        int l = 0;
-        while (tri(l + 1, 0) <= e) ++l;
-        const int m = e - tri(l, 0);
-        if (pair == 1) {
-          // mwork = (-i)^m mpole, then rotation by rdmpi2
-          C v = cscale(mp[tri(l, 0)], tb.rd(tb.R(ROT_MPI2), l, 0, m));
-          for (int q = 1; q <= l; ++q) {
-            C s = mp[tri(l, q)];
-            // (-i)^q
-            switch (q & 3) {
-              case 1: s = cmk<C>(s.y, -s.x); break;
-              case 2: s = cmk<C>(-s.x, -s.y); break;
-              case 3: s = cmk<C>(-s.y, s.x); break;
-              default: break;
-            }
-            v = cadd(v, cadd(cscale(s, tb.rd(tb.R(ROT_MPI2), l, q, m)), cscale(cconj(s), tb.rd(tb.R(ROT_MPI2), l, q, -m))));
+  // rotated multipole: pair 0 none, 1 rotate_ztoy(rdmpi2) of (-i)^m M, 2 rotate_ztox(rdpi2)
+  if (lane < E) {
+    const int e = lane;
+    int l = 0;
+    while (tri(l + 1, 0) <= e) ++l;
+    const int m = e - tri(l, 0);
+    for (int c = 0; c < CB; ++c) {
+      const C* src = mp + c * E;
+      C v;
+      if (g == 0) {
+        v = src[e];
+      } else if (g == 1) {
+        const T* rd = tb.R(ROT_MPI2);
+        v = cscale(src[tri(l, 0)], tb.rd(rd, l, 0, m));
+        for (int q = 1; q <= l; ++q) {
+          C s = src[tri(l, q)];
+          switch (q & 3) {  // (-i)^q
+            case 1: s = cmk<C>(s.y, -s.x); break;
+            case 2: s = cmk<C>(-s.x, -s.y); break;
+            case 3: s = cmk<C>(-s.y, s.x); break;
+            default: break;
           }
-          rot[e] = v;
-        } else {
-          rot[e] = rotate_one<T>(tb, mp, tb.R(ROT_PI2), l, m);
+          v = cadd(v, cadd(cscale(s, tb.rd(rd, l, q, m)), cscale(cconj(s), tb.rd(rd, l, q, -m))));
         }
+      } else {
+        v = rotate_one<T>(tb, src, tb.R(ROT_PI2), l, m);
       }
+      rot[(g * CB + c) * E + e] = v;
     }
-    __syncthreads();
-    // ympoletoexp: Fourier modes (up, down)
-    for (int j = threadIdx.x; j < nexptot; j += blockDim.x) {
-      int l = 0, ntot = 0;
-      while (ntot + tb.numfour[l] <= j) {
-        ntot += tb.numfour[l];
-        ++l;
-      }
-      const int mth = j - ntot;
+  }
+  pair_sync();
+  // ympoletoexp: Fourier modes up (fu) and down (fd) of the pair
+  if (lane < nexptot) {
+    const int j = lane;
+    int l = 0, ntot = 0;
+    while (ntot + tb.numfour[l] <= j) {
+      ntot += tb.numfour[l];
+      ++l;
+    }
+    const int mth = j - ntot;
+    const T sgn = (mth & 1) ? T(-1) : T(1);
+    for (int c = 0; c < CB; ++c) {
+      const C* r = rot + (g * CB + c) * E;
       C z1 = cmk<C>(0, 0), z2 = cmk<C>(0, 0);
-      for (int nm = mth; nm <= NT; nm += 2) z1 = cadd(z1, cscale(rot[tri(nm, mth)], rl[(size_t)tri(nm, mth) * nl + l]));
-      for (int nm = mth + 1; nm <= NT; nm += 2) z2 = cadd(z2, cscale(rot[tri(nm, mth)], rl[(size_t)tri(nm, mth) * nl + l]));
-      fu[j] = cadd(z1, z2);
-      const T sgn = (mth & 1) ? T(-1) : T(1);
-      fd[j] = cscale(csub(z1, z2), sgn);
+      for (int nm = mth; nm <= NT; nm += 2) z1 = cadd(z1, cscale(r[tri(nm, mth)], rl[(size_t)tri(nm, mth) * nl + l]));
+      for (int nm = mth + 1; nm <= NT; nm += 2) z2 = cadd(z2, cscale(r[tri(nm, mth)], rl[(size_t)tri(nm, mth) * nl + l]));
+      fr[((g * 2 + 0) * CB + c) * 64 + j] = cadd(z1, z2);
+      fr[((g * 2 + 1) * CB + c) * 64 + j] = cscale(csub(z1, z2), sgn);
     }
-    __syncthreads();
-    // yftophys for both
-    for (int o = threadIdx.x; o < 2 * np; o += blockDim.x) {
-      const int which = o / np, iw = o - which * np;
-      const C* mf = which ? fd : fu;
-      int l = 0, nptot = 0, nftot = 0, be = 0, bo = 0;
-      while (nptot + numphys[l] / 2 <= iw) {
-        nptot += numphys[l] / 2;
-        nftot += tb.numfour[l];
-        be += (numphys[l] / 2) * (tb.numfour[l] / 2);
-        bo += (numphys[l] / 2) * ((tb.numfour[l] - 1) / 2);
-        ++l;
-      }
-      const int iv = iw - nptot;
-      const int nfo = tb.numfour[l];
-      C val = mf[nftot];
-      int k = 0;
-      for (int mm = 1; mm < nfo; mm += 2, ++k) {
-        const T s = (k & 1) ? T(-2) : T(2);
-        const C fe = fexpe[be + iv * (nfo / 2) + k];
-        const C pm = mf[nftot + mm];
-        val.y += s * (fe.x * pm.x - fe.y * pm.y);
-      }
-      k = 0;
-      for (int mm = 2; mm < nfo; mm += 2, ++k) {
-        const T s = (k & 1) ? T(2) : T(-2);
-        const C fo = fexpo[bo + iv * ((nfo - 1) / 2) + k];
-        const C pm = mf[nftot + mm];
-        val.x += s * (fo.x * pm.x - fo.y * pm.y);
-      }
-      const int dir = 2 * pair + which;  // 0 up 1 down 2 north 3 south 4 east 5 west
-      W[(((size_t)it.node * 6 + dir) * kCh + ch) * tb.np_max + iw] = val;
+  }
+  pair_sync();
+  // yftophys of both waves of the pair
+  if (lane < np) {
+    const int iw = lane;
+    int l = 0, nptot = 0, nftot = 0, be = 0, bo = 0;
+    while (nptot + numphys[l] / 2 <= iw) {
+      nptot += numphys[l] / 2;
+      nftot += tb.numfour[l];
+      be += (numphys[l] / 2) * (tb.numfour[l] / 2);
+      bo += (numphys[l] / 2) * ((tb.numfour[l] - 1) / 2);
+      ++l;
     }
-    __syncthreads();
+    const int iv = iw - nptot;
+    const int nfo = tb.numfour[l];
+    for (int which = 0; which < 2; ++which)
+      for (int c = 0; c < CB; ++c) {
+        const C* mf = fr + ((g * 2 + which) * CB + c) * 64;
+        C val = mf[nftot];
+        int k = 0;
+        for (int mm = 1; mm < nfo; mm += 2, ++k) {
+          const T s = (k & 1) ? T(-2) : T(2);
+          const C fe = fexpe[be + iv * (nfo / 2) + k];
+          const C pm = mf[nftot + mm];
+          val.y += s * (fe.x * pm.x - fe.y * pm.y);
+        }
+        k = 0;
+        for (int mm = 2; mm < nfo; mm += 2, ++k) {
+          const T s = (k & 1) ? T(2) : T(-2);
+          const C fo = fexpo[bo + iv * ((nfo - 1) / 2) + k];
+          const C pm = mf[nftot + mm];
+          val.x += s * (fo.x * pm.x - fo.y * pm.y);
+        }
+        const int dir = 2 * g + which;  // 0 up 1 down 2 north 3 south 4 east 5 west
+        W[(((size_t)it.node * 6 + dir) * kCh + ch0 + c) * NPM + iw] = val;
+      }
   }
 }
 
 // ---------------------------------------------------------------- X2L
+// Half of a parent's interaction list: up to 4 target children, each with
+// its entries sorted by direction (within a direction in table order).
 struct XlItem {
   int parent_level;
-  int first_entry[3], n_entries[3];  // entries of each direction pair (UP/DOWN, N/S, E/W)
-  int targets[8];                    // target child node ids (-1 absent or shadow)
+  int targets[4];  // target child node ids (-1 absent)
+  int first_entry[4], n_entries[4];
 };
+// One diagonal translation: source node, direction, and the translation
+// factor's index combo = up * 343 + (a+3) * 49 + (b+3) * 7 + (c+3) with
+// (a, b, c) the source->target offset in the direction's rotated frame.
 struct XlEntry {
-  int src;          // source node id
-  signed char dir, targ, a, b, c, up;
+  int src;
+  short combo;
+  signed char dir, pad;
+};
+constexpr int kCombos = 686;
+constexpr int kXlTargets = 4;
+constexpr int kXlThreads = kXlTargets * kPairLanes;
+constexpr int kXlUnroll = 8;
+constexpr int kXlMaxEntries = 192;  // >= 189 interactions of one target child
+
+template <typename T>
+struct XlChannels;  // channels per X2L block
+template <>
+struct XlChannels<float> {
+  static constexpr int value = 2;
+};
+template <>
+struct XlChannels<double> {
+  static constexpr int value = 1;
 };
 
-constexpr int kXlGroup = 96;  // threads per direction pair (>= nexptotp)
-constexpr int kXlThreads = 3 * kXlGroup;
-
-// One block per (parent, channel); thread group g handles direction pair g:
-// its diagonal translations accumulated in shared memory per (direction,
-// target child), then yphystof + yexptolocal + rotation back per target;
-// the three pairs' local expansions are summed in a fixed order.
+// One block per (half item, channel block); thread (target tl, lane i).
+// Phase 1: each thread accumulates, in registers, its target's translated
+// waves (translate_up/down_wave: W[src][dir] * factor[combo]) for every
+// direction, stored per (target, direction) once a direction's run ends.
+// Phase 2: yphystof of the six waves.  Phase 3: yexptolocal per pair.
+// Phase 4: rotation back (rotate_ytoz / rotate_ztox) and the sum of the three
+// pairs, assigned to the target's local expansion.
 template <typename T>
 __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__ Tables<T> tb,
                                                          const XlItem* __restrict__ items,
@@ -588,72 +584,87 @@ __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__
                                                          const typename C2T<T>::type* __restrict__ W,
                                                          typename C2T<T>::type* __restrict__ L) {
   using C = typename C2T<T>::type;
+  constexpr int CB = XlChannels<T>::value;
   extern __shared__ unsigned char smem_raw[];
   const int E = tb.E, nl = tb.nl, NPM = tb.np_max;
-  C* acc = reinterpret_cast<C*>(smem_raw);  // [6 dirs][8 targets][NPM]
-  C* mf = acc + 6 * 8 * NPM;                 // [3 pairs][2][64]
-  C* loc = mf + 3 * 2 * 64;                  // [3][E]
-  C* out = loc + 3 * E;                      // [3][E]
-  const XlItem it = items[blockIdx.x / kCh];
-  const int ch = blockIdx.x % kCh;
-  const int lg = 2 * it.parent_level + (ch >= 8 ? 1 : 0);
+  C* acc = reinterpret_cast<C*>(smem_raw);        // [4 targets][6 dirs][CB][NPM]
+  C* mf = acc + kXlTargets * 6 * CB * NPM;         // [4][6][CB][64]
+  XlEntry* ents = reinterpret_cast<XlEntry*>(mf + kXlTargets * 6 * CB * 64);  // [4][kXlMaxEntries]
+  const XlItem it = items[blockIdx.x / (kCh / CB)];
+  const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
+  const int lg = 2 * it.parent_level + (ch0 >= 8 ? 1 : 0);
   const int np = tb.nexptotp[lg], nexptot = tb.nexptot[lg];
-  const int g = threadIdx.x / kXlGroup, lt = threadIdx.x - g * kXlGroup;
-  for (int o = threadIdx.x; o < 6 * 8 * NPM; o += blockDim.x) acc[o] = cmk<C>(0, 0);
-  __syncthreads();
-  // translations of pair g
-  if (lt < np) {
-    const int i = lt;
-    const C* xs = tb.xs + (size_t)lg * 3 * NPM;
-    const C* ys = tb.ys + (size_t)lg * 3 * NPM;
-    const T* zs = tb.zs + (size_t)lg * 3 * NPM;
-    const int e0 = it.first_entry[g], ne = it.n_entries[g];
-    for (int k = 0; k < ne; ++k) {
-      const XlEntry en = entries[e0 + k];
-      const C w = W[(((size_t)en.src * 6 + en.dir) * kCh + ch) * NPM + i];
-      C t;
-      if (en.up) {
-        T tr = 1;
-        if (en.c > 0) tr = zs[(en.c - 1) * NPM + i];
-        t = cmk<C>(tr, 0);
-        if (en.b > 0) t = cmul(t, ys[(en.b - 1) * NPM + i]);
-        else if (en.b < 0) t = cmul(t, cconj(ys[(-en.b - 1) * NPM + i]));
-        if (en.a > 0) t = cmul(t, xs[(en.a - 1) * NPM + i]);
-        else if (en.a < 0) t = cmul(t, cconj(xs[(-en.a - 1) * NPM + i]));
-      } else {
-        T tr = 1;
-        if (en.c < 0) tr = zs[(-en.c - 1) * NPM + i];
-        t = cmk<C>(tr, 0);
-        if (en.b > 0) t = cmul(t, cconj(ys[(en.b - 1) * NPM + i]));
-        else if (en.b < 0) t = cmul(t, ys[(-en.b - 1) * NPM + i]);
-        if (en.a > 0) t = cmul(t, cconj(xs[(en.a - 1) * NPM + i]));
-        else if (en.a < 0) t = cmul(t, xs[(-en.a - 1) * NPM + i]);
+  const int tl = threadIdx.x / kPairLanes, lane = threadIdx.x - tl * kPairLanes;
+  const int tn = it.targets[tl];
+  // the four targets are independent: each one's 64 threads synchronise on
+  // their own named barrier, and absent targets leave at once
+  if (tn < 0) return;
+  auto target_sync = [&]() { asm volatile("bar.sync %0, %1;\n" ::"r"(tl + 1), "n"(kPairLanes) : "memory"); };
+  C* acc_t = acc + (size_t)tl * 6 * CB * NPM;
+  C* loc = acc_t;  // [3 pairs][CB][E]: the target's own accumulators, reused after phase 2
+  for (int o = lane; o < 6 * CB * NPM; o += kPairLanes) acc_t[o] = cmk<C>(0, 0);
+  const int ne = it.n_entries[tl];
+  XlEntry* ent = ents + tl * kXlMaxEntries;
+  for (int o = lane; o < ne; o += kPairLanes) ent[o] = entries[it.first_entry[tl] + o];
+  target_sync();
+  if (lane < np) {
+    const int i = lane;
+    const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
+    C a[CB];
+#pragma unroll
+    for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
+    int cur = ne ? ent[0].dir : 0;
+    for (int k0 = 0; k0 < ne; k0 += kXlUnroll) {
+      XlEntry en[kXlUnroll];
+      C tt[kXlUnroll], w[kXlUnroll][CB];
+#pragma unroll
+      for (int u = 0; u < kXlUnroll; ++u) en[u] = ent[min(k0 + u, ne - 1)];
+#pragma unroll
+      for (int u = 0; u < kXlUnroll; ++u) {
+        tt[u] = tc[(size_t)en[u].combo * NPM];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) w[u][c] = W[(((size_t)en[u].src * 6 + en[u].dir) * kCh + ch0 + c) * NPM + i];
       }
-      C& a = acc[((size_t)en.dir * 8 + en.targ) * NPM + i];
-      a = cadd(a, cmul(w, t));
+#pragma unroll
+      for (int u = 0; u < kXlUnroll; ++u) {
+        if (k0 + u < ne) {
+          if (en[u].dir != cur) {
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+              acc[((tl * 6 + cur) * CB + c) * NPM + i] = a[c];
+              a[c] = cmk<C>(0, 0);
+            }
+            cur = en[u].dir;
+          }
+#pragma unroll
+          for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
+        }
+      }
     }
+    if (ne)
+#pragma unroll
+      for (int c = 0; c < CB; ++c) acc[((tl * 6 + cur) * CB + c) * NPM + i] = a[c];
   }
+  target_sync();
   const int* numphys = tb.numphys + (size_t)lg * nl;
   const C* fb = tb.fexpback + tb.fexpback_off[lg];
   const T* rl = tb.rlsc + (size_t)lg * E * nl;
-  for (int t = 0; t < 8; ++t) {
-    const int tn = it.targets[t];
-    if (tn < 0) continue;
-    __syncthreads();
-    // yphystof of the pair's up (2g) and down (2g+1) waves
-    for (int o = lt; o < 2 * 64; o += kXlGroup) {
-      const int which = o / 64, j = o - which * 64;
-      if (j >= nexptot) continue;
-      int l = 0, nftot = 0, nptot = 0, bb = 0;
-      while (nftot + tb.numfour[l] <= j) {
-        nftot += tb.numfour[l];
-        nptot += numphys[l] / 2;
-        bb += (tb.numfour[l] - 1) * (numphys[l] / 2);
-        ++l;
-      }
-      const int mm = j - nftot + 1;
-      const int na = numphys[l], na2 = na / 2;
-      const C* ph = acc + ((size_t)(2 * g + which) * 8 + t) * NPM + nptot;
+  // yphystof of the six waves
+  if (lane < nexptot) {
+    const int j = lane;
+    int l = 0, nftot = 0, nptot = 0, bb = 0;
+    while (nftot + tb.numfour[l] <= j) {
+      nftot += tb.numfour[l];
+      nptot += numphys[l] / 2;
+      bb += (tb.numfour[l] - 1) * (numphys[l] / 2);
+      ++l;
+    }
+    const int mm = j - nftot + 1;
+    const int na = numphys[l], na2 = na / 2;
+    const T ina = T(1) / T(na);
+    const int nodd = (tb.numfour[l] - 1) / 2;
+    for (int dc = 0; dc < 6 * CB; ++dc) {
+      const C* ph = acc + ((size_t)tl * 6 * CB + dc) * NPM + nptot;
       C sum = cmk<C>(0, 0);
       if (mm == 1) {
         for (int iv = 0; iv < na2; ++iv) sum.x += T(2) * ph[iv].x;
@@ -661,66 +672,63 @@ __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__
         const C* f = fb + bb + ((mm - 3) / 2) * na2;
         for (int iv = 0; iv < na2; ++iv) sum = cadd(sum, cscale(f[iv], T(2) * ph[iv].x));
       } else {
-        const int nodd = (tb.numfour[l] - 1) / 2;
         const C* f = fb + bb + nodd * na2 + ((mm - 2) / 2) * na2;
         for (int iv = 0; iv < na2; ++iv) sum = cadd(sum, cmul(f[iv], cmk<C>(0, T(2) * ph[iv].y)));
       }
-      mf[(g * 2 + which) * 64 + j] = cscale(sum, T(1) / T(na));
+      mf[((size_t)tl * 6 * CB + dc) * 64 + j] = cscale(sum, ina);
     }
-    __syncthreads();
-    // yexptolocal
-    for (int e = lt; e < E; e += kXlGroup) {
-      int nm = 0;
-      while (tri(nm + 1, 0) <= e) ++nm;
-      const int mth = e - tri(nm, 0);
-      const C* fu = mf + (g * 2 + 0) * 64;
-      const C* fd = mf + (g * 2 + 1) * 64;
-      C v = cmk<C>(0, 0);
-      int ntot = 0;
-      for (int l = 0; l < nl; ++l) {
-        const int mmax = tb.numfour[l] - 1 > nm ? nm : tb.numfour[l] - 1;
-        if (mth <= mmax) {
-          const C pm = (nm & 1) ? csub(fd[ntot + mth], fu[ntot + mth]) : cadd(fd[ntot + mth], fu[ntot + mth]);
-          v = cadd(v, cscale(pm, rl[(size_t)e * nl + l] * tb.weights[l]));
+  }
+  target_sync();
+  // yexptolocal per pair (loc overwrites acc, which is no longer read)
+  if (lane < E) {
+    const int e = lane;
+    int nm = 0;
+    while (tri(nm + 1, 0) <= e) ++nm;
+    const int mth = e - tri(nm, 0);
+    const T rs = T(3.14159265358979323846) / (tb.betascal[lg] * T(2)) * tb.sfac[e];
+    for (int g = 0; g < 3; ++g)
+      for (int c = 0; c < CB; ++c) {
+        const C* fu = mf + ((size_t)(tl * 6 + 2 * g) * CB + c) * 64;
+        const C* fd = mf + ((size_t)(tl * 6 + 2 * g + 1) * CB + c) * 64;
+        C v = cmk<C>(0, 0);
+        int ntot = 0;
+        for (int l = 0; l < nl; ++l) {
+          const int mmax = tb.numfour[l] - 1 > nm ? nm : tb.numfour[l] - 1;
+          if (mth <= mmax) {
+            const C pm = (nm & 1) ? csub(fd[ntot + mth], fu[ntot + mth]) : cadd(fd[ntot + mth], fu[ntot + mth]);
+            v = cadd(v, cscale(pm, rl[(size_t)e * nl + l] * tb.weights[l]));
+          }
+          ntot += tb.numfour[l];
         }
-        ntot += tb.numfour[l];
-      }
-      const T rs = T(3.14159265358979323846) / (tb.betascal[lg] * T(2)) * tb.sfac[e];
-      v = cscale(v, rs);
-      switch (mth & 3) {  // * i^m
-        case 1: v = cmk<C>(-v.y, v.x); break;
-        case 2: v = cmk<C>(-v.x, -v.y); break;
-        case 3: v = cmk<C>(v.y, -v.x); break;
-        default: break;
-      }
-      loc[g * E + e] = v;
-    }
-    __syncthreads();
-    // rotate back
-    for (int e = lt; e < E; e += kXlGroup) {
-      if (g == 0) {
-        out[e] = loc[e];
-        continue;
-      }
-      int l = 0;
-      while (tri(l + 1, 0) <= e) ++l;
-      const int m = e - tri(l, 0);
-      if (g == 1) {  // rotate_ytoz(rdpi2): rotate then * i^m
-        C v = rotate_one<T>(tb, loc + E, tb.R(ROT_PI2), l, m);
-        switch (m & 3) {
+        v = cscale(v, rs);
+        switch (mth & 3) {  // * i^m
           case 1: v = cmk<C>(-v.y, v.x); break;
           case 2: v = cmk<C>(-v.x, -v.y); break;
           case 3: v = cmk<C>(v.y, -v.x); break;
           default: break;
         }
-        out[E + e] = v;
-      } else {  // rotate_ztox(rdmpi2)
-        out[2 * E + e] = rotate_one<T>(tb, loc + 2 * E, tb.R(ROT_MPI2), l, m);
+        loc[((size_t)g * CB + c) * E + e] = v;
       }
+  }
+  target_sync();
+  // rotate back and sum the pairs
+  if (lane < E) {
+    const int e = lane;
+    int l = 0;
+    while (tri(l + 1, 0) <= e) ++l;
+    const int m = e - tri(l, 0);
+    for (int c = 0; c < CB; ++c) {
+      const C v0 = loc[((size_t)0 * CB + c) * E + e];
+      C v1 = rotate_one<T>(tb, loc + ((size_t)1 * CB + c) * E, tb.R(ROT_PI2), l, m);
+      switch (m & 3) {  // rotate_ytoz: * i^m
+        case 1: v1 = cmk<C>(-v1.y, v1.x); break;
+        case 2: v1 = cmk<C>(-v1.x, -v1.y); break;
+        case 3: v1 = cmk<C>(v1.y, -v1.x); break;
+        default: break;
+      }
+      const C v2 = rotate_one<T>(tb, loc + ((size_t)2 * CB + c) * E, tb.R(ROT_MPI2), l, m);
+      L[((size_t)tn * kCh + ch0 + c) * E + e] = cadd(cadd(v0, v1), v2);
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < E; e += blockDim.x)
-      L[((size_t)tn * kCh + ch) * E + e] = cadd(cadd(out[e], out[E + e]), out[2 * E + e]);
   }
 }
 
@@ -923,83 +931,120 @@ __global__ void __launch_bounds__(64) l2p_prep_kernel(const __grid_constant__ Ta
   }
 }
 
-// One thread per target patch: q(n, m) generated on the fly (Bessel,
-// Legendre recurrence in n for each m, e^{i m phi}) and contracted with the
-// leaf's F and H_j; y_f += f / 4 pi, y_h += n . h / 4 pi.
 constexpr int kEvalChunk = 64;  // targets per l2p_eval block
 
+// q(n, m) = i_n(beta r) P_n^m(cos theta) e^{i m phi} of every target patch
+// relative to its leaf centre, n <= nt + 2, per screening group: geometry
+// alone, tabulated once per problem as Q[item][g][tri(n, m)][lane].
 template <typename T>
-__global__ void __launch_bounds__(kEvalChunk) l2p_eval_kernel(const __grid_constant__ Tables<T> tb,
-                                                       const LeafItem* __restrict__ items,
-                                                       const int32_t* __restrict__ contents,
-                                                       const double* __restrict__ centroid,
-                                                       const double* __restrict__ normal,
-                                                       const typename C2T<T>::type* __restrict__ D, int n,
-                                                       double* __restrict__ y) {
+__global__ void __launch_bounds__(kEvalChunk) l2p_basis_kernel(const __grid_constant__ Tables<T> tb,
+                                                               const LeafItem* __restrict__ items,
+                                                               const int32_t* __restrict__ contents,
+                                                               const double* __restrict__ centroid,
+                                                               typename C2T<T>::type* __restrict__ Q) {
   using C = typename C2T<T>::type;
-  extern __shared__ unsigned char smem_raw[];
   const int NT = tb.nt, N2 = NT + 2;
   const int EQ = (NT + 3) * (NT + 4) / 2;
-  C* Ds = reinterpret_cast<C*>(smem_raw);  // [2][4][EQ]
+  const LeafItem it = items[blockIdx.x];
+  const int k = threadIdx.x;
+  if (k >= it.count) return;
+  const int i = contents[it.start + k];
+  const double rx = centroid[3 * i] - it.c[0], ry = centroid[3 * i + 1] - it.c[1], rz = centroid[3 * i + 2] - it.c[2];
+  double proj = rx * rx + ry * ry;
+  const double rr = proj + rz * rz;
+  proj = sqrt(proj);
+  const double d = sqrt(rr);
+  const double PREC = 2.220446049250313e-16;
+  const T x = (T)((d <= PREC) ? 0.0 : rz / d);
+  const C e1 = (proj <= PREC * d) ? cmk<C>(1, 0) : cmk<C>((T)(rx / proj), (T)(ry / proj));
+  const T u = -sqrt(T(1) - x * x);
+  T bi[kMaxNT + 4];
+  for (int g = 0; g < 2; ++g) {
+    const int lg = 2 * it.level + g;
+    bessel_in_dev<T>(tb.scale[lg], (T)(d * (double)tb.beta[g]), N2, bi);
+    C* q = Q + ((size_t)blockIdx.x * 2 + g) * EQ * kEvalChunk + k;
+    C em = cmk<C>(1, 0);  // e^{i m phi}
+    T pmm = 1;            // P_m^m
+    for (int m = 0; m <= N2; ++m) {
+      if (m > 0) {
+        pmm = pmm * u * T(2 * m - 1);
+        em = cmul(em, e1);
+      }
+      T p0 = 0, p1 = pmm;  // P_{n-1}^m, P_n^m at n = m
+      for (int nn = m; nn <= N2; ++nn) {
+        T pn;
+        if (nn == m) {
+          pn = pmm;
+        } else if (nn == m + 1) {
+          pn = T(2 * m + 1) * x * pmm;
+        } else {
+          pn = ((T(2) * nn - T(1)) * x * p1 - T(nn + m - 1) * p0) / T(nn - m);
+        }
+        if (nn > m) {
+          p0 = p1;
+          p1 = pn;
+        }
+        const T amp = (nn == 0) ? bi[0] : bi[nn] * pn;
+        q[(size_t)tri(nn, m) * kEvalChunk] = cscale(em, amp);
+      }
+    }
+  }
+}
+
+// One block per chunk of <= 64 targets of a leaf; thread (slice s, target k)
+// sums a quarter of the terms (s = 2 g + half: screening group g, half of
+// the tri(n, m) range) of f = Re sum q F, h_j = Re sum q H_j (F only to
+// n <= nt+1); the four partial sums are added in a fixed order and
+// y_f = f / 4 pi, y_h = n . h / 4 pi assigned to the far-field buffer.
+constexpr int kEvalThreads = 4 * kEvalChunk;
+
+template <typename T>
+__global__ void __launch_bounds__(kEvalThreads) l2p_eval_kernel(int nt, const LeafItem* __restrict__ items,
+                                                                const int32_t* __restrict__ contents,
+                                                                const double* __restrict__ normal,
+                                                                const typename C2T<T>::type* __restrict__ D,
+                                                                const typename C2T<T>::type* __restrict__ Q, int n,
+                                                                double* __restrict__ y) {
+  using C = typename C2T<T>::type;
+  extern __shared__ unsigned char smem_raw[];
+  const int EQ = (nt + 3) * (nt + 4) / 2, EF = (nt + 2) * (nt + 3) / 2;
+  C* Ds = reinterpret_cast<C*>(smem_raw);                   // [2][4][EQ]
+  T* part = reinterpret_cast<T*>(Ds + 8 * EQ);              // [4 slices][4 sums][kEvalChunk]
   const LeafItem it = items[blockIdx.x];
   for (int o = threadIdx.x; o < 8 * EQ; o += blockDim.x) Ds[o] = D[(size_t)it.leaf * 8 * EQ + o];
   __syncthreads();
-  for (int k = threadIdx.x; k < it.count; k += blockDim.x) {
-    const int i = contents[it.start + k];
-    const double rx = centroid[3 * i] - it.c[0], ry = centroid[3 * i + 1] - it.c[1], rz = centroid[3 * i + 2] - it.c[2];
-    double proj = rx * rx + ry * ry;
-    const double rr = proj + rz * rz;
-    proj = sqrt(proj);
-    const double d = sqrt(rr);
-    const double PREC = 2.220446049250313e-16;
-    const T x = (T)((d <= PREC) ? 0.0 : rz / d);
-    const C e1 = (proj <= PREC * d) ? cmk<C>(1, 0) : cmk<C>((T)(rx / proj), (T)(ry / proj));
-    const T u = -sqrt(T(1) - x * x);
-    T f = 0, h0 = 0, h1 = 0, h2 = 0;
-    T bi[kMaxNT + 4];
-    for (int g = 0; g < 2; ++g) {
-      const int lg = 2 * it.level + g;
-      bessel_in_dev<T>(tb.scale[lg], (T)(d * (double)tb.beta[g]), N2, bi);
-      const C* F = Ds + g * 4 * EQ;
-      const C* H0 = F + EQ;
-      const C* H1 = F + 2 * EQ;
-      const C* H2 = F + 3 * EQ;
-      C em = cmk<C>(1, 0);  // e^{i m phi}
-      T pmm = 1;            // P_m^m
-      for (int m = 0; m <= N2; ++m) {
-        if (m > 0) {
-          pmm = pmm * u * T(2 * m - 1);
-          em = cmul(em, e1);
-        }
-        T p0 = 0, p1 = pmm;  // P_{n-1}^m, P_n^m at n = m
-        for (int nn = m; nn <= N2; ++nn) {
-          T pn;
-          if (nn == m) {
-            pn = pmm;
-          } else if (nn == m + 1) {
-            pn = T(2 * m + 1) * x * pmm;
-          } else {
-            pn = ((T(2) * nn - T(1)) * x * p1 - T(nn + m - 1) * p0) / T(nn - m);
-          }
-          if (nn > m) {
-            p0 = p1;
-            p1 = pn;
-          }
-          const T amp = (nn == 0) ? bi[0] : bi[nn] * pn;
-          const C q = cscale(em, amp);
-          const int e = tri(nn, m);
-          if (nn <= NT + 1) f += q.x * F[e].x - q.y * F[e].y;
-          h0 += q.x * H0[e].x - q.y * H0[e].y;
-          h1 += q.x * H1[e].x - q.y * H1[e].y;
-          h2 += q.x * H2[e].x - q.y * H2[e].y;
-        }
-      }
+  const int s = threadIdx.x / kEvalChunk, k = threadIdx.x - s * kEvalChunk;
+  const int g = s >> 1, half = EQ / 2;
+  const int e0 = (s & 1) ? half : 0, e1 = (s & 1) ? EQ : half;
+  T f = 0, h0 = 0, h1 = 0, h2 = 0;
+  if (k < it.count) {
+    const C* q = Q + ((size_t)blockIdx.x * 2 + g) * EQ * kEvalChunk + k;
+    const C* F = Ds + g * 4 * EQ;
+#pragma unroll 8
+    for (int e = e0; e < e1; ++e) {
+      const C v = q[(size_t)e * kEvalChunk];
+      if (e < EF) f += v.x * F[e].x - v.y * F[e].y;
+      h0 += v.x * F[EQ + e].x - v.y * F[EQ + e].y;
+      h1 += v.x * F[2 * EQ + e].x - v.y * F[2 * EQ + e].y;
+      h2 += v.x * F[3 * EQ + e].x - v.y * F[3 * EQ + e].y;
     }
-    const double k4 = 0.07957747154594767;
-    const double h = normal[3 * i] * (double)h0 + normal[3 * i + 1] * (double)h1 + normal[3 * i + 2] * (double)h2;
-    y[i] = (double)f * k4;  // far-field buffer: every patch is in exactly one leaf
-    y[n + i] = h * k4;
   }
+  part[(s * 4 + 0) * kEvalChunk + k] = f;
+  part[(s * 4 + 1) * kEvalChunk + k] = h0;
+  part[(s * 4 + 2) * kEvalChunk + k] = h1;
+  part[(s * 4 + 3) * kEvalChunk + k] = h2;
+  __syncthreads();
+  if (s != 0 || k >= it.count) return;
+  T sum[4];
+  for (int j = 0; j < 4; ++j)
+    sum[j] = ((part[(0 * 4 + j) * kEvalChunk + k] + part[(1 * 4 + j) * kEvalChunk + k]) +
+              part[(2 * 4 + j) * kEvalChunk + k]) + part[(3 * 4 + j) * kEvalChunk + k];
+  const int i = contents[it.start + k];
+  const double k4 = 0.07957747154594767;
+  const double h = normal[3 * i] * (double)sum[1] + normal[3 * i + 1] * (double)sum[2] +
+                   normal[3 * i + 2] * (double)sum[3];
+  y[i] = (double)sum[0] * k4;  // far-field buffer: every patch is in exactly one leaf
+  y[n + i] = h * k4;
 }
 
 template <typename C, typename S>
@@ -1044,45 +1089,133 @@ __global__ void __launch_bounds__(64) shift_basis_kernel(const __grid_constant__
   const bool multipole = kind == 0;
   const T* rd = multipole ? tb.R(oct > 4 ? ROT_MSQ3 : ROT_SQ3) : tb.R(oct > 4 ? ROT_SQ3 : ROT_MSQ3);
   shift_block<T>(tb, oct, multipole, level, in, w1, w2, acc, rd, g ? 8 : 0, 1);
-  T* col = ops + ((size_t)op * R + k) * R;  // column k: [op][k][r]
+  const int RP = (R + 3) & ~3;
+  T* col = ops + ((size_t)op * R + k) * RP;  // column k: [op][k][r], rows padded to RP with zeros
   for (int o = threadIdx.x; o < E; o += blockDim.x) {
     col[2 * o] = acc[o].x;
     col[2 * o + 1] = acc[o].y;
   }
+  for (int r = R + threadIdx.x; r < RP; r += blockDim.x) col[r] = 0;
 }
 
-struct DenseShift {
-  int target, first_src, n_src;  // sources listed in DenseSrc
-};
-struct DenseSrc {
-  int node, op;  // source expansion node and operator index
-};
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
-// y[target][ch] (=, or += for L2L) sum over sources of A_op x[source][ch];
-// one block per (target, channel), thread per output real
+// Operator form of M2M and L2L as a gather-GEMM.  A tile is up to 16
+// columns sharing one operator (kind, level, screening group, octant); a
+// column is (source node, destination row, channel).  M2M writes one
+// partial per (parent, child) and shift_reduce_kernel sums a parent's
+// partials in child order; L2L writes the child's local expansion directly
+// (assigned, or added to the X2L result).
+struct ShiftTile {
+  int op;  // operator index including the screening-group offset
+  int first_col, n_cols;
+};
+struct ShiftCol {
+  int src, dst, ch, accumulate;
+};
+struct ShiftReduce {
+  int parent, first_slot, n_slots;
+};
+constexpr int kTileCols = 16;
+constexpr int kGemmThreads = 128;
+
 template <typename T>
-__global__ void __launch_bounds__(128) dense_shift_kernel(int E, const DenseShift* __restrict__ items,
-                                                          const DenseSrc* __restrict__ srcs,
-                                                          const T* __restrict__ ops, const T* __restrict__ X,
-                                                          T* __restrict__ Y, int accumulate) {
-  extern __shared__ unsigned char smem_raw[];
-  const int R = 2 * E;
-  T* xs = reinterpret_cast<T*>(smem_raw);  // [8][R]
-  const DenseShift it = items[blockIdx.x / kCh];
-  const int ch = blockIdx.x % kCh;
-  for (int o = threadIdx.x; o < it.n_src * R; o += blockDim.x) {
-    const DenseSrc sc = srcs[it.first_src + o / R];
-    xs[o] = X[((size_t)sc.node * kCh + ch) * R + o % R];
+__device__ __forceinline__ void load4(const T* p, T (&v)[4]);
+template <>
+__device__ __forceinline__ void load4<float>(const float* p, float (&v)[4]) {
+  const float4 u = *reinterpret_cast<const float4*>(p);
+  v[0] = u.x, v[1] = u.y, v[2] = u.z, v[3] = u.w;
+}
+template <>
+__device__ __forceinline__ void load4<double>(const double* p, double (&v)[4]) {
+  const double2 u = reinterpret_cast<const double2*>(p)[0], w = reinterpret_cast<const double2*>(p)[1];
+  v[0] = u.x, v[1] = u.y, v[2] = w.x, v[3] = w.y;
+}
+
+// One block per tile; thread (row group rg, column group cg) computes rows
+// 4rg..4rg+3 of columns 4cg..4cg+3: Y[dst][ch] (= or +=) A_op X[src][ch].
+// The operator (its transpose, rows padded to RP) arrives in shared memory
+// in one cp.async burst while the tile's inputs are gathered.
+template <typename T>
+__global__ void __launch_bounds__(kGemmThreads) shift_gemm_kernel(int E, const ShiftTile* __restrict__ tiles,
+                                                                  const ShiftCol* __restrict__ cols,
+                                                                  const T* __restrict__ ops,
+                                                                  const T* __restrict__ X, T* __restrict__ Y) {
+  const int R = 2 * E, RP = (R + 3) & ~3;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);  // [R][RP]
+  T* xs = As + (size_t)R * RP;              // [R][kTileCols]
+  const ShiftTile tl = tiles[blockIdx.x];
+  {
+    const char* src = reinterpret_cast<const char*>(ops + (size_t)tl.op * R * RP);
+    char* dst = reinterpret_cast<char*>(As);
+    const int n16 = R * RP * (int)sizeof(T) / 16;
+    for (int j = threadIdx.x; j < n16; j += blockDim.x) cp_async16(dst + 16 * j, src + 16 * j);
+    cp_async_commit();
   }
-  __syncthreads();
-  for (int r = threadIdx.x; r < R; r += blockDim.x) {
-    T acc = accumulate ? Y[((size_t)it.target * kCh + ch) * R + r] : T(0);
-    for (int c = 0; c < it.n_src; ++c) {
-      const T* A = ops + (size_t)(srcs[it.first_src + c].op + (ch >= 8 ? 8 : 0)) * R * R;  // group offset
-      const T* x = xs + c * R;
-      for (int k = 0; k < R; ++k) acc += A[(size_t)k * R + r] * x[k];
+  for (int o = threadIdx.x; o < kTileCols * R; o += blockDim.x) {
+    const int j = o / R, k = o - j * R;
+    T v = 0;
+    if (j < tl.n_cols) {
+      const ShiftCol c = cols[tl.first_col + j];
+      v = X[((size_t)c.src * kCh + c.ch) * R + k];
     }
-    Y[((size_t)it.target * kCh + ch) * R + r] = acc;
+    xs[k * kTileCols + j] = v;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  const int ngr = RP / 4;
+  if (threadIdx.x >= ngr * (kTileCols / 4)) return;
+  const int rg = threadIdx.x % ngr, cg = threadIdx.x / ngr;
+  if (4 * cg >= tl.n_cols) return;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+  const T* a = As + 4 * rg;
+  const T* x = xs + 4 * cg;
+#pragma unroll 10
+  for (int k = 0; k < R; ++k) {
+    T av[4], xv[4];
+    load4<T>(a + (size_t)k * RP, av);
+    load4<T>(x + k * kTileCols, xv);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] += av[i] * xv[j];
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (4 * cg + j >= tl.n_cols) break;
+    const ShiftCol c = cols[tl.first_col + 4 * cg + j];
+    T* y = Y + ((size_t)c.dst * kCh + c.ch) * R;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = 4 * rg + i;
+      if (r < R) y[r] = c.accumulate ? y[r] + acc[i][j] : acc[i][j];
+    }
+  }
+}
+
+// M[parent] = sum of its children's partials, in child order
+template <typename T>
+__global__ void __launch_bounds__(256) shift_reduce_kernel(int E, const ShiftReduce* __restrict__ items,
+                                                           const T* __restrict__ P, T* __restrict__ M) {
+  const int R = 2 * E;
+  const ShiftReduce it = items[blockIdx.x];
+  for (int o = threadIdx.x; o < kCh * R; o += blockDim.x) {
+    T v = P[(size_t)it.first_slot * kCh * R + o];
+    for (int j = 1; j < it.n_slots; ++j) v += P[(size_t)(it.first_slot + j) * kCh * R + o];
+    M[(size_t)it.parent * kCh * R + o] = v;
   }
 }
 
@@ -1130,21 +1263,32 @@ struct FmmState {
   Tables<double> tb_d{};
   Tables<float> tb_f{};
   DevBuf M, L, W;  // expansions and plane waves
-  DevBuf p2m_items, m2x_items, xl_items, xl_entries, leaf_items, m2m_items, m2m_children, l2l_items, l2l_children;
+  DevBuf p2m_items, m2x_items, xl_items, xl_entries, leaf_items;
   int n_p2m = 0, n_m2x = 0, n_xl = 0, n_leaf = 0;
-  std::vector<int> m2m_first, m2m_count;  // per child level
-  std::vector<int> l2l_first, l2l_count;  // per parent level
-  size_t smem_p2m = 0, smem_shift = 0, smem_m2x = 0, smem_xl = 0, smem_prep = 0, smem_eval = 0;
+  size_t smem_shift = 0, smem_m2x = 0, smem_xl = 0, smem_prep = 0, smem_eval = 0;
   DevBuf leaf_exp;  // per leaf: [2 groups][F, H0, H1, H2][EQ]
   DevBuf eval_items;
+  DevBuf p2m_basis;   // [patch position][2 groups][E], geometry only
+  DevBuf eval_basis;  // [eval item][2 groups][EQ][kEvalChunk], geometry only
   int n_eval = 0;
   // operator form of M2M / L2L and of the L2P preparation
-  DevBuf shift_ops;                       // [op][k][r], op = ((kind*nlev + level)*2 + group)*8 + octant-1
-  DevBuf m2m_dense, m2m_src, l2l_dense, l2l_src;
-  std::vector<int> m2m_dfirst, m2m_dcount, l2l_dfirst, l2l_dcount;
+  DevBuf shift_ops;  // [op][k][r], op = ((kind*nlev + level)*2 + group)*8 + octant-1
+  DevBuf shift_tiles, shift_cols, m2m_reduce, m2m_partials;
+  std::vector<int> m2m_tfirst, m2m_tcount, m2m_rfirst, m2m_rcount;  // per child level
+  std::vector<int> l2l_tfirst, l2l_tcount;                          // per parent level
   DevBuf prep_rowptr, prep_cols, prep_vals;
-  size_t smem_dense = 0, smem_csr = 0;
-  bool use_operators = true;
+  size_t smem_gemm = 0, smem_csr = 0;
+  // per level: M2X items of the level's nodes, X2L half items whose targets
+  // are on the level; a stream per level runs them as soon as the level's
+  // multipoles exist (events order them against the up and down passes)
+  std::vector<int> m2x_first, m2x_count, xl_first, xl_count;
+  std::vector<cudaStream_t> lstreams;
+  std::vector<cudaEvent_t> ev_m, ev_x;
+  ~FmmState() {
+    for (cudaEvent_t e : ev_m) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_x) cudaEventDestroy(e);
+    for (cudaStream_t t : lstreams) cudaStreamDestroy(t);
+  }
 };
 
 void fmm_destroy(FmmState* s) { delete s; }
@@ -1224,7 +1368,7 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
   size_t o_rot = putT(rot), o_sfac = putT(G.scale_factors), o_w = putT(LT[0].weights), o_nf = putI(LT[0].numfour);
   std::vector<int> numphys, nexptot, nexptotp, fe_off, fo_off, fb_off;
   std::vector<double> scale, betascal, rlsc, zs, mps, lcs;
-  std::vector<cplx> fexpe, fexpo, fexpback, xs, ys;
+  std::vector<cplx> fexpe, fexpo, fexpback, xs, ys, tcomb;
   for (auto& t : LT) {
     numphys.insert(numphys.end(), t.numphys.begin(), t.numphys.end());
     nexptot.push_back(t.nexptot);
@@ -1248,6 +1392,36 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
     }
     mps.insert(mps.end(), t.mpshift.begin(), t.mpshift.end());
     lcs.insert(lcs.end(), t.lcshift.begin(), t.lcshift.end());
+    // translate_up/down_wave factor of every (up, a, b, c) offset combo:
+    // up: zs[c] ys[b] xs[a] (conjugated factors for negative offsets),
+    // down: zs[-c] with the conjugations reversed
+    for (int combo = 0; combo < kCombos; ++combo) {
+      const int up = combo / 343, a = (combo / 49) % 7 - 3, b = (combo / 7) % 7 - 3, c = combo % 7 - 3;
+      for (int i = 0; i < npm; ++i) {
+        if (i >= t.nexptotp) {
+          tcomb.push_back(cplx(0));
+          continue;
+        }
+        auto X = [&](int k) { return t.xs[(size_t)(k - 1) * t.nexptotp + i]; };
+        auto Y = [&](int k) { return t.ys[(size_t)(k - 1) * t.nexptotp + i]; };
+        auto Z = [&](int k) { return t.zs[(size_t)(k - 1) * t.nexptotp + i]; };
+        cplx f;
+        if (up) {
+          f = cplx(c > 0 ? Z(c) : 1.0, 0.0);
+          if (b > 0) f *= Y(b);
+          else if (b < 0) f *= std::conj(Y(-b));
+          if (a > 0) f *= X(a);
+          else if (a < 0) f *= std::conj(X(-a));
+        } else {
+          f = cplx(c < 0 ? Z(-c) : 1.0, 0.0);
+          if (b > 0) f *= std::conj(Y(b));
+          else if (b < 0) f *= Y(-b);
+          if (a > 0) f *= std::conj(X(a));
+          else if (a < 0) f *= X(-a);
+        }
+        tcomb.push_back(f);
+      }
+    }
   }
   if (fexpe.empty()) fexpe.push_back(0);
   if (fexpo.empty()) fexpo.push_back(0);
@@ -1255,7 +1429,7 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
          o_bs = putT(betascal), o_beta = putT(std::vector<double>{beta, P.params.beta0}), o_rl = putT(rlsc),
          o_fe = putC(fexpe), o_fo = putC(fexpo), o_fb = putC(fexpback), o_feo = putI(fe_off), o_foo = putI(fo_off),
          o_fbo = putI(fb_off), o_xs = putC(xs), o_ys = putC(ys), o_zs = putT(zs), o_mps = putT(mps),
-         o_lcs = putT(lcs);
+         o_lcs = putT(lcs), o_tc = putC(tcomb);
   S.tables_buf.alloc(P.ctx, blob.size());
   BP_CUDA(cudaMemcpyAsync(S.tables_buf.get(), blob.data(), blob.size(), cudaMemcpyHostToDevice, P.ctx->stream));
   BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
@@ -1287,6 +1461,7 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
   tb.zs = reinterpret_cast<const T*>(base + o_zs);
   tb.mpshift = reinterpret_cast<const T*>(base + o_mps);
   tb.lcshift = reinterpret_cast<const T*>(base + o_lcs);
+  tb.tcomb = reinterpret_cast<const C*>(base + o_tc);
   for (auto& t : LT)
     if (t.nexptot > 64) throw std::invalid_argument("FMM order with more than 64 Fourier modes is not supported");
 }
@@ -1294,10 +1469,12 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
 }  // namespace
 
 
+// Tabulates the operator form of M2M / L2L (one dense R x R matrix per
+// kind, level, screening group and octant, R = 2E reals) and of the L2P
+// preparation (one sparse matrix per leaf level) by applying the structured
+// kernels to unit vectors.
 template <typename T>
-static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const std::vector<ShiftItem>& m2m,
-                            const std::vector<ShiftChild>& m2m_ch, const std::vector<ShiftItem>& l2l,
-                            const std::vector<ShiftChild>& l2l_ch, const std::vector<LeafItem>& leaves) {
+static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const std::vector<LeafItem>& leaves) {
   using C = typename C2T<T>::type;
   Ctx* c = P.ctx;
   cudaStream_t st = c->stream;
@@ -1305,44 +1482,9 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   const int EQ = (NT + 3) * (NT + 4) / 2;
   // shifts: kind 0 = M2M (level = child level), kind 1 = L2L (level = parent level)
   const int n_ops = 2 * nlev * 2 * 8;
-  S.shift_ops.alloc(c, sizeof(T) * (size_t)n_ops * R * R);
+  S.shift_ops.alloc(c, sizeof(T) * (size_t)n_ops * R * ((R + 3) & ~3));
   shift_basis_kernel<T><<<n_ops * R, 64, S.smem_shift, st>>>(tb, nlev, S.shift_ops.as<T>());
   BP_LAUNCH_CHECK();
-  auto op_base = [&](int kind, int level, int oct) { return ((kind * nlev + level) * 2) * 8 + oct - 1; };
-  std::vector<DenseShift> md, ld;
-  std::vector<DenseSrc> ms, ls;
-  S.m2m_dfirst.assign(nlev, 0);
-  S.m2m_dcount.assign(nlev, 0);
-  for (int lev = nlev - 1; lev >= 1; --lev) {
-    S.m2m_dfirst[lev] = (int)md.size();
-    for (int q = S.m2m_first[lev]; q < S.m2m_first[lev] + S.m2m_count[lev]; ++q) {
-      const ShiftItem& it = m2m[q];
-      DenseShift d{it.parent, (int)ms.size(), it.n_children};
-      for (int k = 0; k < it.n_children; ++k) {
-        const ShiftChild& ch = m2m_ch[it.first_child + k];
-        ms.push_back({ch.node, op_base(0, lev, ch.octant)});
-      }
-      md.push_back(d);
-    }
-    S.m2m_dcount[lev] = (int)md.size() - S.m2m_dfirst[lev];
-  }
-  S.l2l_dfirst.assign(nlev, 0);
-  S.l2l_dcount.assign(nlev, 0);
-  for (int lev = 0; lev < nlev - 1; ++lev) {
-    S.l2l_dfirst[lev] = (int)ld.size();
-    for (int q = S.l2l_first[lev]; q < S.l2l_first[lev] + S.l2l_count[lev]; ++q) {
-      const ShiftItem& it = l2l[q];
-      const ShiftChild& ch = l2l_ch[it.first_child];
-      ld.push_back({ch.node, (int)ls.size(), 1});
-      ls.push_back({it.parent, op_base(1, lev, ch.octant)});
-    }
-    S.l2l_dcount[lev] = (int)ld.size() - S.l2l_dfirst[lev];
-  }
-  S.m2m_dense = upload(c, md);
-  S.m2m_src = upload(c, ms);
-  S.l2l_dense = upload(c, ld);
-  S.l2l_src = upload(c, ls);
-  S.smem_dense = sizeof(T) * 8 * (size_t)R;
   // L2P preparation operator per level that holds leaves
   const int nb = kCh * R, rows = 8 * 2 * EQ;
   std::vector<int> levels_with_leaves(nlev, 0);
@@ -1390,6 +1532,12 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   BP_CUDA(cudaStreamSynchronize(st));
 }
 
+// Builds the FMM schedule of a problem.  Only work that can reach a result
+// is scheduled: X2L halves with at least one interaction, M2X of the nodes
+// that are translation sources, M2M / P2M of the nodes whose multipoles feed
+// one of those, L2L out of nodes whose locals can be non-zero.  Every local
+// expansion that is read is written in the same matvec (X2L or L2L assign
+// it) or is identically zero (set once here).
 void fmm_setup(Problem& P) {
   auto S = new FmmState();
   P.fmm.reset(S);
@@ -1402,6 +1550,7 @@ void fmm_setup(Problem& P) {
     fill_tables<double>(*S, P, S->tb_d);
   else
     fill_tables<float>(*S, P, S->tb_f);
+  if (S->np_max > kPairLanes) throw std::invalid_argument("FMM order too large for the plane-wave thread layout");
   const int nn = (int)T.nodes.size();
   const size_t celem = S->fp64 ? sizeof(double2) : sizeof(float2);
   const size_t exp_bytes = (size_t)nn * kCh * S->E * celem;
@@ -1410,104 +1559,147 @@ void fmm_setup(Problem& P) {
   BP_CUDA(cudaMemsetAsync(S->L.get(), 0, exp_bytes, P.ctx->stream));
   S->W.alloc(P.ctx, (size_t)nn * 6 * kCh * S->np_max * celem);
   BP_CUDA(cudaMemsetAsync(S->W.get(), 0, S->W.bytes(), P.ctx->stream));
+  const int nlev = S->nlev;
   auto flags = [&](int k) { return T.nodes[k].flags; };
   auto cnt = [&](int k) { return T.nodes[k].content_count; };
   auto octant = [&](int k) { return 1 + (T.nodes[k].ix & 1) + 2 * (T.nodes[k].iy & 1) + 4 * (T.nodes[k].iz & 1); };
+  // X2L: halves (targets 0-3, 4-7) of parents that are neither leaf nor
+  // shadow; entries per target sorted by direction
+  const auto table = interaction_table();
+  std::vector<std::vector<int>> by_target_dir(8 * 6);
+  for (int q = 0; q < (int)table.size(); ++q) by_target_dir[table[q].targ * 6 + table[q].dir].push_back(q);
+  std::vector<XlItem> xl;
+  std::vector<XlEntry> xle;
+  std::vector<char> is_source(nn, 0), written(nn, 0);
+  for (int k = 0; k < nn; ++k) {
+    const TreeNode& nd = T.nodes[k];
+    if (nd.level >= nlev - 1) continue;
+    if ((nd.flags & TREE_LEAF) || (nd.flags & TREE_SHADOW)) continue;
+    for (int half = 0; half < 2; ++half) {
+      XlItem it;
+      it.parent_level = nd.level;
+      int total = 0;
+      for (int tl = 0; tl < kXlTargets; ++tl) {
+        const int t = half * kXlTargets + tl;
+        const int ck = nd.children[t];
+        it.targets[tl] = (ck >= 0 && !(flags(ck) & TREE_SHADOW)) ? ck : -1;
+        it.first_entry[tl] = (int)xle.size();
+        it.n_entries[tl] = 0;
+        if (it.targets[tl] < 0) continue;
+        for (int dir = 0; dir < 6; ++dir)
+          for (int q : by_target_dir[t * 6 + dir]) {
+            const RawInteraction& r = table[q];
+            const int nbk = nd.neighbours[r.nb];
+            if (nbk < 0 || cnt(nbk) == 0) continue;
+            const int sk = T.nodes[nbk].children[r.src];
+            if (sk < 0 || cnt(sk) == 0) continue;
+            int a, b, c;
+            switch (r.dir) {
+              case 0: case 1: a = r.dx; b = r.dy; c = r.dz; break;
+              case 2: case 3: a = r.dz; b = r.dx; c = r.dy; break;
+              default: a = -r.dz; b = r.dy; c = r.dx; break;
+            }
+            const int up = r.dir % 2 == 0 ? 1 : 0;
+            XlEntry e;
+            e.src = sk;
+            e.combo = (short)(up * 343 + (a + 3) * 49 + (b + 3) * 7 + (c + 3));
+            e.dir = (signed char)r.dir;
+            e.pad = 0;
+            xle.push_back(e);
+            is_source[sk] = 1;
+          }
+        it.n_entries[tl] = (int)xle.size() - it.first_entry[tl];
+        total += it.n_entries[tl];
+      }
+      if (total == 0) {
+        xle.resize(it.first_entry[0]);
+        continue;
+      }
+      for (int tl = 0; tl < kXlTargets; ++tl) {
+        if (it.n_entries[tl] > kXlMaxEntries) throw std::logic_error("X2L target with too many interactions");
+        if (it.targets[tl] >= 0) written[it.targets[tl]] = 1;
+      }
+      xl.push_back(it);
+    }
+  }
+  // multipoles needed: translation sources and every node below one
+  // (nodes are stored level by level, parents first)
+  std::vector<char> mneed(nn, 0), lnz(nn, 0);
+  for (int k = 0; k < nn; ++k) {
+    const int p = T.nodes[k].parent;
+    mneed[k] = is_source[k] || (p >= 0 && mneed[p]);
+    lnz[k] = written[k] || (p >= 0 && lnz[p]);
+  }
   // P2M items
   std::vector<P2mItem> p2m;
+  int p2m_rows = 0;
   for (int k = 0; k < nn; ++k) {
-    if ((flags(k) & TREE_HAS_CHILDREN) || cnt(k) == 0) continue;
-    P2mItem it{k, T.nodes[k].level, (int)T.nodes[k].content_start, cnt(k), {0, 0, 0}};
+    if ((flags(k) & TREE_HAS_CHILDREN) || cnt(k) == 0 || !mneed[k]) continue;
+    P2mItem it{k, T.nodes[k].level, (int)T.nodes[k].content_start, cnt(k), p2m_rows, {0, 0, 0}};
     for (int d = 0; d < 3; ++d) it.c[d] = T.nodes[k].centre[d];
     p2m.push_back(it);
+    p2m_rows += cnt(k);
   }
-  // M2M per child level: parents with non-empty children
-  std::vector<ShiftItem> m2m;
-  std::vector<ShiftChild> m2m_ch;
-  S->m2m_first.assign(S->nlev, 0);
-  S->m2m_count.assign(S->nlev, 0);
-  for (int lev = S->nlev - 1; lev >= 1; --lev) {
-    S->m2m_first[lev] = (int)m2m.size();
+  auto op_base = [&](int kind, int level, int oct) { return ((kind * nlev + level) * 2) * 8 + oct - 1; };
+  // M2M / L2L tiles: columns bucketed by (octant, screening group) so that
+  // a tile shares one operator; M2M columns write partial slots
+  std::vector<ShiftTile> tiles;
+  std::vector<ShiftCol> tcols;
+  std::vector<ShiftReduce> reds;
+  auto add_bucket = [&](int op, const std::vector<ShiftCol>& bucket) {
+    for (size_t b0 = 0; b0 < bucket.size(); b0 += kTileCols) {
+      ShiftTile t{op, (int)tcols.size(), (int)std::min<size_t>(kTileCols, bucket.size() - b0)};
+      tcols.insert(tcols.end(), bucket.begin() + b0, bucket.begin() + b0 + t.n_cols);
+      tiles.push_back(t);
+    }
+  };
+  S->m2m_tfirst.assign(nlev, 0);
+  S->m2m_tcount.assign(nlev, 0);
+  S->m2m_rfirst.assign(nlev, 0);
+  S->m2m_rcount.assign(nlev, 0);
+  int n_slots = 0;
+  for (int lev = nlev - 1; lev >= 1; --lev) {
+    std::vector<std::vector<ShiftCol>> bucket(16);  // [group][octant-1]
+    S->m2m_rfirst[lev] = (int)reds.size();
     for (int k = T.level_start[lev - 1]; k < T.level_start[lev]; ++k) {
-      if (!(flags(k) & TREE_HAS_CHILDREN) || cnt(k) == 0) continue;
-      ShiftItem it{k, (int)m2m_ch.size(), 0};
+      if (!(flags(k) & TREE_HAS_CHILDREN) || cnt(k) == 0 || !mneed[k]) continue;
+      ShiftReduce r{k, n_slots, 0};
       for (int c = 0; c < 8; ++c) {
         const int ck = T.nodes[k].children[c];
         if (ck < 0 || cnt(ck) == 0) continue;
-        m2m_ch.push_back(ShiftChild{ck, (int)octant(ck)});
-        it.n_children++;
+        const int oct = octant(ck), slot = n_slots + r.n_slots++;
+        for (int ch = 0; ch < kCh; ++ch) bucket[(ch >= 8 ? 8 : 0) + oct - 1].push_back({ck, slot, ch, 0});
       }
-      if (it.n_children) m2m.push_back(it);
+      if (r.n_slots) {
+        reds.push_back(r);
+        n_slots += r.n_slots;
+      }
     }
-    S->m2m_count[lev] = (int)m2m.size() - S->m2m_first[lev];
+    S->m2m_rcount[lev] = (int)reds.size() - S->m2m_rfirst[lev];
+    S->m2m_tfirst[lev] = (int)tiles.size();
+    for (int b = 0; b < 16; ++b) add_bucket(op_base(0, lev, b % 8 + 1) + (b >= 8 ? 8 : 0), bucket[b]);
+    S->m2m_tcount[lev] = (int)tiles.size() - S->m2m_tfirst[lev];
   }
-  // M2X items: non-empty nodes below the root
+  // M2X items: translation sources
   std::vector<M2xItem> m2x;
   for (int k = 0; k < nn; ++k)
-    if (T.nodes[k].level >= 1 && cnt(k) > 0) m2x.push_back({k, T.nodes[k].level});
-  // X2L: parents neither leaf nor shadow, levels 0..bottom-1
-  const auto table = interaction_table();
-  std::vector<XlItem> xl;
-  std::vector<XlEntry> xle;
-  for (int k = 0; k < nn; ++k) {
-    const TreeNode& nd = T.nodes[k];
-    if (nd.level >= S->nlev - 1) continue;
-    if ((nd.flags & TREE_LEAF) || (nd.flags & TREE_SHADOW)) continue;
-    XlItem it;
-    it.parent_level = nd.level;
-    bool any_target = false;
-    for (int c = 0; c < 8; ++c) {
-      const int ck = nd.children[c];
-      it.targets[c] = (ck >= 0 && !(flags(ck) & TREE_SHADOW)) ? ck : -1;
-      any_target |= it.targets[c] >= 0;
-    }
-    if (!any_target) continue;
-    for (int pair = 0; pair < 3; ++pair) {
-      it.first_entry[pair] = (int)xle.size();
-      for (const RawInteraction& r : table) {
-        if (r.dir / 2 != pair) continue;
-        if (it.targets[r.targ] < 0) continue;
-        const int nbk = nd.neighbours[r.nb];
-        if (nbk < 0 || cnt(nbk) == 0) continue;
-        const int sk = T.nodes[nbk].children[r.src];
-        if (sk < 0 || cnt(sk) == 0) continue;
-        XlEntry e;
-        e.src = sk;
-        e.dir = (signed char)r.dir;
-        e.targ = (signed char)r.targ;
-        int a, b, c;
-        switch (r.dir) {
-          case 0: case 1: a = r.dx; b = r.dy; c = r.dz; break;
-          case 2: case 3: a = r.dz; b = r.dx; c = r.dy; break;
-          default: a = -r.dz; b = r.dy; c = r.dx; break;
-        }
-        e.a = (signed char)a;
-        e.b = (signed char)b;
-        e.c = (signed char)c;
-        e.up = (r.dir % 2 == 0) ? 1 : 0;
-        xle.push_back(e);
-      }
-      it.n_entries[pair] = (int)xle.size() - it.first_entry[pair];
-    }
-    xl.push_back(it);
-  }
-  // L2L per parent level: one item per (parent, child)
-  std::vector<ShiftItem> l2l;
-  std::vector<ShiftChild> l2l_ch;
-  S->l2l_first.assign(S->nlev, 0);
-  S->l2l_count.assign(S->nlev, 0);
-  for (int lev = 0; lev < S->nlev - 1; ++lev) {
-    S->l2l_first[lev] = (int)l2l.size();
+    if (is_source[k]) m2x.push_back({k, T.nodes[k].level});
+  // L2L per parent level, top-down: child (= or +=) shift(parent)
+  S->l2l_tfirst.assign(nlev, 0);
+  S->l2l_tcount.assign(nlev, 0);
+  for (int lev = 0; lev < nlev - 1; ++lev) {
+    std::vector<std::vector<ShiftCol>> bucket(16);
     for (int k = T.level_start[lev]; k < T.level_start[lev + 1]; ++k) {
-      if (!(flags(k) & TREE_HAS_CHILDREN) || (flags(k) & TREE_LEAF)) continue;
+      if (!(flags(k) & TREE_HAS_CHILDREN) || (flags(k) & TREE_LEAF) || !lnz[k]) continue;
       for (int c = 0; c < 8; ++c) {
         const int ck = T.nodes[k].children[c];
         if (ck < 0 || cnt(ck) == 0 || (flags(ck) & TREE_SHADOW)) continue;
-        l2l.push_back({k, (int)l2l_ch.size(), 1});
-        l2l_ch.push_back({ck, c + 1});
+        for (int ch = 0; ch < kCh; ++ch) bucket[(ch >= 8 ? 8 : 0) + c].push_back({k, ck, ch, written[ck] ? 1 : 0});
       }
     }
-    S->l2l_count[lev] = (int)l2l.size() - S->l2l_first[lev];
+    S->l2l_tfirst[lev] = (int)tiles.size();
+    for (int b = 0; b < 16; ++b) add_bucket(op_base(1, lev, b % 8 + 1) + (b >= 8 ? 8 : 0), bucket[b]);
+    S->l2l_tcount[lev] = (int)tiles.size() - S->l2l_tfirst[lev];
   }
   // leaves
   std::vector<LeafItem> leaves, evals;
@@ -1526,62 +1718,112 @@ void fmm_setup(Problem& P) {
   Ctx* c = P.ctx;
   S->p2m_items = upload(c, p2m);
   S->n_p2m = (int)p2m.size();
-  S->m2m_items = upload(c, m2m);
-  S->m2m_children = upload(c, m2m_ch);
   S->m2x_items = upload(c, m2x);
   S->n_m2x = (int)m2x.size();
   S->xl_items = upload(c, xl);
   S->xl_entries = upload(c, xle);
   S->n_xl = (int)xl.size();
-  S->l2l_items = upload(c, l2l);
-  S->l2l_children = upload(c, l2l_ch);
+  S->m2x_first.assign(nlev, 0);
+  S->m2x_count.assign(nlev, 0);
+  S->xl_first.assign(nlev, 0);
+  S->xl_count.assign(nlev, 0);
+  for (int q = (int)m2x.size() - 1; q >= 0; --q) {
+    S->m2x_first[m2x[q].level] = q;
+    S->m2x_count[m2x[q].level]++;
+  }
+  for (int q = (int)xl.size() - 1; q >= 0; --q) {
+    S->xl_first[xl[q].parent_level + 1] = q;
+    S->xl_count[xl[q].parent_level + 1]++;
+  }
+  for (int lev = 0; lev < nlev; ++lev) {
+    for (int q = S->m2x_first[lev]; q < S->m2x_first[lev] + S->m2x_count[lev]; ++q)
+      if (m2x[q].level != lev) throw std::logic_error("M2X items are not grouped by level");
+    for (int q = S->xl_first[lev]; q < S->xl_first[lev] + S->xl_count[lev]; ++q)
+      if (xl[q].parent_level + 1 != lev) throw std::logic_error("X2L items are not grouped by level");
+  }
+  S->lstreams.assign(nlev, nullptr);
+  S->ev_m.assign(nlev, nullptr);
+  S->ev_x.assign(nlev, nullptr);
+  for (int lev = 0; lev < nlev; ++lev) {
+    BP_CUDA(cudaStreamCreateWithFlags(&S->lstreams[lev], cudaStreamNonBlocking));
+    BP_CUDA(cudaEventCreateWithFlags(&S->ev_m[lev], cudaEventDisableTiming));
+    BP_CUDA(cudaEventCreateWithFlags(&S->ev_x[lev], cudaEventDisableTiming));
+  }
+  S->shift_tiles = upload(c, tiles);
+  S->shift_cols = upload(c, tcols);
+  S->m2m_reduce = upload(c, reds);
+  S->m2m_partials.alloc(c, celem * kCh * (size_t)S->E * std::max(1, n_slots));
   S->leaf_items = upload(c, leaves);
   S->n_leaf = (int)leaves.size();
   S->eval_items = upload(c, evals);
   S->n_eval = (int)evals.size();
-  // contents on the device (node-major patch lists)
   const int E = S->E, NT = S->nt;
-  S->smem_p2m = celem * 2 * kP2mChunk * E + (S->fp64 ? 8 : 4) * kP2mChunk * kCh;
+  if (E > kPairLanes) throw std::invalid_argument("FMM order above 9 is not supported");
   S->smem_shift = 4 * celem * E;
-  S->smem_m2x = celem * (2 * E + 128);
-  S->smem_xl = celem * (6 * 8 * (size_t)S->np_max + 3 * 2 * 64 + 6 * E);
-  if (S->np_max > kXlGroup) throw std::invalid_argument("FMM order too large for the X2L thread layout");
-  const int EQ = (NT + 3) * (NT + 4) / 2, EG = (NT + 2) * (NT + 3) / 2;
+  S->smem_gemm = (S->fp64 ? 8 : 4) * (size_t)(2 * E) * (((2 * E + 3) & ~3) + kTileCols);
+  S->smem_m2x = celem * (size_t)(4 * kM2xChannels * E + 6 * kM2xChannels * 64);
+  const int xcb = S->fp64 ? XlChannels<double>::value : XlChannels<float>::value;
+  S->smem_xl = celem * (size_t)kXlTargets * 6 * xcb * (S->np_max + 64) + sizeof(XlEntry) * kXlTargets * kXlMaxEntries;
+  const int EQ = (NT + 3) * (NT + 4) / 2;
   S->smem_prep = celem * 2 * 24 * (size_t)EQ;
-  S->smem_eval = celem * 8 * (size_t)EQ;
+  S->smem_eval = celem * 8 * (size_t)EQ + (S->fp64 ? 8 : 4) * (size_t)16 * kEvalChunk;
   S->leaf_exp.alloc(P.ctx, celem * 8 * (size_t)EQ * std::max(1, S->n_leaf));
-  (void)EG;
-  auto attr = [&](const void* fn, size_t bytes) {
-    ensure_dynamic_smem(fn, bytes);
-  };
-  if (S->fp64) {
-    attr((const void*)p2m_kernel<double>, S->smem_p2m);
-    attr((const void*)m2m_kernel<double>, S->smem_shift);
-    attr((const void*)l2l_kernel<double>, S->smem_shift);
-    attr((const void*)m2x_kernel<double>, S->smem_m2x);
-    attr((const void*)x2l_kernel<double>, S->smem_xl);
-    attr((const void*)l2p_prep_kernel<double>, S->smem_prep);
-    attr((const void*)l2p_eval_kernel<double>, S->smem_eval);
-  } else {
-    attr((const void*)p2m_kernel<float>, S->smem_p2m);
-    attr((const void*)m2m_kernel<float>, S->smem_shift);
-    attr((const void*)l2l_kernel<float>, S->smem_shift);
-    attr((const void*)m2x_kernel<float>, S->smem_m2x);
-    attr((const void*)x2l_kernel<float>, S->smem_xl);
-    attr((const void*)l2p_prep_kernel<float>, S->smem_prep);
-    attr((const void*)l2p_eval_kernel<float>, S->smem_eval);
-  }
-  if (S->smem_xl > 227 * 1024 || S->smem_prep > 227 * 1024)
+  S->p2m_basis.alloc(P.ctx, celem * 2 * (size_t)E * std::max(1, p2m_rows));
+  S->eval_basis.alloc(P.ctx, celem * 2 * (size_t)EQ * kEvalChunk * std::max(1, S->n_eval));
+  if (S->smem_xl > 227 * 1024 || S->smem_prep > 227 * 1024 || S->smem_m2x > 227 * 1024 ||
+      S->smem_gemm > 227 * 1024)
     throw std::invalid_argument("FMM order too large for the shared-memory layout");
+  if (S->fp64) {
+    ensure_dynamic_smem((const void*)m2x_kernel<double>, S->smem_m2x);
+    ensure_dynamic_smem((const void*)x2l_kernel<double>, S->smem_xl);
+    ensure_dynamic_smem((const void*)shift_gemm_kernel<double>, S->smem_gemm);
+    ensure_dynamic_smem((const void*)l2p_prep_kernel<double>, S->smem_prep);
+    ensure_dynamic_smem((const void*)l2p_eval_kernel<double>, S->smem_eval);
+  } else {
+    ensure_dynamic_smem((const void*)m2x_kernel<float>, S->smem_m2x);
+    ensure_dynamic_smem((const void*)x2l_kernel<float>, S->smem_xl);
+    ensure_dynamic_smem((const void*)shift_gemm_kernel<float>, S->smem_gemm);
+    ensure_dynamic_smem((const void*)l2p_prep_kernel<float>, S->smem_prep);
+    ensure_dynamic_smem((const void*)l2p_eval_kernel<float>, S->smem_eval);
+  }
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
   BP_CUDA(cudaStreamSynchronize(c->stream));
   if (S->fp64)
-    build_operators<double>(P, *S, S->tb_d, m2m, m2m_ch, l2l, l2l_ch, leaves);
+    build_operators<double>(P, *S, S->tb_d, leaves);
   else
-    build_operators<float>(P, *S, S->tb_f, m2m, m2m_ch, l2l, l2l_ch, leaves);
+    build_operators<float>(P, *S, S->tb_f, leaves);
+  // geometry-only bases of P2M and of the L2P evaluation
+  const double* cen = P.d_centroid.as<double>();
+  if (S->fp64) {
+    if (S->n_p2m)
+      p2m_basis_kernel<double><<<S->n_p2m, 64, 0, c->stream>>>(S->tb_d, S->p2m_items.as<P2mItem>(),
+                                                               P.fmm_contents.as<int32_t>(), cen,
+                                                               S->p2m_basis.as<double2>());
+    if (S->n_eval)
+      l2p_basis_kernel<double><<<S->n_eval, kEvalChunk, 0, c->stream>>>(S->tb_d, S->eval_items.as<LeafItem>(),
+                                                                         P.fmm_contents.as<int32_t>(), cen,
+                                                                         S->eval_basis.as<double2>());
+  } else {
+    if (S->n_p2m)
+      p2m_basis_kernel<float><<<S->n_p2m, 64, 0, c->stream>>>(S->tb_f, S->p2m_items.as<P2mItem>(),
+                                                              P.fmm_contents.as<int32_t>(), cen,
+                                                              S->p2m_basis.as<float2>());
+    if (S->n_eval)
+      l2p_basis_kernel<float><<<S->n_eval, kEvalChunk, 0, c->stream>>>(S->tb_f, S->eval_items.as<LeafItem>(),
+                                                                        P.fmm_contents.as<int32_t>(), cen,
+                                                                        S->eval_basis.as<float2>());
+  }
+  BP_LAUNCH_CHECK();
+  BP_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+// One FMM pass.  With st == nullptr the levels overlap: the upward chain
+// (P2M, M2M level by level) and the downward chain (L2L, L2P) run on the
+// FMM stream, and each level's M2X + X2L runs on its own stream as soon as
+// that level's multipoles are complete; L2L into a level waits for the
+// level's X2L.  With st != nullptr (stage profiling) everything runs in
+// order on one stream.
 template <typename T>
 static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* x, double* y, StageTimes* st,
                     cudaStream_t s) {
@@ -1590,79 +1832,103 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   C* Lx = S.L.as<C>();
   C* W = S.W.as<C>();
   const int32_t* contents = P.fmm_contents.as<int32_t>();
-  auto begin = [&](int stage) {
-    if (st) st->begin(stage, s);
+  const bool overlap = st == nullptr;
+  auto begin = [&](int stage, cudaStream_t q) {
+    if (st) st->begin(stage, q);
   };
   auto end = [&](int launches) {
     if (st) st->end(launches);
   };
-  if (S.n_p2m == 0 || S.n_m2x == 0 || S.n_xl == 0 || S.n_leaf == 0)
-    throw std::runtime_error("inconsistent FMM schedule (empty stage)");
-  begin(1);
-  p2m_kernel<T><<<S.n_p2m, 256, S.smem_p2m, s>>>(tb, S.p2m_items.as<P2mItem>(), contents, P.d_centroid.as<double>(),
-                                                 P.d_area.as<double>(), P.d_normal.as<double>(), P.d_eps.as<double>(),
-                                                 x, P.n, M);
-  BP_LAUNCH_CHECK();
-  end(1);
-  begin(2);
-  int l_m2m = 0;
-  for (int lev = S.nlev - 1; lev >= 1; --lev) {
-    if (S.use_operators) {
-      if (!S.m2m_dcount[lev]) continue;
-      dense_shift_kernel<T><<<S.m2m_dcount[lev] * kCh, 128, S.smem_dense, s>>>(
-          S.E, S.m2m_dense.as<DenseShift>() + S.m2m_dfirst[lev], S.m2m_src.as<DenseSrc>(), S.shift_ops.as<T>(),
-          reinterpret_cast<const T*>(M), reinterpret_cast<T*>(M), 0);
-    } else {
-      if (!S.m2m_count[lev]) continue;
-      m2m_kernel<T><<<S.m2m_count[lev] * kCh, 64, S.smem_shift, s>>>(
-          tb, S.m2m_items.as<ShiftItem>() + S.m2m_first[lev], S.m2m_children.as<ShiftChild>(), lev, M);
+  if (S.n_leaf == 0) throw std::runtime_error("inconsistent FMM schedule (no leaves)");
+  const int nlev = S.nlev;
+  auto has_x = [&](int lev) { return S.m2x_count[lev] > 0 || S.xl_count[lev] > 0; };
+  // M2X and X2L of one level on stream q
+  auto level_x = [&](int lev, cudaStream_t q) {
+    if (S.m2x_count[lev]) {
+      begin(3, q);
+      m2x_kernel<T><<<S.m2x_count[lev] * (kCh / kM2xChannels), kM2xThreads, S.smem_m2x, q>>>(
+          tb, S.m2x_items.as<M2xItem>() + S.m2x_first[lev], M, W);
+      BP_LAUNCH_CHECK();
+      end(1);
     }
-    BP_LAUNCH_CHECK();
-    ++l_m2m;
-  }
-  end(l_m2m);
-  begin(3);
-  m2x_kernel<T><<<S.n_m2x * kCh, kM2xThreads, S.smem_m2x, s>>>(tb, S.m2x_items.as<M2xItem>(), M, W);
-  BP_LAUNCH_CHECK();
-  end(1);
-  begin(4);
-  x2l_kernel<T><<<S.n_xl * kCh, kXlThreads, S.smem_xl, s>>>(tb, S.xl_items.as<XlItem>(),
-                                                                     S.xl_entries.as<XlEntry>(), W, Lx);
-  BP_LAUNCH_CHECK();
-  end(1);
-  begin(6);
-  int l_l2l = 0;
-  for (int lev = 0; lev < S.nlev - 1; ++lev) {
-    if (S.use_operators) {
-      if (!S.l2l_dcount[lev]) continue;
-      dense_shift_kernel<T><<<S.l2l_dcount[lev] * kCh, 128, S.smem_dense, s>>>(
-          S.E, S.l2l_dense.as<DenseShift>() + S.l2l_dfirst[lev], S.l2l_src.as<DenseSrc>(), S.shift_ops.as<T>(),
-          reinterpret_cast<const T*>(Lx), reinterpret_cast<T*>(Lx), 1);
-    } else {
-      if (!S.l2l_count[lev]) continue;
-      l2l_kernel<T><<<S.l2l_count[lev] * kCh, 64, S.smem_shift, s>>>(
-          tb, S.l2l_items.as<ShiftItem>() + S.l2l_first[lev], S.l2l_children.as<ShiftChild>(), lev, Lx);
+    if (S.xl_count[lev]) {
+      constexpr int xcb = XlChannels<T>::value;
+      begin(4, q);
+      x2l_kernel<T><<<S.xl_count[lev] * (kCh / xcb), kXlThreads, S.smem_xl, q>>>(
+          tb, S.xl_items.as<XlItem>() + S.xl_first[lev], S.xl_entries.as<XlEntry>(), W, Lx);
+      BP_LAUNCH_CHECK();
+      end(1);
     }
+  };
+  auto fork_x = [&](int lev) {
+    if (!has_x(lev)) return;
+    if (!overlap) {
+      level_x(lev, s);
+      return;
+    }
+    BP_CUDA(cudaEventRecord(S.ev_m[lev], s));
+    BP_CUDA(cudaStreamWaitEvent(S.lstreams[lev], S.ev_m[lev], 0));
+    level_x(lev, S.lstreams[lev]);
+    BP_CUDA(cudaEventRecord(S.ev_x[lev], S.lstreams[lev]));
+  };
+  auto join_x = [&](int lev) {
+    if (overlap && has_x(lev)) BP_CUDA(cudaStreamWaitEvent(s, S.ev_x[lev], 0));
+  };
+  // upward pass
+  begin(1, s);
+  int l_p2m = 0;
+  if (S.n_p2m) {
+    p2m_kernel<T><<<S.n_p2m, 128, 0, s>>>(S.p2m_items.as<P2mItem>(), S.E, contents, P.d_area.as<double>(),
+                                          P.d_normal.as<double>(), P.d_eps.as<double>(), x, P.n,
+                                          S.p2m_basis.as<C>(), M);
     BP_LAUNCH_CHECK();
-    ++l_l2l;
+    ++l_p2m;
   }
-  end(l_l2l);
-  begin(5);
-  if (S.use_operators) {
+  end(l_p2m);
+  T* Mr = reinterpret_cast<T*>(M);
+  T* Pr = S.m2m_partials.as<T>();
+  for (int lev = nlev - 1; lev >= 0; --lev) {
+    // multipoles of level lev are complete once its children's are shifted in
+    if (lev + 1 < nlev && S.m2m_tcount[lev + 1]) {
+      begin(2, s);
+      shift_gemm_kernel<T><<<S.m2m_tcount[lev + 1], kGemmThreads, S.smem_gemm, s>>>(
+          S.E, S.shift_tiles.as<ShiftTile>() + S.m2m_tfirst[lev + 1], S.shift_cols.as<ShiftCol>(),
+          S.shift_ops.as<T>(), Mr, Pr);
+      BP_LAUNCH_CHECK();
+      shift_reduce_kernel<T><<<S.m2m_rcount[lev + 1], 256, 0, s>>>(
+          S.E, S.m2m_reduce.as<ShiftReduce>() + S.m2m_rfirst[lev + 1], Pr, Mr);
+      BP_LAUNCH_CHECK();
+      end(2);
+    }
+    fork_x(lev);
+  }
+  // downward pass: locals of level lev + 1 = X2L result (+) L2L of level lev
+  for (int lev = 0; lev < nlev - 1; ++lev) {
+    if (!S.l2l_tcount[lev]) continue;
+    join_x(lev);
+    join_x(lev + 1);
+    begin(6, s);
+    shift_gemm_kernel<T><<<S.l2l_tcount[lev], kGemmThreads, S.smem_gemm, s>>>(
+        S.E, S.shift_tiles.as<ShiftTile>() + S.l2l_tfirst[lev], S.shift_cols.as<ShiftCol>(), S.shift_ops.as<T>(),
+        reinterpret_cast<const T*>(Lx), reinterpret_cast<T*>(Lx));
+    BP_LAUNCH_CHECK();
+    end(1);
+  }
+  for (int lev = 0; lev < nlev; ++lev) join_x(lev);  // every level stream rejoins the FMM stream
+  begin(5, s);
+  {
     const int NT = S.nt, EQ = (NT + 3) * (NT + 4) / 2;
     prep_csr_kernel<T><<<S.n_leaf, 256, S.smem_csr, s>>>(S.E, EQ, S.leaf_items.as<LeafItem>(), S.prep_rowptr.as<int>(),
                                                           S.prep_cols.as<int>(), S.prep_vals.as<T>(),
                                                           reinterpret_cast<const T*>(Lx),
                                                           reinterpret_cast<T*>(S.leaf_exp.as<C>()));
-  } else {
-    l2p_prep_kernel<T><<<S.n_leaf, 64, S.smem_prep, s>>>(tb, S.leaf_items.as<LeafItem>(), Lx, S.leaf_exp.as<C>());
+    BP_LAUNCH_CHECK();
   }
-  BP_LAUNCH_CHECK();
   end(1);
-  begin(7);
-  l2p_eval_kernel<T><<<S.n_eval, kEvalChunk, S.smem_eval, s>>>(tb, S.eval_items.as<LeafItem>(), contents,
-                                                        P.d_centroid.as<double>(), P.d_normal.as<double>(),
-                                                        S.leaf_exp.as<C>(), P.n, y);
+  begin(7, s);
+  l2p_eval_kernel<T><<<S.n_eval, kEvalThreads, S.smem_eval, s>>>(S.nt, S.eval_items.as<LeafItem>(), contents,
+                                                                P.d_normal.as<double>(), S.leaf_exp.as<C>(),
+                                                                S.eval_basis.as<C>(), P.n, y);
   BP_LAUNCH_CHECK();
   end(1);
 }

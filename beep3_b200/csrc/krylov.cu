@@ -155,6 +155,9 @@ void ensure_dynamic_smem(const void* kernel, size_t bytes) {
   size_t& cur = granted[{dev, kernel}];
   if (bytes <= cur) return;
   BP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // kernels with this much shared memory run more blocks per SM with the
+  // largest shared-memory carveout
+  BP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   cur = bytes;
 }
 
