@@ -5,26 +5,33 @@
 // Channels (src/bem/node_patch.h:339-394): with a = patch area, n its normal,
 // eps the dielectric ratio, charges [a f n, a h] and [a f n/eps, a h/eps]
 // are screened with kappa (channels 0-7), [a f n/eps, a h] with beta0 = 1e-10
-// (channels 8-11, standing in for Laplace).  Each matvec runs:
-//   P2M   one launch for all non-empty childless nodes (yformmp)
-//   M2M   one launch per level, bottom-up, one block per parent gathering its
-//         children (ympshift: rotate, z-shift, rotate back)
-//   M2X   one launch for all non-empty nodes below the root: multipole ->
-//         6 directional plane waves (rotate z->y / z->x, ympoletoexp,
-//         yftophys), with the parent level's tables
-//   X2L   one launch for all parents that are neither leaf nor shadow: the
-//         diagonal plane-wave translations of the 1512-entry interaction list
-//         (translate_up/down_wave) accumulated in shared memory per target
-//         child, then converted to local expansions (yphystof,
-//         yexptolocal, rotate back) -- translation and conversion fused, no
-//         accumulator ever goes to HBM
-//   L2L   one launch per level, top-down (ylcshift)
-//   L2P   one launch over leaves: potential, field and Hessian of the 12
-//         local expansions at each patch centroid, reduced on the fly to the
-//         f and h results of FMM_results_to_BEM (src/bem/bem_kernels.cpp:12-121)
-// Precision: T = double (FP64 engine) or float (mixed engine); tables are
-// computed on the host in FP64 (fmm_tables.cpp) and rounded to T.
-// Expansions are stored [node][channel][tri(n, m)] as complex T; plane waves
+// (channels 8-11, standing in for Laplace).
+//
+// Every stage that is a fixed linear map runs as a dense or sparse operator
+// tabulated once per problem by applying the structured kernels of the
+// reference's operators (ympshift / ylcshift, ympoletoexp + yftophys,
+// yphystof + yexptolocal + rotations, the L2P derivative ladders) to unit
+// vectors; geometry-only bases (P2M, L2P) are tabulated the same way.  Each
+// matvec then runs:
+//   P2M   basis x charges, one block per childless node (yformmp)
+//   M2M   per level: gather-GEMM of the children through their octant's
+//         110 x 110 shift operator into per-child partials, then the partials
+//         of each parent summed in child order
+//   M2X   per level: gather-GEMM of the sources' multipoles through the
+//         684 x 110 multipole -> 6 plane-wave operator of the parent level
+//   X2L   per level: diagonal translations of each target's interaction list
+//         (translate_up/down_wave, factors tabulated per offset) summed per
+//         direction, then the 110 x 684 wave -> local GEMM
+//   L2L   per level: gather-GEMM of the parents through the child octant's
+//         shift operator, added to (or assigned) the child's locals
+//   L2P   sparse derivative-expansion operator per leaf, then q(n, m) of each
+//         target contracted with them (FMM_results_to_BEM,
+//         src/bem/bem_kernels.cpp:12-121)
+// M2X + X2L of a level run on the level's own stream as soon as its
+// multipoles exist.  Work that cannot reach a result is not scheduled.
+// Precision: T = double (FP64 engine) or float (mixed engine); tables and
+// operators are computed in FP64 and rounded to T.  Expansions are stored
+// [node][channel][tri(n, m)] as complex T; plane waves
 // [node][direction][channel][i].
 #include <cuda_runtime.h>
 
@@ -538,12 +545,17 @@ __global__ void __launch_bounds__(kM2xThreads) m2x_kernel(const __grid_constant_
 }
 
 // ---------------------------------------------------------------- X2L
-// Half of a parent's interaction list: up to 4 target children, each with
-// its entries sorted by direction (within a direction in table order).
-struct XlItem {
-  int parent_level;
-  int targets[4];  // target child node ids (-1 absent)
-  int first_entry[4], n_entries[4];
+// X2L is split in two.  xl_translate_kernel applies the diagonal plane-wave
+// translations (translate_up/down_wave) of every target's interaction list
+// and leaves, per (target, channel), the six accumulated waves as 6 x 2NPM
+// reals in the ACC scratch.  The conversion of those waves to a local
+// expansion (yphystof, yexptolocal, rotate_ytoz / rotate_ztox back, sum of
+// the three direction pairs) is R-linear and fixed per (level, screening
+// group): it is tabulated once per problem by xl_convert_basis_kernel and
+// applied by op_gemm_kernel.
+struct XlTarget {
+  int node, acc_row;             // target node; its row block of the ACC scratch
+  int first_entry, n_entries;    // interactions sorted by direction
 };
 // One diagonal translation: source node, direction, and the translation
 // factor's index combo = up * 343 + (a+3) * 49 + (b+3) * 7 + (c+3) with
@@ -554,98 +566,107 @@ struct XlEntry {
   signed char dir, pad;
 };
 constexpr int kCombos = 686;
-constexpr int kXlTargets = 4;
+constexpr int kXlTargets = 4;                     // targets per translate block
 constexpr int kXlThreads = kXlTargets * kPairLanes;
+constexpr int kXlChannels = 4;                    // channels per translate block (one screening group)
 constexpr int kXlUnroll = 8;
-constexpr int kXlMaxEntries = 192;  // >= 189 interactions of one target child
 
+// One block per (4 targets of a level, 4 channels); thread (target tl,
+// lane i = plane wave): per direction run of the target's entries, the sum
+// of W[src][dir][ch][i] * factor[combo][i] is kept in registers and stored
+// as ACC[acc_row][ch][dir][i] (re, im); directions without entries store 0.
 template <typename T>
-struct XlChannels;  // channels per X2L block
-template <>
-struct XlChannels<float> {
-  static constexpr int value = 2;
-};
-template <>
-struct XlChannels<double> {
-  static constexpr int value = 1;
-};
-
-// One block per (half item, channel block); thread (target tl, lane i).
-// Phase 1: each thread accumulates, in registers, its target's translated
-// waves (translate_up/down_wave: W[src][dir] * factor[combo]) for every
-// direction, stored per (target, direction) once a direction's run ends.
-// Phase 2: yphystof of the six waves.  Phase 3: yexptolocal per pair.
-// Phase 4: rotation back (rotate_ytoz / rotate_ztox) and the sum of the three
-// pairs, assigned to the target's local expansion.
-template <typename T>
-__global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__ Tables<T> tb,
-                                                         const XlItem* __restrict__ items,
-                                                         const XlEntry* __restrict__ entries,
-                                                         const typename C2T<T>::type* __restrict__ W,
-                                                         typename C2T<T>::type* __restrict__ L) {
+__global__ void __launch_bounds__(kXlThreads) xl_translate_kernel(const __grid_constant__ Tables<T> tb, int parent_level,
+                                                                  const XlTarget* __restrict__ targets, int n_targets,
+                                                                  const XlEntry* __restrict__ entries,
+                                                                  const typename C2T<T>::type* __restrict__ W,
+                                                                  typename C2T<T>::type* __restrict__ ACC) {
   using C = typename C2T<T>::type;
-  constexpr int CB = XlChannels<T>::value;
-  extern __shared__ unsigned char smem_raw[];
-  const int E = tb.E, nl = tb.nl, NPM = tb.np_max;
-  C* acc = reinterpret_cast<C*>(smem_raw);        // [4 targets][6 dirs][CB][NPM]
-  C* mf = acc + kXlTargets * 6 * CB * NPM;         // [4][6][CB][64]
-  XlEntry* ents = reinterpret_cast<XlEntry*>(mf + kXlTargets * 6 * CB * 64);  // [4][kXlMaxEntries]
-  const XlItem it = items[blockIdx.x / (kCh / CB)];
+  constexpr int CB = kXlChannels;
+  constexpr int U = sizeof(T) == 4 ? kXlUnroll : kXlUnroll / 2;  // loads in flight per thread
+  const int NPM = tb.np_max;
+  const int tq = blockIdx.x / (kCh / CB);
   const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
-  const int lg = 2 * it.parent_level + (ch0 >= 8 ? 1 : 0);
-  const int np = tb.nexptotp[lg], nexptot = tb.nexptot[lg];
-  const int tl = threadIdx.x / kPairLanes, lane = threadIdx.x - tl * kPairLanes;
-  const int tn = it.targets[tl];
-  // the four targets are independent: each one's 64 threads synchronise on
-  // their own named barrier, and absent targets leave at once
-  if (tn < 0) return;
-  auto target_sync = [&]() { asm volatile("bar.sync %0, %1;\n" ::"r"(tl + 1), "n"(kPairLanes) : "memory"); };
-  C* acc_t = acc + (size_t)tl * 6 * CB * NPM;
-  C* loc = acc_t;  // [3 pairs][CB][E]: the target's own accumulators, reused after phase 2
-  for (int o = lane; o < 6 * CB * NPM; o += kPairLanes) acc_t[o] = cmk<C>(0, 0);
-  const int ne = it.n_entries[tl];
-  XlEntry* ent = ents + tl * kXlMaxEntries;
-  for (int o = lane; o < ne; o += kPairLanes) ent[o] = entries[it.first_entry[tl] + o];
-  target_sync();
-  if (lane < np) {
-    const int i = lane;
-    const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
-    C a[CB];
+  const int tl = threadIdx.x / kPairLanes, i = threadIdx.x - tl * kPairLanes;
+  const int t = tq * kXlTargets + tl;
+  const int lg = 2 * parent_level + (ch0 >= 8 ? 1 : 0);
+  if (t >= n_targets || i >= NPM) return;
+  const XlTarget tg = targets[t];
+  const int np = tb.nexptotp[lg];
+  // ACC[acc_row][ch][dir][i]: 6 * NPM complex per (target, channel)
+  C* out = ACC + ((size_t)tg.acc_row * kCh + ch0) * 6 * NPM + i;
+  if (i >= np) {  // plane waves beyond this level's count are never read
+    for (int c = 0; c < CB; ++c)
+      for (int d = 0; d < 6; ++d) out[((size_t)c * 6 + d) * NPM] = cmk<C>(0, 0);
+    return;
+  }
+  const XlEntry* ent = entries + tg.first_entry;
+  const int ne = tg.n_entries;
+  const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
+  C a[CB];
 #pragma unroll
-    for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
-    int cur = ne ? ent[0].dir : 0;
-    for (int k0 = 0; k0 < ne; k0 += kXlUnroll) {
-      XlEntry en[kXlUnroll];
-      C tt[kXlUnroll], w[kXlUnroll][CB];
+  for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
+  int cur = 0;  // next direction to store
+  for (int k0 = 0; k0 < ne; k0 += U) {
+    XlEntry en[U];
+    C tt[U], w[U][CB];
 #pragma unroll
-      for (int u = 0; u < kXlUnroll; ++u) en[u] = ent[min(k0 + u, ne - 1)];
+    for (int u = 0; u < U; ++u) en[u] = ent[min(k0 + u, ne - 1)];
 #pragma unroll
-      for (int u = 0; u < kXlUnroll; ++u) {
-        tt[u] = tc[(size_t)en[u].combo * NPM];
+    for (int u = 0; u < U; ++u) {
+      tt[u] = tc[(size_t)en[u].combo * NPM];
 #pragma unroll
-        for (int c = 0; c < CB; ++c) w[u][c] = W[(((size_t)en[u].src * 6 + en[u].dir) * kCh + ch0 + c) * NPM + i];
-      }
+      for (int c = 0; c < CB; ++c) w[u][c] = W[(((size_t)en[u].src * 6 + en[u].dir) * kCh + ch0 + c) * NPM + i];
+    }
 #pragma unroll
-      for (int u = 0; u < kXlUnroll; ++u) {
-        if (k0 + u < ne) {
-          if (en[u].dir != cur) {
+    for (int u = 0; u < U; ++u) {
+      if (k0 + u < ne) {
+        while (cur < en[u].dir) {  // close the current direction (and any without entries)
 #pragma unroll
-            for (int c = 0; c < CB; ++c) {
-              acc[((tl * 6 + cur) * CB + c) * NPM + i] = a[c];
-              a[c] = cmk<C>(0, 0);
-            }
-            cur = en[u].dir;
+          for (int c = 0; c < CB; ++c) {
+            out[((size_t)c * 6 + cur) * NPM] = a[c];
+            a[c] = cmk<C>(0, 0);
           }
-#pragma unroll
-          for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
+          ++cur;
         }
+#pragma unroll
+        for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
       }
     }
-    if (ne)
-#pragma unroll
-      for (int c = 0; c < CB; ++c) acc[((tl * 6 + cur) * CB + c) * NPM + i] = a[c];
   }
-  target_sync();
+  for (; cur < 6; ++cur)
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+      out[((size_t)c * 6 + cur) * NPM] = a[c];
+      a[c] = cmk<C>(0, 0);
+    }
+}
+
+// Conversion of one accumulated-wave vector to a local expansion, applied
+// to unit vectors: block (b, g) computes column b of the conversion operator
+// of screening group g for targets below parent_level, written as
+// ops[lg][b][r] (r < 2E real components, rows padded to RP).
+template <typename T>
+__global__ void __launch_bounds__(kPairLanes) xl_convert_basis_kernel(const __grid_constant__ Tables<T> tb,
+                                                                      int parent_level, int RP,
+                                                                      T* __restrict__ ops) {
+  using C = typename C2T<T>::type;
+  extern __shared__ unsigned char smem_raw[];
+  const int E = tb.E, nl = tb.nl, NPM = tb.np_max, K = 12 * NPM;
+  C* acc = reinterpret_cast<C*>(smem_raw);  // [6 dirs][NPM]
+  C* loc = acc;                              // [3 pairs][E], reuses acc after yphystof
+  C* mf = acc + 6 * NPM;                     // [6][64]
+  const int b = blockIdx.x % K, g = blockIdx.x / K;
+  const int lg = 2 * parent_level + g;
+  const int lane = threadIdx.x;
+  const int nexptot = tb.nexptot[lg];
+  for (int o = lane; o < 6 * NPM; o += blockDim.x) acc[o] = cmk<C>(0, 0);
+  __syncthreads();
+  if (lane == 0) {
+    const int dir = b / (2 * NPM), rem = b % (2 * NPM);
+    acc[dir * NPM + rem / 2] = (rem & 1) ? cmk<C>(0, 1) : cmk<C>(1, 0);
+  }
+  __syncthreads();
   const int* numphys = tb.numphys + (size_t)lg * nl;
   const C* fb = tb.fexpback + tb.fexpback_off[lg];
   const T* rl = tb.rlsc + (size_t)lg * E * nl;
@@ -663,8 +684,8 @@ __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__
     const int na = numphys[l], na2 = na / 2;
     const T ina = T(1) / T(na);
     const int nodd = (tb.numfour[l] - 1) / 2;
-    for (int dc = 0; dc < 6 * CB; ++dc) {
-      const C* ph = acc + ((size_t)tl * 6 * CB + dc) * NPM + nptot;
+    for (int d = 0; d < 6; ++d) {
+      const C* ph = acc + (size_t)d * NPM + nptot;
       C sum = cmk<C>(0, 0);
       if (mm == 1) {
         for (int iv = 0; iv < na2; ++iv) sum.x += T(2) * ph[iv].x;
@@ -675,61 +696,62 @@ __global__ void __launch_bounds__(kXlThreads) x2l_kernel(const __grid_constant__
         const C* f = fb + bb + nodd * na2 + ((mm - 2) / 2) * na2;
         for (int iv = 0; iv < na2; ++iv) sum = cadd(sum, cmul(f[iv], cmk<C>(0, T(2) * ph[iv].y)));
       }
-      mf[((size_t)tl * 6 * CB + dc) * 64 + j] = cscale(sum, ina);
+      mf[(size_t)d * 64 + j] = cscale(sum, ina);
     }
   }
-  target_sync();
-  // yexptolocal per pair (loc overwrites acc, which is no longer read)
+  __syncthreads();
+  // yexptolocal per pair
   if (lane < E) {
     const int e = lane;
     int nm = 0;
     while (tri(nm + 1, 0) <= e) ++nm;
     const int mth = e - tri(nm, 0);
     const T rs = T(3.14159265358979323846) / (tb.betascal[lg] * T(2)) * tb.sfac[e];
-    for (int g = 0; g < 3; ++g)
-      for (int c = 0; c < CB; ++c) {
-        const C* fu = mf + ((size_t)(tl * 6 + 2 * g) * CB + c) * 64;
-        const C* fd = mf + ((size_t)(tl * 6 + 2 * g + 1) * CB + c) * 64;
-        C v = cmk<C>(0, 0);
-        int ntot = 0;
-        for (int l = 0; l < nl; ++l) {
-          const int mmax = tb.numfour[l] - 1 > nm ? nm : tb.numfour[l] - 1;
-          if (mth <= mmax) {
-            const C pm = (nm & 1) ? csub(fd[ntot + mth], fu[ntot + mth]) : cadd(fd[ntot + mth], fu[ntot + mth]);
-            v = cadd(v, cscale(pm, rl[(size_t)e * nl + l] * tb.weights[l]));
-          }
-          ntot += tb.numfour[l];
+    for (int pg = 0; pg < 3; ++pg) {
+      const C* fu = mf + (size_t)(2 * pg) * 64;
+      const C* fd = mf + (size_t)(2 * pg + 1) * 64;
+      C v = cmk<C>(0, 0);
+      int ntot = 0;
+      for (int l = 0; l < nl; ++l) {
+        const int mmax = tb.numfour[l] - 1 > nm ? nm : tb.numfour[l] - 1;
+        if (mth <= mmax) {
+          const C pm = (nm & 1) ? csub(fd[ntot + mth], fu[ntot + mth]) : cadd(fd[ntot + mth], fu[ntot + mth]);
+          v = cadd(v, cscale(pm, rl[(size_t)e * nl + l] * tb.weights[l]));
         }
-        v = cscale(v, rs);
-        switch (mth & 3) {  // * i^m
-          case 1: v = cmk<C>(-v.y, v.x); break;
-          case 2: v = cmk<C>(-v.x, -v.y); break;
-          case 3: v = cmk<C>(v.y, -v.x); break;
-          default: break;
-        }
-        loc[((size_t)g * CB + c) * E + e] = v;
+        ntot += tb.numfour[l];
       }
+      v = cscale(v, rs);
+      switch (mth & 3) {  // * i^m
+        case 1: v = cmk<C>(-v.y, v.x); break;
+        case 2: v = cmk<C>(-v.x, -v.y); break;
+        case 3: v = cmk<C>(v.y, -v.x); break;
+        default: break;
+      }
+      loc[(size_t)pg * E + e] = v;
+    }
   }
-  target_sync();
+  __syncthreads();
   // rotate back and sum the pairs
   if (lane < E) {
     const int e = lane;
     int l = 0;
     while (tri(l + 1, 0) <= e) ++l;
     const int m = e - tri(l, 0);
-    for (int c = 0; c < CB; ++c) {
-      const C v0 = loc[((size_t)0 * CB + c) * E + e];
-      C v1 = rotate_one<T>(tb, loc + ((size_t)1 * CB + c) * E, tb.R(ROT_PI2), l, m);
-      switch (m & 3) {  // rotate_ytoz: * i^m
-        case 1: v1 = cmk<C>(-v1.y, v1.x); break;
-        case 2: v1 = cmk<C>(-v1.x, -v1.y); break;
-        case 3: v1 = cmk<C>(v1.y, -v1.x); break;
-        default: break;
-      }
-      const C v2 = rotate_one<T>(tb, loc + ((size_t)2 * CB + c) * E, tb.R(ROT_MPI2), l, m);
-      L[((size_t)tn * kCh + ch0 + c) * E + e] = cadd(cadd(v0, v1), v2);
+    const C v0 = loc[e];
+    C v1 = rotate_one<T>(tb, loc + E, tb.R(ROT_PI2), l, m);
+    switch (m & 3) {  // rotate_ytoz: * i^m
+      case 1: v1 = cmk<C>(-v1.y, v1.x); break;
+      case 2: v1 = cmk<C>(-v1.x, -v1.y); break;
+      case 3: v1 = cmk<C>(v1.y, -v1.x); break;
+      default: break;
     }
+    const C v2 = rotate_one<T>(tb, loc + 2 * E, tb.R(ROT_MPI2), l, m);
+    const C v = cadd(cadd(v0, v1), v2);
+    T* col = ops + ((size_t)lg * K + b) * RP;
+    col[2 * e] = v.x;
+    col[2 * e + 1] = v.y;
   }
+  for (int r = 2 * E + lane; r < RP; r += blockDim.x) ops[((size_t)lg * K + b) * RP + r] = 0;
 }
 
 // ---------------------------------------------------------------- L2P
@@ -1206,6 +1228,126 @@ __global__ void __launch_bounds__(kGemmThreads) shift_gemm_kernel(int E, const S
   }
 }
 
+// Dense operator applied to gathered columns: Y[col] = A_op X[col] for the
+// multipole -> plane-wave map (684 x 110 per level and screening group) and
+// the accumulated-wave -> local map (110 x 684).  A tile is 112 rows of one
+// operator by up to 32 columns; K streams through shared memory in chunks
+// (cp.async, double-buffered); thread (rg, cg) owns rows 4rg..4rg+3 and
+// columns 8cg..8cg+7.  Output row r of column c goes to
+// Y[dst_c + (r / seg) * seg_stride + r % seg].
+struct GemmTile {
+  int op, first_col, n_cols, row0;
+};
+struct GemmCol {
+  long long src, dst;  // element offsets of the column's input vector and output base
+};
+constexpr int kOpRows = 112;
+constexpr int kOpCols = 32;
+constexpr int kOpThreads = (kOpRows / 4) * (kOpCols / 8);
+
+template <typename T>
+struct OpChunk;  // K rows per pipeline stage
+template <>
+struct OpChunk<float> {
+  static constexpr int value = 56;
+};
+template <>
+struct OpChunk<double> {
+  static constexpr int value = 28;
+};
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem);
+template <>
+__device__ __forceinline__ void cp_async_elem<float>(float* smem, const float* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <>
+__device__ __forceinline__ void cp_async_elem<double>(double* smem, const double* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kOpThreads) op_gemm_kernel(const GemmTile* __restrict__ tiles,
+                                                             const GemmCol* __restrict__ cols,
+                                                             const T* __restrict__ ops, int K, int RP, int R,
+                                                             int seg, long long seg_stride,
+                                                             const T* __restrict__ X, T* __restrict__ Y) {
+  constexpr int KC = OpChunk<T>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);  // [2][KC][kOpRows]
+  T* xs = As + 2 * KC * kOpRows;            // [2][KC][kOpCols]
+  const GemmTile tl = tiles[blockIdx.x];
+  const T* A0 = ops + (size_t)tl.op * K * RP + tl.row0;
+  const int nchunks = (K + KC - 1) / KC;
+  auto stage = [&](int c, int buf) {
+    const int kb = c * KC, kn = min(KC, K - kb);
+    T* a = As + (size_t)buf * KC * kOpRows;
+    constexpr int per16 = 16 / (int)sizeof(T), chunks = kOpRows / per16;  // 16-byte copies per row
+    for (int j = threadIdx.x; j < kn * chunks; j += blockDim.x) {
+      const int k = j / chunks, q = j - k * chunks;
+      cp_async16(a + k * kOpRows + per16 * q, A0 + (size_t)(kb + k) * RP + per16 * q);
+    }
+    T* x = xs + (size_t)buf * KC * kOpCols;
+    for (int j = threadIdx.x; j < kn * kOpCols; j += blockDim.x) {
+      const int k = j / kOpCols, n = j - k * kOpCols;
+      if (n < tl.n_cols)
+        cp_async_elem<T>(x + k * kOpCols + n, X + cols[tl.first_col + n].src + kb + k);
+      else
+        x[k * kOpCols + n] = 0;
+    }
+    cp_async_commit();
+  };
+  const int rg = threadIdx.x % (kOpRows / 4), cg = threadIdx.x / (kOpRows / 4);
+  T acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0;
+  stage(0, 0);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      stage(c + 1, (c + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int kn = min(KC, K - c * KC);
+    const T* a = As + (size_t)(c & 1) * KC * kOpRows + 4 * rg;
+    const T* x = xs + (size_t)(c & 1) * KC * kOpCols + 8 * cg;
+#pragma unroll 4
+    for (int k = 0; k < kn; ++k) {
+      T av[4], x0[4], x1[4];
+      load4<T>(a + k * kOpRows, av);
+      load4<T>(x + k * kOpCols, x0);
+      load4<T>(x + k * kOpCols + 4, x1);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j] += av[i] * x0[j];
+          acc[i][4 + j] += av[i] * x1[j];
+        }
+      }
+    }
+    __syncthreads();  // buffer (c & 1) is refilled by the stage of chunk c + 2
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int n = 8 * cg + j;
+    if (n >= tl.n_cols) break;
+    const long long dst = cols[tl.first_col + n].dst;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = tl.row0 + 4 * rg + i;
+      if (r < R) Y[dst + (long long)(r / seg) * seg_stride + r % seg] = acc[i][j];
+    }
+  }
+}
+
 // M[parent] = sum of its children's partials, in child order
 template <typename T>
 __global__ void __launch_bounds__(256) shift_reduce_kernel(int E, const ShiftReduce* __restrict__ items,
@@ -1259,13 +1401,20 @@ __global__ void __launch_bounds__(256) prep_csr_kernel(int E, int EQ, const Leaf
 struct FmmState {
   int nt = 9, E = 55, nlev = 0, np_max = 0, nl = 0;
   bool fp64 = true;
-  DevBuf tables_buf;  // one allocation holding every table
+  DevBuf tables_buf;    // one allocation holding every table
+  DevBuf tables_buf_d;  // FP64 tables used only to tabulate operators of an FP32 problem
   Tables<double> tb_d{};
   Tables<float> tb_f{};
   DevBuf M, L, W;  // expansions and plane waves
-  DevBuf p2m_items, m2x_items, xl_items, xl_entries, leaf_items;
-  int n_p2m = 0, n_m2x = 0, n_xl = 0, n_leaf = 0;
-  size_t smem_shift = 0, smem_m2x = 0, smem_xl = 0, smem_prep = 0, smem_eval = 0;
+  DevBuf p2m_items, xl_targets, xl_entries, leaf_items;
+  int n_p2m = 0, n_leaf = 0;
+  size_t smem_shift = 0, smem_m2x = 0, smem_prep = 0, smem_eval = 0, smem_op = 0, smem_xlb = 0;
+  // operator form of multipole -> plane waves and accumulated waves -> local
+  DevBuf m2x_ops;  // [lg][2E][m2x_rp]
+  DevBuf xl_ops;   // [lg][12 NPM][xl_rp]
+  int m2x_rp = 0, xl_rp = 0;
+  DevBuf op_tiles, op_cols;
+  DevBuf acc;      // [target row][channel][6 dirs][NPM] accumulated waves
   DevBuf leaf_exp;  // per leaf: [2 groups][F, H0, H1, H2][EQ]
   DevBuf eval_items;
   DevBuf p2m_basis;   // [patch position][2 groups][E], geometry only
@@ -1278,10 +1427,11 @@ struct FmmState {
   std::vector<int> l2l_tfirst, l2l_tcount;                          // per parent level
   DevBuf prep_rowptr, prep_cols, prep_vals;
   size_t smem_gemm = 0, smem_csr = 0;
-  // per level: M2X items of the level's nodes, X2L half items whose targets
-  // are on the level; a stream per level runs them as soon as the level's
-  // multipoles exist (events order them against the up and down passes)
-  std::vector<int> m2x_first, m2x_count, xl_first, xl_count;
+  // per level: M2X tiles of the level's nodes, X2L targets on the level and
+  // their conversion tiles; a stream per level runs them as soon as the
+  // level's multipoles exist (events order them against the up and down
+  // passes)
+  std::vector<int> m2x_tfirst, m2x_tcount, xlt_first, xlt_count, xlc_tfirst, xlc_tcount;
   std::vector<cudaStream_t> lstreams;
   std::vector<cudaEvent_t> ev_m, ev_x;
   ~FmmState() {
@@ -1330,7 +1480,7 @@ std::vector<RawInteraction> interaction_table() {
 }
 
 template <typename T>
-void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
+void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb, DevBuf& buf) {
   using C = typename C2T<T>::type;
   const int nt = S.nt, E = S.E, nlev = S.nlev;
   GlobalTables G;
@@ -1430,10 +1580,10 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb) {
          o_fe = putC(fexpe), o_fo = putC(fexpo), o_fb = putC(fexpback), o_feo = putI(fe_off), o_foo = putI(fo_off),
          o_fbo = putI(fb_off), o_xs = putC(xs), o_ys = putC(ys), o_zs = putT(zs), o_mps = putT(mps),
          o_lcs = putT(lcs), o_tc = putC(tcomb);
-  S.tables_buf.alloc(P.ctx, blob.size());
-  BP_CUDA(cudaMemcpyAsync(S.tables_buf.get(), blob.data(), blob.size(), cudaMemcpyHostToDevice, P.ctx->stream));
+  buf.alloc(P.ctx, blob.size());
+  BP_CUDA(cudaMemcpyAsync(buf.get(), blob.data(), blob.size(), cudaMemcpyHostToDevice, P.ctx->stream));
   BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
-  unsigned char* base = S.tables_buf.as<unsigned char>();
+  unsigned char* base = buf.as<unsigned char>();
   tb.nt = nt;
   tb.E = E;
   tb.nl = S.nl;
@@ -1532,6 +1682,71 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   BP_CUDA(cudaStreamSynchronize(st));
 }
 
+// Tabulates, in FP64, the multipole -> plane-wave operator (m2x_kernel on
+// unit multipoles, one per real component) and the accumulated-wave ->
+// local operator (xl_convert_basis_kernel on unit waves) of every level and
+// screening group, stored k-major ([lg][k][row], rows padded) in the
+// engine's precision.
+static void build_wave_operators(Problem& P, FmmState& S) {
+  Ctx* c = P.ctx;
+  cudaStream_t st = c->stream;
+  const int E = S.E, R2 = 2 * E, NPM = S.np_max, KW = 12 * NPM, nlev = S.nlev, nlg = 2 * nlev;
+  std::vector<double> m2x((size_t)nlg * R2 * S.m2x_rp, 0.0);
+  {
+    std::vector<double2> hm((size_t)R2 * kCh * E, make_double2(0.0, 0.0));
+    for (int b = 0; b < R2; ++b)
+      for (int ch = 0; ch < kCh; ++ch) {
+        double2& v = hm[((size_t)b * kCh + ch) * E + b / 2];
+        if (b & 1) v.y = 1.0;
+        else v.x = 1.0;
+      }
+    DevBuf Mb = upload(c, hm);
+    DevBuf Wb(c, sizeof(double2) * (size_t)R2 * 6 * kCh * NPM);
+    std::vector<double2> hw((size_t)R2 * 6 * kCh * NPM);
+    for (int lev = 1; lev < nlev; ++lev) {
+      std::vector<M2xItem> items(R2);
+      for (int b = 0; b < R2; ++b) items[b] = M2xItem{b, lev};
+      DevBuf di = upload(c, items);
+      BP_CUDA(cudaMemsetAsync(Wb.get(), 0, Wb.bytes(), st));
+      m2x_kernel<double><<<R2 * (kCh / kM2xChannels), kM2xThreads, S.smem_m2x, st>>>(
+          S.tb_d, di.as<M2xItem>(), Mb.as<double2>(), Wb.as<double2>());
+      BP_LAUNCH_CHECK();
+      BP_CUDA(cudaMemcpyAsync(hw.data(), Wb.get(), Wb.bytes(), cudaMemcpyDeviceToHost, st));
+      BP_CUDA(cudaStreamSynchronize(st));
+      for (int g = 0; g < 2; ++g) {
+        const int ch = g ? 8 : 0, lg = 2 * (lev - 1) + g;
+        for (int b = 0; b < R2; ++b)
+          for (int dir = 0; dir < 6; ++dir)
+            for (int i = 0; i < NPM; ++i) {
+              const double2 w = hw[(((size_t)b * 6 + dir) * kCh + ch) * NPM + i];
+              double* col = m2x.data() + ((size_t)lg * R2 + b) * S.m2x_rp + (size_t)dir * 2 * NPM + 2 * i;
+              col[0] = w.x;
+              col[1] = w.y;
+            }
+      }
+    }
+  }
+  std::vector<double> xl((size_t)nlg * KW * S.xl_rp, 0.0);
+  {
+    DevBuf Ob(c, sizeof(double) * xl.size());
+    BP_CUDA(cudaMemsetAsync(Ob.get(), 0, Ob.bytes(), st));
+    for (int pl = 0; pl + 1 < nlev; ++pl) {
+      xl_convert_basis_kernel<double><<<2 * KW, kPairLanes, S.smem_xlb, st>>>(S.tb_d, pl, S.xl_rp, Ob.as<double>());
+      BP_LAUNCH_CHECK();
+    }
+    BP_CUDA(cudaMemcpyAsync(xl.data(), Ob.get(), Ob.bytes(), cudaMemcpyDeviceToHost, st));
+    BP_CUDA(cudaStreamSynchronize(st));
+  }
+  if (S.fp64) {
+    S.m2x_ops = upload(c, m2x);
+    S.xl_ops = upload(c, xl);
+  } else {
+    S.m2x_ops = upload(c, std::vector<float>(m2x.begin(), m2x.end()));
+    S.xl_ops = upload(c, std::vector<float>(xl.begin(), xl.end()));
+  }
+  BP_CUDA(cudaStreamSynchronize(st));
+}
+
 // Builds the FMM schedule of a problem.  Only work that can reach a result
 // is scheduled: X2L halves with at least one interaction, M2X of the nodes
 // that are translation sources, M2M / P2M of the nodes whose multipoles feed
@@ -1546,10 +1761,9 @@ void fmm_setup(Problem& P) {
   S->E = (S->nt + 1) * (S->nt + 2) / 2;
   S->nlev = T.n_levels;
   S->fp64 = P.fp64;
-  if (S->fp64)
-    fill_tables<double>(*S, P, S->tb_d);
-  else
-    fill_tables<float>(*S, P, S->tb_f);
+  // FP64 tables always: they tabulate the dense operators of both engines
+  fill_tables<double>(*S, P, S->tb_d, S->fp64 ? S->tables_buf : S->tables_buf_d);
+  if (!S->fp64) fill_tables<float>(*S, P, S->tb_f, S->tables_buf);
   if (S->np_max > kPairLanes) throw std::invalid_argument("FMM order too large for the plane-wave thread layout");
   const int nn = (int)T.nodes.size();
   const size_t celem = S->fp64 ? sizeof(double2) : sizeof(float2);
@@ -1563,63 +1777,48 @@ void fmm_setup(Problem& P) {
   auto flags = [&](int k) { return T.nodes[k].flags; };
   auto cnt = [&](int k) { return T.nodes[k].content_count; };
   auto octant = [&](int k) { return 1 + (T.nodes[k].ix & 1) + 2 * (T.nodes[k].iy & 1) + 4 * (T.nodes[k].iz & 1); };
-  // X2L: halves (targets 0-3, 4-7) of parents that are neither leaf nor
-  // shadow; entries per target sorted by direction
+  // X2L targets: non-shadow children of parents that are neither leaf nor
+  // shadow, with at least one interaction; entries sorted by direction
   const auto table = interaction_table();
   std::vector<std::vector<int>> by_target_dir(8 * 6);
   for (int q = 0; q < (int)table.size(); ++q) by_target_dir[table[q].targ * 6 + table[q].dir].push_back(q);
-  std::vector<XlItem> xl;
+  std::vector<std::vector<XlTarget>> xlt_lev(nlev);
   std::vector<XlEntry> xle;
   std::vector<char> is_source(nn, 0), written(nn, 0);
   for (int k = 0; k < nn; ++k) {
     const TreeNode& nd = T.nodes[k];
     if (nd.level >= nlev - 1) continue;
     if ((nd.flags & TREE_LEAF) || (nd.flags & TREE_SHADOW)) continue;
-    for (int half = 0; half < 2; ++half) {
-      XlItem it;
-      it.parent_level = nd.level;
-      int total = 0;
-      for (int tl = 0; tl < kXlTargets; ++tl) {
-        const int t = half * kXlTargets + tl;
-        const int ck = nd.children[t];
-        it.targets[tl] = (ck >= 0 && !(flags(ck) & TREE_SHADOW)) ? ck : -1;
-        it.first_entry[tl] = (int)xle.size();
-        it.n_entries[tl] = 0;
-        if (it.targets[tl] < 0) continue;
-        for (int dir = 0; dir < 6; ++dir)
-          for (int q : by_target_dir[t * 6 + dir]) {
-            const RawInteraction& r = table[q];
-            const int nbk = nd.neighbours[r.nb];
-            if (nbk < 0 || cnt(nbk) == 0) continue;
-            const int sk = T.nodes[nbk].children[r.src];
-            if (sk < 0 || cnt(sk) == 0) continue;
-            int a, b, c;
-            switch (r.dir) {
-              case 0: case 1: a = r.dx; b = r.dy; c = r.dz; break;
-              case 2: case 3: a = r.dz; b = r.dx; c = r.dy; break;
-              default: a = -r.dz; b = r.dy; c = r.dx; break;
-            }
-            const int up = r.dir % 2 == 0 ? 1 : 0;
-            XlEntry e;
-            e.src = sk;
-            e.combo = (short)(up * 343 + (a + 3) * 49 + (b + 3) * 7 + (c + 3));
-            e.dir = (signed char)r.dir;
-            e.pad = 0;
-            xle.push_back(e);
-            is_source[sk] = 1;
+    for (int t = 0; t < 8; ++t) {
+      const int ck = nd.children[t];
+      if (ck < 0 || (flags(ck) & TREE_SHADOW)) continue;
+      XlTarget tg{ck, 0, (int)xle.size(), 0};
+      for (int dir = 0; dir < 6; ++dir)
+        for (int q : by_target_dir[t * 6 + dir]) {
+          const RawInteraction& r = table[q];
+          const int nbk = nd.neighbours[r.nb];
+          if (nbk < 0 || cnt(nbk) == 0) continue;
+          const int sk = T.nodes[nbk].children[r.src];
+          if (sk < 0 || cnt(sk) == 0) continue;
+          int a, b, c;
+          switch (r.dir) {
+            case 0: case 1: a = r.dx; b = r.dy; c = r.dz; break;
+            case 2: case 3: a = r.dz; b = r.dx; c = r.dy; break;
+            default: a = -r.dz; b = r.dy; c = r.dx; break;
           }
-        it.n_entries[tl] = (int)xle.size() - it.first_entry[tl];
-        total += it.n_entries[tl];
-      }
-      if (total == 0) {
-        xle.resize(it.first_entry[0]);
-        continue;
-      }
-      for (int tl = 0; tl < kXlTargets; ++tl) {
-        if (it.n_entries[tl] > kXlMaxEntries) throw std::logic_error("X2L target with too many interactions");
-        if (it.targets[tl] >= 0) written[it.targets[tl]] = 1;
-      }
-      xl.push_back(it);
+          const int up = r.dir % 2 == 0 ? 1 : 0;
+          XlEntry e;
+          e.src = sk;
+          e.combo = (short)(up * 343 + (a + 3) * 49 + (b + 3) * 7 + (c + 3));
+          e.dir = (signed char)r.dir;
+          e.pad = 0;
+          xle.push_back(e);
+          is_source[sk] = 1;
+        }
+      tg.n_entries = (int)xle.size() - tg.first_entry;
+      if (tg.n_entries == 0) continue;
+      written[ck] = 1;
+      xlt_lev[nd.level + 1].push_back(tg);
     }
   }
   // multipoles needed: translation sources and every node below one
@@ -1680,10 +1879,10 @@ void fmm_setup(Problem& P) {
     for (int b = 0; b < 16; ++b) add_bucket(op_base(0, lev, b % 8 + 1) + (b >= 8 ? 8 : 0), bucket[b]);
     S->m2m_tcount[lev] = (int)tiles.size() - S->m2m_tfirst[lev];
   }
-  // M2X items: translation sources
-  std::vector<M2xItem> m2x;
+  // translation sources per level (their multipoles become plane waves)
+  std::vector<std::vector<int>> src_lev(nlev);
   for (int k = 0; k < nn; ++k)
-    if (is_source[k]) m2x.push_back({k, T.nodes[k].level});
+    if (is_source[k]) src_lev[T.nodes[k].level].push_back(k);
   // L2L per parent level, top-down: child (= or +=) shift(parent)
   S->l2l_tfirst.assign(nlev, 0);
   S->l2l_tcount.assign(nlev, 0);
@@ -1718,29 +1917,60 @@ void fmm_setup(Problem& P) {
   Ctx* c = P.ctx;
   S->p2m_items = upload(c, p2m);
   S->n_p2m = (int)p2m.size();
-  S->m2x_items = upload(c, m2x);
-  S->n_m2x = (int)m2x.size();
-  S->xl_items = upload(c, xl);
+  // operator GEMM tiles: M2X columns (source node, channel) per (level,
+  // group) into W; X->L columns (target, channel) per (level, group) from the
+  // ACC scratch into L
+  const int NPM = S->np_max, R2 = 2 * S->E, KW = 12 * NPM;
+  S->m2x_rp = (KW + kOpRows - 1) / kOpRows * kOpRows;
+  S->xl_rp = (R2 + kOpRows - 1) / kOpRows * kOpRows;
+  std::vector<GemmTile> otiles;
+  std::vector<GemmCol> ocols;
+  auto add_cols = [&](int op, int rows_pad, const std::vector<GemmCol>& cl) {
+    for (size_t c0 = 0; c0 < cl.size(); c0 += kOpCols) {
+      const int n = (int)std::min<size_t>(kOpCols, cl.size() - c0);
+      const int first = (int)ocols.size();
+      ocols.insert(ocols.end(), cl.begin() + c0, cl.begin() + c0 + n);
+      for (int row0 = 0; row0 < rows_pad; row0 += kOpRows) otiles.push_back({op, first, n, row0});
+    }
+  };
+  S->m2x_tfirst.assign(nlev, 0);
+  S->m2x_tcount.assign(nlev, 0);
+  S->xlt_first.assign(nlev, 0);
+  S->xlt_count.assign(nlev, 0);
+  S->xlc_tfirst.assign(nlev, 0);
+  S->xlc_tcount.assign(nlev, 0);
+  std::vector<XlTarget> xlt;
+  for (int lev = 1; lev < nlev; ++lev) {
+    S->m2x_tfirst[lev] = (int)otiles.size();
+    for (int g = 0; g < 2; ++g) {
+      std::vector<GemmCol> cl;
+      for (int k : src_lev[lev])
+        for (int ch = g ? 8 : 0; ch < (g ? kCh : 8); ++ch)
+          cl.push_back({((long long)k * kCh + ch) * R2, ((long long)k * 6 * kCh + ch) * 2 * NPM});
+      add_cols(2 * (lev - 1) + g, S->m2x_rp, cl);
+    }
+    S->m2x_tcount[lev] = (int)otiles.size() - S->m2x_tfirst[lev];
+    S->xlt_first[lev] = (int)xlt.size();
+    for (XlTarget tg : xlt_lev[lev]) {
+      tg.acc_row = (int)xlt.size();
+      xlt.push_back(tg);
+    }
+    S->xlt_count[lev] = (int)xlt.size() - S->xlt_first[lev];
+    S->xlc_tfirst[lev] = (int)otiles.size();
+    for (int g = 0; g < 2; ++g) {
+      std::vector<GemmCol> cl;
+      for (int q = S->xlt_first[lev]; q < S->xlt_first[lev] + S->xlt_count[lev]; ++q)
+        for (int ch = g ? 8 : 0; ch < (g ? kCh : 8); ++ch)
+          cl.push_back({((long long)xlt[q].acc_row * kCh + ch) * KW, ((long long)xlt[q].node * kCh + ch) * R2});
+      add_cols(2 * (lev - 1) + g, S->xl_rp, cl);
+    }
+    S->xlc_tcount[lev] = (int)otiles.size() - S->xlc_tfirst[lev];
+  }
+  S->op_tiles = upload(c, otiles);
+  S->op_cols = upload(c, ocols);
+  S->xl_targets = upload(c, xlt);
   S->xl_entries = upload(c, xle);
-  S->n_xl = (int)xl.size();
-  S->m2x_first.assign(nlev, 0);
-  S->m2x_count.assign(nlev, 0);
-  S->xl_first.assign(nlev, 0);
-  S->xl_count.assign(nlev, 0);
-  for (int q = (int)m2x.size() - 1; q >= 0; --q) {
-    S->m2x_first[m2x[q].level] = q;
-    S->m2x_count[m2x[q].level]++;
-  }
-  for (int q = (int)xl.size() - 1; q >= 0; --q) {
-    S->xl_first[xl[q].parent_level + 1] = q;
-    S->xl_count[xl[q].parent_level + 1]++;
-  }
-  for (int lev = 0; lev < nlev; ++lev) {
-    for (int q = S->m2x_first[lev]; q < S->m2x_first[lev] + S->m2x_count[lev]; ++q)
-      if (m2x[q].level != lev) throw std::logic_error("M2X items are not grouped by level");
-    for (int q = S->xl_first[lev]; q < S->xl_first[lev] + S->xl_count[lev]; ++q)
-      if (xl[q].parent_level + 1 != lev) throw std::logic_error("X2L items are not grouped by level");
-  }
+  S->acc.alloc(c, celem * kCh * 6 * (size_t)NPM * std::max<size_t>(1, xlt.size()));
   S->lstreams.assign(nlev, nullptr);
   S->ev_m.assign(nlev, nullptr);
   S->ev_x.assign(nlev, nullptr);
@@ -1761,31 +1991,31 @@ void fmm_setup(Problem& P) {
   if (E > kPairLanes) throw std::invalid_argument("FMM order above 9 is not supported");
   S->smem_shift = 4 * celem * E;
   S->smem_gemm = (S->fp64 ? 8 : 4) * (size_t)(2 * E) * (((2 * E + 3) & ~3) + kTileCols);
-  S->smem_m2x = celem * (size_t)(4 * kM2xChannels * E + 6 * kM2xChannels * 64);
-  const int xcb = S->fp64 ? XlChannels<double>::value : XlChannels<float>::value;
-  S->smem_xl = celem * (size_t)kXlTargets * 6 * xcb * (S->np_max + 64) + sizeof(XlEntry) * kXlTargets * kXlMaxEntries;
+  S->smem_m2x = sizeof(double2) * (size_t)(4 * kM2xChannels * E + 6 * kM2xChannels * 64);  // FP64 tabulation
+  S->smem_xlb = sizeof(double2) * (size_t)(6 * S->np_max + 6 * 64);
+  S->smem_op = (S->fp64 ? 8 : 4) * (size_t)2 * (S->fp64 ? OpChunk<double>::value : OpChunk<float>::value) *
+               (kOpRows + kOpCols);
   const int EQ = (NT + 3) * (NT + 4) / 2;
   S->smem_prep = celem * 2 * 24 * (size_t)EQ;
   S->smem_eval = celem * 8 * (size_t)EQ + (S->fp64 ? 8 : 4) * (size_t)16 * kEvalChunk;
   S->leaf_exp.alloc(P.ctx, celem * 8 * (size_t)EQ * std::max(1, S->n_leaf));
   S->p2m_basis.alloc(P.ctx, celem * 2 * (size_t)E * std::max(1, p2m_rows));
   S->eval_basis.alloc(P.ctx, celem * 2 * (size_t)EQ * kEvalChunk * std::max(1, S->n_eval));
-  if (S->smem_xl > 227 * 1024 || S->smem_prep > 227 * 1024 || S->smem_m2x > 227 * 1024 ||
+  if (S->smem_op > 227 * 1024 || S->smem_prep > 227 * 1024 || S->smem_m2x > 227 * 1024 ||
       S->smem_gemm > 227 * 1024)
     throw std::invalid_argument("FMM order too large for the shared-memory layout");
   if (S->fp64) {
-    ensure_dynamic_smem((const void*)m2x_kernel<double>, S->smem_m2x);
-    ensure_dynamic_smem((const void*)x2l_kernel<double>, S->smem_xl);
+    ensure_dynamic_smem((const void*)op_gemm_kernel<double>, S->smem_op);
     ensure_dynamic_smem((const void*)shift_gemm_kernel<double>, S->smem_gemm);
     ensure_dynamic_smem((const void*)l2p_prep_kernel<double>, S->smem_prep);
     ensure_dynamic_smem((const void*)l2p_eval_kernel<double>, S->smem_eval);
   } else {
-    ensure_dynamic_smem((const void*)m2x_kernel<float>, S->smem_m2x);
-    ensure_dynamic_smem((const void*)x2l_kernel<float>, S->smem_xl);
+    ensure_dynamic_smem((const void*)op_gemm_kernel<float>, S->smem_op);
     ensure_dynamic_smem((const void*)shift_gemm_kernel<float>, S->smem_gemm);
     ensure_dynamic_smem((const void*)l2p_prep_kernel<float>, S->smem_prep);
     ensure_dynamic_smem((const void*)l2p_eval_kernel<float>, S->smem_eval);
   }
+  ensure_dynamic_smem((const void*)m2x_kernel<double>, S->smem_m2x);
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
   BP_CUDA(cudaStreamSynchronize(c->stream));
@@ -1793,6 +2023,8 @@ void fmm_setup(Problem& P) {
     build_operators<double>(P, *S, S->tb_d, leaves);
   else
     build_operators<float>(P, *S, S->tb_f, leaves);
+  build_wave_operators(P, *S);
+  S->tables_buf_d.reset();  // the FP64 copy of an FP32 problem's tables is no longer needed
   // geometry-only bases of P2M and of the L2P evaluation
   const double* cen = P.d_centroid.as<double>();
   if (S->fp64) {
@@ -1841,23 +2073,31 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   };
   if (S.n_leaf == 0) throw std::runtime_error("inconsistent FMM schedule (no leaves)");
   const int nlev = S.nlev;
-  auto has_x = [&](int lev) { return S.m2x_count[lev] > 0 || S.xl_count[lev] > 0; };
-  // M2X and X2L of one level on stream q
+  const int NPM = S.np_max, KW = 12 * NPM, R2 = 2 * S.E;
+  auto has_x = [&](int lev) { return S.m2x_tcount[lev] > 0 || S.xlt_count[lev] > 0; };
+  // multipole -> plane waves, translations, accumulated waves -> locals of
+  // one level on stream q
   auto level_x = [&](int lev, cudaStream_t q) {
-    if (S.m2x_count[lev]) {
+    if (S.m2x_tcount[lev]) {
       begin(3, q);
-      m2x_kernel<T><<<S.m2x_count[lev] * (kCh / kM2xChannels), kM2xThreads, S.smem_m2x, q>>>(
-          tb, S.m2x_items.as<M2xItem>() + S.m2x_first[lev], M, W);
+      op_gemm_kernel<T><<<S.m2x_tcount[lev], kOpThreads, S.smem_op, q>>>(
+          S.op_tiles.as<GemmTile>() + S.m2x_tfirst[lev], S.op_cols.as<GemmCol>(), S.m2x_ops.as<T>(), R2, S.m2x_rp,
+          KW, 2 * NPM, (long long)kCh * 2 * NPM, reinterpret_cast<const T*>(M), reinterpret_cast<T*>(W));
       BP_LAUNCH_CHECK();
       end(1);
     }
-    if (S.xl_count[lev]) {
-      constexpr int xcb = XlChannels<T>::value;
+    if (S.xlt_count[lev]) {
       begin(4, q);
-      x2l_kernel<T><<<S.xl_count[lev] * (kCh / xcb), kXlThreads, S.smem_xl, q>>>(
-          tb, S.xl_items.as<XlItem>() + S.xl_first[lev], S.xl_entries.as<XlEntry>(), W, Lx);
+      const int nb = (S.xlt_count[lev] + kXlTargets - 1) / kXlTargets * (kCh / kXlChannels);
+      xl_translate_kernel<T><<<nb, kXlThreads, 0, q>>>(tb, lev - 1, S.xl_targets.as<XlTarget>() + S.xlt_first[lev],
+                                                      S.xlt_count[lev], S.xl_entries.as<XlEntry>(), W,
+                                                      S.acc.as<C>());
       BP_LAUNCH_CHECK();
-      end(1);
+      op_gemm_kernel<T><<<S.xlc_tcount[lev], kOpThreads, S.smem_op, q>>>(
+          S.op_tiles.as<GemmTile>() + S.xlc_tfirst[lev], S.op_cols.as<GemmCol>(), S.xl_ops.as<T>(), KW, S.xl_rp,
+          R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()), reinterpret_cast<T*>(Lx));
+      BP_LAUNCH_CHECK();
+      end(2);
     }
   };
   auto fork_x = [&](int lev) {
