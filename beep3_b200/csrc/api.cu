@@ -310,6 +310,7 @@ BP_API int32_t bp_matvec(bp_problem p, const double* x, double* y) {
     matvec_device(*P, P->d_x.as<double>(), P->d_y.as<double>());
     BP_CUDA(cudaMemcpyAsync(y, P->d_y.get(), bytes, cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
+    fmm_check_waits(*P);
     return BP_OK;
   });
 }
@@ -346,6 +347,7 @@ BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, 
     int its = gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, &rr);
     BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
+    fmm_check_waits(*P);
     if (iterations) *iterations = its;
     if (rel_residual) *rel_residual = rr;
     if (rr > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");

@@ -21,6 +21,9 @@ struct CudaError : std::runtime_error {
 struct BudgetError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+struct TimeoutError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 #define BP_CUDA(call)                                                                               \
   do {                                                                                              \
@@ -47,6 +50,8 @@ int32_t guarded_engine(F&& f) {
     return fail(BP_ERR_BUDGET, e.what());
   } catch (const CudaError& e) {
     return fail(BP_ERR_CUDA, e.what());
+  } catch (const TimeoutError& e) {
+    return fail(BP_ERR_TIMEOUT, e.what());
   } catch (const std::bad_alloc&) {
     return fail(BP_ERR_NOMEM, "host allocation failed");
   } catch (const std::invalid_argument& e) {
@@ -263,6 +268,10 @@ void nf_assemble(Problem& P);
 void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t stream);
 // fmm.cu
 bool fmm_active(const Problem& P);
+// Throws TimeoutError if a tensor-core FMM kernel of this problem gave up on
+// a bounded wait since the problem was created (its results are then void).
+// Synchronises the context stream.
+void fmm_check_waits(Problem& P);
 void fmm_setup(Problem& P);
 void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st, cudaStream_t stream);
 void matvec_setup(Problem& P);

@@ -39,6 +39,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -1237,6 +1238,8 @@ __global__ void __launch_bounds__(kGemmThreads) shift_gemm_kernel(int E, const S
 // Y[dst_c + (r / seg) * seg_stride + r % seg].
 struct GemmTile {
   int op, first_col, n_cols, row0;
+  int kc0, nkc;        // tensor-core tiles: k chunks [kc0, kc0 + nkc) of the operator
+  long long dst_off;   // added to every column's output offset (split-K partial slot)
 };
 struct GemmCol {
   long long src, dst;  // element offsets of the column's input vector and output base
@@ -1348,6 +1351,244 @@ __global__ void __launch_bounds__(kOpThreads) op_gemm_kernel(const GemmTile* __r
   }
 }
 
+// ---------------------------------------------------------------- tensor-core operator GEMM
+// The same gathered GEMM on the 5th-generation tensor cores for the FP32
+// engine: tcgen05.mma kind::tf32 with FP32 accuracy from the 3xTF32 split
+// (A = A_hi + A_lo, X = X_hi + X_lo, A X ~ A_hi X_hi + A_hi X_lo + A_lo X_hi,
+// hi = the value with its 13 low mantissa bits cleared).  A CTA owns 128
+// operator rows x 128 columns; K streams in chunks of 32 through two
+// shared-memory stages; the accumulator lives in tensor memory (128 lanes x
+// 128 columns FP32).  Operands are K-major in the no-swizzle canonical
+// layout: 16-byte core rows (4 values of k), row r of an 8-row group at
+// 16 r bytes, 8-row groups 128 bytes apart, the two 16-byte k halves of one
+// MMA step a full 128-row panel apart.  The operator's hi and lo halves are
+// stored in global memory already in that layout, one 32 KB block per
+// (operator, row tile, k chunk).
+namespace tc {
+
+constexpr int kRows = 128, kKC = 32, kThreads = 128;
+// tile widths: multipole -> waves (K = 110, many columns) and waves -> local
+// (K = 684, fewer columns: narrower tiles give more CTAs)
+constexpr int kColsM2x = 128, kColsXl = 64;
+constexpr int kPanel = kRows * 16;                  // bytes of one 4-wide k panel of 128 rows
+constexpr int kHalf = kKC / 4 * kPanel;             // bytes of the operator's hi (or lo) part of a chunk: 16 KB
+// dynamic shared memory of a tile NC columns wide: two stages of operator
+// and column chunks, and the column tables
+constexpr int smem_bytes(int nc) { return 2 * (2 * kHalf + 2 * (kKC / 4 * nc * 16)) + 16 * nc; }
+constexpr long long kWaitCycles = 2000000000LL;     // about one second at the boost clock
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// shared-memory matrix descriptor: start, leading (k-half) and stride
+// (8-row group) byte offsets, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for a barrier phase; false after about a second
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, phase))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+__device__ __forceinline__ float hi_part(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+}  // namespace tc
+
+// Y[dst_n + (r / seg) * seg_stride + r % seg] = sum_k A_op[r][k] X[src_n + k]
+// for the 128 rows of the tile's row block and its <= NC columns.  packed
+// holds [op][row tile][k chunk] blocks of [hi, lo][8 panels][128 rows][4].
+// Software pipeline over two shared-memory stages: right after thread 0
+// issues the MMAs of chunk c, all threads start the operator copy
+// (cp.async) and the column loads (into registers) of chunk c + 1, so the
+// loads overlap the tensor-core work; the columns are split into hi / lo
+// when they are stored.  Every wait is bounded and a timeout sets *err (the
+// kernel still waits, with a bound, for its MMAs and frees its tensor
+// memory).
+template <int NC>
+__global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
+    const GemmTile* __restrict__ tiles, const GemmCol* __restrict__ cols, const float* __restrict__ packed,
+    int n_mtiles, int n_chunks, int K, int R, int seg, long long seg_stride, const float* __restrict__ X,
+    float* __restrict__ Y, int* __restrict__ err) {
+  static_assert(NC % 32 == 0 && NC >= 32 && NC <= 256, "tile width");
+  constexpr int kXHalf = tc::kKC / 4 * NC * 16;     // bytes of the columns' hi (or lo) part of a chunk
+  constexpr int kStageB = 2 * tc::kHalf + 2 * kXHalf;
+  constexpr int kGroups = NC / 32;                  // 8-column groups per warp
+  extern __shared__ __align__(1024) unsigned char smem_tc[];
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ uint32_t tmem_slot;
+  long long* dsts = reinterpret_cast<long long*>(smem_tc + 2 * kStageB);  // [NC]
+  long long* srcs = dsts + NC;                                            // [NC]
+  const GemmTile tl = tiles[blockIdx.x];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int n = tid; n < NC; n += tc::kThreads) {
+    long long sv = -1, dv = 0;
+    if (n < tl.n_cols) {
+      const GemmCol cl = cols[tl.first_col + n];
+      sv = cl.src;
+      dv = cl.dst;
+    }
+    srcs[n] = sv;
+    dsts[n] = dv;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_slot)),
+                 "r"(NC));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    tc::mbar_init(&bars[0]);
+    tc::mbar_init(&bars[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NC >> 3) << 17) |
+                         ((uint32_t)(tc::kRows >> 4) << 24);
+  const int mt = tl.row0 / tc::kRows;
+  const char* ablk = reinterpret_cast<const char*>(packed) + (size_t)(tl.op * n_mtiles + mt) * n_chunks * 2 * tc::kHalf;
+  // lane (j, u) of warp w handles column n = 8 (w + 4 gi) + j and k = 4q + u
+  const int u = lane & 3;
+  float xr[kGroups][tc::kKC / 4];
+  auto issue = [&](int i) {  // local chunk i = operator chunk kc0 + i
+    const int c = tl.kc0 + i;
+    unsigned char* st = smem_tc + (i & 1) * kStageB;
+    const char* ga = ablk + (size_t)c * 2 * tc::kHalf;
+    for (int j = tid; j < 2 * tc::kHalf / 16; j += tc::kThreads) cp_async16(st + 16 * j, ga + 16 * j);
+    cp_async_commit();
+    const int kb = c * tc::kKC;
+#pragma unroll
+    for (int gi = 0; gi < kGroups; ++gi) {
+      const long long sv = srcs[8 * (warp + 4 * gi) + (lane >> 2)];
+#pragma unroll
+      for (int q = 0; q < tc::kKC / 4; ++q) {
+        const int k = kb + 4 * q + u;
+        xr[gi][q] = (sv >= 0 && k < K) ? X[sv + k] : 0.f;
+      }
+    }
+  };
+  __syncthreads();  // column tables visible before the first gather
+  issue(0);
+  bool ok = true;
+  int last = -1;  // last local chunk whose MMAs were committed
+  for (int c = 0; c < tl.nkc; ++c) {
+    unsigned char* st = smem_tc + (c & 1) * kStageB;
+    float* xh = reinterpret_cast<float*>(st + 2 * tc::kHalf);
+    float* xl = reinterpret_cast<float*>(st + 2 * tc::kHalf + kXHalf);
+#pragma unroll
+    for (int gi = 0; gi < kGroups; ++gi) {
+      const int n = 8 * (warp + 4 * gi) + (lane >> 2);
+#pragma unroll
+      for (int q = 0; q < tc::kKC / 4; ++q) {
+        const float h = tc::hi_part(xr[gi][q]);
+        xh[(q * NC + n) * 4 + u] = h;
+        xl[(q * NC + n) * 4 + u] = xr[gi][q] - h;
+      }
+    }
+    cp_async_wait<0>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = tc::smem_u32(st), x0 = a0 + 2 * tc::kHalf;
+#pragma unroll
+      for (int ks = 0; ks < tc::kKC / 8; ++ks) {
+        const uint32_t offa = (uint32_t)ks * 2 * tc::kPanel, offx = (uint32_t)ks * 2 * NC * 16;
+        const uint64_t ah = tc::desc(a0 + offa, tc::kPanel, 128);
+        const uint64_t al = tc::desc(a0 + tc::kHalf + offa, tc::kPanel, 128);
+        const uint64_t bh = tc::desc(x0 + offx, NC * 16, 128);
+        const uint64_t bl = tc::desc(x0 + kXHalf + offx, NC * 16, 128);
+        tc::mma_tf32(tmem, ah, bh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+        tc::mma_tf32(tmem, ah, bl, idesc, 1u);
+        tc::mma_tf32(tmem, al, bh, idesc, 1u);
+      }
+      tc::commit(&bars[c & 1]);
+    }
+    last = c;
+    if (c + 1 < tl.nkc) {
+      // stage (c + 1) & 1 was read by the MMAs of chunk c - 1
+      if (c >= 1 && !tc::mbar_wait(&bars[(c + 1) & 1], (uint32_t)(((c - 1) >> 1) & 1))) ok = false;
+      if (ok) issue(c + 1);
+    }
+  }
+  // every MMA of this CTA is complete once the last committed chunk's phase is
+  if (last >= 0 && !tc::mbar_wait(&bars[last & 1], (uint32_t)((last >> 1) & 1))) ok = false;
+  cp_async_wait<0>();
+  ok = __syncthreads_and(ok) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int r = tl.row0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < tl.n_cols; c0 += 16) {
+      uint32_t v[16];
+      tc::ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (r < R) {
+        float* yr = Y + (long long)(r / seg) * seg_stride + r % seg;
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (c0 + j < tl.n_cols) yr[dsts[c0 + j] + tl.dst_off] = __uint_as_float(v[j]);
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(err, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
+}
+
+constexpr int kXlSplit = 3;  // k ranges of the tensor-core wave -> local GEMM
+
+// L[ldst[col] + r] = sum over the k-range partials of column col (in order)
+__global__ void __launch_bounds__(256) xl_reduce_kernel(int ncols, int R2, const long long* __restrict__ ldst,
+                                                        const float* __restrict__ P, float* __restrict__ L) {
+  const long long total = (long long)ncols * R2;
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total; o += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(o / R2), r = (int)(o - (long long)col * R2);
+    float v = P[o];
+#pragma unroll
+    for (int sp = 1; sp < kXlSplit; ++sp) v += P[(long long)sp * total + o];
+    L[ldst[col] + r] = v;
+  }
+}
+
 // M[parent] = sum of its children's partials, in child order
 template <typename T>
 __global__ void __launch_bounds__(256) shift_reduce_kernel(int E, const ShiftReduce* __restrict__ items,
@@ -1415,6 +1656,16 @@ struct FmmState {
   int m2x_rp = 0, xl_rp = 0;
   DevBuf op_tiles, op_cols;
   DevBuf acc;      // [target row][channel][6 dirs][NPM] accumulated waves
+  // FP32 engine: the same operators packed for the tensor cores (hi / lo
+  // halves in the MMA's shared-memory layout), row tiles and k chunks
+  bool tensor = false;
+  DevBuf m2x_tc, xl_tc;
+  int m2x_mt = 0, m2x_nc = 0, xl_mt = 0, xl_nc = 0;
+  DevBuf tc_err;   // int: set by a tensor-core kernel whose wait timed out
+  // split-K wave -> local: per level the columns' L offsets and the partials
+  DevBuf xl_ldst, xl_partials;
+  std::vector<int> xlr_first, xlr_count;
+  std::vector<long long> xlr_pbase;
   DevBuf leaf_exp;  // per leaf: [2 groups][F, H0, H1, H2][EQ]
   DevBuf eval_items;
   DevBuf p2m_basis;   // [patch position][2 groups][E], geometry only
@@ -1444,6 +1695,15 @@ struct FmmState {
 void fmm_destroy(FmmState* s) { delete s; }
 
 bool fmm_active(const Problem& P) { return P.tree.n_levels - 1 >= 2; }
+
+void fmm_check_waits(Problem& P) {
+  FmmState* S = P.fmm.get();
+  if (!S || !S->tc_err.get()) return;
+  int flag = 0;
+  BP_CUDA(cudaMemcpyAsync(&flag, S->tc_err.get(), sizeof(int), cudaMemcpyDeviceToHost, P.ctx->stream));
+  BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
+  if (flag) throw TimeoutError("a tensor-core FMM kernel timed out waiting for its matrix multiplies");
+}
 
 namespace {
 
@@ -1682,6 +1942,39 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   BP_CUDA(cudaStreamSynchronize(st));
 }
 
+// Operator [lg][k][row] (rows padded to RP, R valid) as tensor-core blocks
+// [lg][row tile of 128][k chunk of 32][hi, lo][8 panels of 4 k][128 rows][4]
+// with hi = the FP32 value with its 13 low mantissa bits cleared and
+// lo = value - hi.
+static std::vector<float> pack_tensor(const std::vector<double>& ops, int nlg, int K, int RP, int R, int& n_mt,
+                                      int& n_ch) {
+  n_mt = (R + tc::kRows - 1) / tc::kRows;
+  n_ch = (K + tc::kKC - 1) / tc::kKC;
+  const size_t blk = 2 * tc::kHalf / sizeof(float);
+  std::vector<float> out((size_t)nlg * n_mt * n_ch * blk, 0.f);
+  for (int lg = 0; lg < nlg; ++lg)
+    for (int mt = 0; mt < n_mt; ++mt)
+      for (int ch = 0; ch < n_ch; ++ch) {
+        float* b = out.data() + ((size_t)(lg * n_mt + mt) * n_ch + ch) * blk;
+        for (int q = 0; q < tc::kKC / 4; ++q)
+          for (int r = 0; r < tc::kRows; ++r)
+            for (int u = 0; u < 4; ++u) {
+              const int row = mt * tc::kRows + r, k = ch * tc::kKC + 4 * q + u;
+              if (row >= R || k >= K) continue;
+              const float a = (float)ops[((size_t)lg * K + k) * RP + row];
+              uint32_t bits;
+              std::memcpy(&bits, &a, 4);
+              bits &= 0xFFFFE000u;
+              float hi;
+              std::memcpy(&hi, &bits, 4);
+              const size_t o = (size_t)q * tc::kRows * 4 + (size_t)r * 4 + u;
+              b[o] = hi;
+              b[blk / 2 + o] = a - hi;
+            }
+      }
+  return out;
+}
+
 // Tabulates, in FP64, the multipole -> plane-wave operator (m2x_kernel on
 // unit multipoles, one per real component) and the accumulated-wave ->
 // local operator (xl_convert_basis_kernel on unit waves) of every level and
@@ -1737,7 +2030,10 @@ static void build_wave_operators(Problem& P, FmmState& S) {
     BP_CUDA(cudaMemcpyAsync(xl.data(), Ob.get(), Ob.bytes(), cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
   }
-  if (S.fp64) {
+  if (S.tensor) {
+    S.m2x_tc = upload(c, pack_tensor(m2x, nlg, R2, S.m2x_rp, KW, S.m2x_mt, S.m2x_nc));
+    S.xl_tc = upload(c, pack_tensor(xl, nlg, KW, S.xl_rp, R2, S.xl_mt, S.xl_nc));
+  } else if (S.fp64) {
     S.m2x_ops = upload(c, m2x);
     S.xl_ops = upload(c, xl);
   } else {
@@ -1925,14 +2221,32 @@ void fmm_setup(Problem& P) {
   S->xl_rp = (R2 + kOpRows - 1) / kOpRows * kOpRows;
   std::vector<GemmTile> otiles;
   std::vector<GemmCol> ocols;
-  auto add_cols = [&](int op, int rows_pad, const std::vector<GemmCol>& cl) {
-    for (size_t c0 = 0; c0 < cl.size(); c0 += kOpCols) {
-      const int n = (int)std::min<size_t>(kOpCols, cl.size() - c0);
+  // FP32 engine: 128 x 128 tensor-core tiles over the valid rows; FP64
+  // engine: 112 x 32 SIMT tiles over the padded rows
+  S->tensor = !S->fp64;
+  const int tile_rows = S->tensor ? tc::kRows : kOpRows;
+  S->m2x_mt = (KW + tc::kRows - 1) / tc::kRows;
+  S->m2x_nc = (R2 + tc::kKC - 1) / tc::kKC;
+  S->xl_mt = (R2 + tc::kRows - 1) / tc::kRows;
+  S->xl_nc = (KW + tc::kKC - 1) / tc::kKC;
+  // k chunks [kc0, kc0 + nkc) of every tile; dst_off shifts its outputs
+  auto add_cols = [&](int op, int rows_pad, const std::vector<GemmCol>& cl, int tile_cols, int kc0, int nkc,
+                      long long dst_off) {
+    for (size_t c0 = 0; c0 < cl.size(); c0 += tile_cols) {
+      const int n = (int)std::min<size_t>(tile_cols, cl.size() - c0);
       const int first = (int)ocols.size();
       ocols.insert(ocols.end(), cl.begin() + c0, cl.begin() + c0 + n);
-      for (int row0 = 0; row0 < rows_pad; row0 += kOpRows) otiles.push_back({op, first, n, row0});
+      for (int row0 = 0; row0 < rows_pad; row0 += tile_rows) otiles.push_back({op, first, n, row0, kc0, nkc, dst_off});
     }
   };
+  // wave -> local on the tensor cores: K split into kXlSplit ranges, each
+  // tile writing a partial; xl_reduce_kernel sums the partials into L
+  const int xl_per = (S->xl_nc + kXlSplit - 1) / kXlSplit;
+  std::vector<long long> xl_ldst;
+  long long xl_part = 0;
+  S->xlr_first.assign(nlev, 0);
+  S->xlr_count.assign(nlev, 0);
+  S->xlr_pbase.assign(nlev, 0);
   S->m2x_tfirst.assign(nlev, 0);
   S->m2x_tcount.assign(nlev, 0);
   S->xlt_first.assign(nlev, 0);
@@ -1947,7 +2261,7 @@ void fmm_setup(Problem& P) {
       for (int k : src_lev[lev])
         for (int ch = g ? 8 : 0; ch < (g ? kCh : 8); ++ch)
           cl.push_back({((long long)k * kCh + ch) * R2, ((long long)k * 6 * kCh + ch) * 2 * NPM});
-      add_cols(2 * (lev - 1) + g, S->m2x_rp, cl);
+      add_cols(2 * (lev - 1) + g, S->tensor ? KW : S->m2x_rp, cl, S->tensor ? tc::kColsM2x : kOpCols, 0, S->m2x_nc, 0);
     }
     S->m2x_tcount[lev] = (int)otiles.size() - S->m2x_tfirst[lev];
     S->xlt_first[lev] = (int)xlt.size();
@@ -1957,20 +2271,42 @@ void fmm_setup(Problem& P) {
     }
     S->xlt_count[lev] = (int)xlt.size() - S->xlt_first[lev];
     S->xlc_tfirst[lev] = (int)otiles.size();
+    S->xlr_first[lev] = (int)xl_ldst.size();
+    S->xlr_pbase[lev] = xl_part;
+    const long long ncl = (long long)S->xlt_count[lev] * kCh;  // columns of this level
     for (int g = 0; g < 2; ++g) {
       std::vector<GemmCol> cl;
       for (int q = S->xlt_first[lev]; q < S->xlt_first[lev] + S->xlt_count[lev]; ++q)
-        for (int ch = g ? 8 : 0; ch < (g ? kCh : 8); ++ch)
-          cl.push_back({((long long)xlt[q].acc_row * kCh + ch) * KW, ((long long)xlt[q].node * kCh + ch) * R2});
-      add_cols(2 * (lev - 1) + g, S->xl_rp, cl);
+        for (int ch = g ? 8 : 0; ch < (g ? kCh : 8); ++ch) {
+          GemmCol col{((long long)xlt[q].acc_row * kCh + ch) * KW, ((long long)xlt[q].node * kCh + ch) * R2};
+          if (S->tensor) {  // output goes to the column's partial slot
+            xl_ldst.push_back(col.dst);
+            col.dst = (long long)(xl_ldst.size() - 1 - S->xlr_first[lev]) * R2;
+          }
+          cl.push_back(col);
+        }
+      if (!S->tensor) {
+        add_cols(2 * (lev - 1) + g, S->xl_rp, cl, kOpCols, 0, 0, 0);
+        continue;
+      }
+      for (int sp = 0; sp < kXlSplit; ++sp) {
+        const int kc0 = sp * xl_per, nkc = std::min(xl_per, S->xl_nc - kc0);
+        if (nkc > 0) add_cols(2 * (lev - 1) + g, R2, cl, tc::kColsXl, kc0, nkc, xl_part + sp * ncl * R2);
+      }
     }
     S->xlc_tcount[lev] = (int)otiles.size() - S->xlc_tfirst[lev];
+    S->xlr_count[lev] = (int)xl_ldst.size() - S->xlr_first[lev];
+    if (S->tensor) xl_part += (long long)kXlSplit * ncl * R2;
   }
   S->op_tiles = upload(c, otiles);
   S->op_cols = upload(c, ocols);
   S->xl_targets = upload(c, xlt);
   S->xl_entries = upload(c, xle);
   S->acc.alloc(c, celem * kCh * 6 * (size_t)NPM * std::max<size_t>(1, xlt.size()));
+  if (S->tensor) {
+    S->xl_ldst = upload(c, xl_ldst);
+    S->xl_partials.alloc(c, sizeof(float) * (size_t)std::max<long long>(1, xl_part));
+  }
   S->lstreams.assign(nlev, nullptr);
   S->ev_m.assign(nlev, nullptr);
   S->ev_x.assign(nlev, nullptr);
@@ -2016,6 +2352,12 @@ void fmm_setup(Problem& P) {
     ensure_dynamic_smem((const void*)l2p_eval_kernel<float>, S->smem_eval);
   }
   ensure_dynamic_smem((const void*)m2x_kernel<double>, S->smem_m2x);
+  if (S->tensor) {
+    ensure_dynamic_smem((const void*)op_gemm_tc_kernel<tc::kColsM2x>, tc::smem_bytes(tc::kColsM2x));
+    ensure_dynamic_smem((const void*)op_gemm_tc_kernel<tc::kColsXl>, tc::smem_bytes(tc::kColsXl));
+  }
+  S->tc_err.alloc(c, sizeof(int));
+  BP_CUDA(cudaMemsetAsync(S->tc_err.get(), 0, sizeof(int), c->stream));
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
   BP_CUDA(cudaStreamSynchronize(c->stream));
@@ -2056,6 +2398,31 @@ void fmm_setup(Problem& P) {
 // that level's multipoles are complete; L2L into a level waits for the
 // level's X2L.  With st != nullptr (stage profiling) everything runs in
 // order on one stream.
+// One operator GEMM launch over tiles [first, first + count): tcgen05 for the
+// FP32 engine, the SIMT kernel for the FP64 engine.
+template <typename T>
+static void launch_op_gemm(FmmState& S, int first, int count, const T* simt_ops, const float* tc_ops, int n_mt,
+                           int n_ch, int K, int RP, int R, int seg, long long seg_stride, const T* X, T* Y,
+                           cudaStream_t q, int tc_cols) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (S.tensor) {
+      if (tc_cols == tc::kColsM2x)
+        op_gemm_tc_kernel<tc::kColsM2x><<<count, tc::kThreads, tc::smem_bytes(tc::kColsM2x), q>>>(
+            S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride, X,
+            Y, S.tc_err.as<int>());
+      else
+        op_gemm_tc_kernel<tc::kColsXl><<<count, tc::kThreads, tc::smem_bytes(tc::kColsXl), q>>>(
+            S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride, X,
+            Y, S.tc_err.as<int>());
+      BP_LAUNCH_CHECK();
+      return;
+    }
+  }
+  op_gemm_kernel<T><<<count, kOpThreads, S.smem_op, q>>>(S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(),
+                                                          simt_ops, K, RP, R, seg, seg_stride, X, Y);
+  BP_LAUNCH_CHECK();
+}
+
 template <typename T>
 static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* x, double* y, StageTimes* st,
                     cudaStream_t s) {
@@ -2080,10 +2447,9 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   auto level_x = [&](int lev, cudaStream_t q) {
     if (S.m2x_tcount[lev]) {
       begin(3, q);
-      op_gemm_kernel<T><<<S.m2x_tcount[lev], kOpThreads, S.smem_op, q>>>(
-          S.op_tiles.as<GemmTile>() + S.m2x_tfirst[lev], S.op_cols.as<GemmCol>(), S.m2x_ops.as<T>(), R2, S.m2x_rp,
-          KW, 2 * NPM, (long long)kCh * 2 * NPM, reinterpret_cast<const T*>(M), reinterpret_cast<T*>(W));
-      BP_LAUNCH_CHECK();
+      launch_op_gemm<T>(S, S.m2x_tfirst[lev], S.m2x_tcount[lev], S.m2x_ops.as<T>(), S.m2x_tc.as<float>(), S.m2x_mt,
+                        S.m2x_nc, R2, S.m2x_rp, KW, 2 * NPM, (long long)kCh * 2 * NPM,
+                        reinterpret_cast<const T*>(M), reinterpret_cast<T*>(W), q, tc::kColsM2x);
       end(1);
     }
     if (S.xlt_count[lev]) {
@@ -2093,11 +2459,23 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
                                                       S.xlt_count[lev], S.xl_entries.as<XlEntry>(), W,
                                                       S.acc.as<C>());
       BP_LAUNCH_CHECK();
-      op_gemm_kernel<T><<<S.xlc_tcount[lev], kOpThreads, S.smem_op, q>>>(
-          S.op_tiles.as<GemmTile>() + S.xlc_tfirst[lev], S.op_cols.as<GemmCol>(), S.xl_ops.as<T>(), KW, S.xl_rp,
-          R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()), reinterpret_cast<T*>(Lx));
-      BP_LAUNCH_CHECK();
-      end(2);
+      if (S.tensor) {  // k-range partials, then their fixed-order sum into L
+        launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops.as<T>(), S.xl_tc.as<float>(), S.xl_mt,
+                          S.xl_nc, KW, S.xl_rp, R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()),
+                          reinterpret_cast<T*>(S.xl_partials.as<float>()), q, tc::kColsXl);
+        const long long total = (long long)S.xlr_count[lev] * R2;
+        const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
+        xl_reduce_kernel<<<grid, 256, 0, q>>>(S.xlr_count[lev], R2, S.xl_ldst.as<long long>() + S.xlr_first[lev],
+                                              S.xl_partials.as<float>() + S.xlr_pbase[lev],
+                                              reinterpret_cast<float*>(Lx));
+        BP_LAUNCH_CHECK();
+        end(3);
+      } else {
+        launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops.as<T>(), S.xl_tc.as<float>(), S.xl_mt,
+                          S.xl_nc, KW, S.xl_rp, R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()),
+                          reinterpret_cast<T*>(Lx), q, tc::kColsXl);
+        end(2);
+      }
     }
   };
   auto fork_x = [&](int lev) {
