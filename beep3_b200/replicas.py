@@ -19,20 +19,47 @@ def shard(items: Sequence[Any], rank: int, world: int) -> list[tuple[int, Any]]:
     return [(i, it) for i, it in enumerate(items) if i % world == rank]
 
 
+class ReplicaError(RuntimeError):
+    """Raised on rank 0 when work items failed on some rank; ``failures``
+    maps item index -> (rank, error text)."""
+
+    def __init__(self, failures: dict[int, tuple[int, str]]):
+        lines = [f"item {i} on rank {r}: {msg}" for i, (r, msg) in sorted(failures.items())]
+        super().__init__("replicated work failed:\n  " + "\n  ".join(lines))
+        self.failures = failures
+
+
 def run_replicated(items: Sequence[Any], fn: Callable[[Any], Any], dist=None) -> list[Any] | None:
     """Runs ``fn`` over this rank's share and gathers all results on rank 0
     in item order (None on the other ranks).  ``dist`` is torch.distributed
-    (already initialised) or None for a single process."""
+    (already initialised) or None for a single process.
+
+    An item whose ``fn`` raises does not take its rank out of the gather:
+    the rank reports the error text instead of a result, the gather
+    completes on every rank, and rank 0 raises ReplicaError naming the
+    failed items.  (A rank that dies outright is caught by the process
+    group's timeout, which the caller sets.)"""
     if dist is None or not dist.is_initialized():
         return [fn(it) for it in items]
     rank, world = dist.get_rank(), dist.get_world_size()
-    mine = [(i, fn(it)) for i, it in shard(items, rank, world)]
+    mine = []
+    for i, it in shard(items, rank, world):
+        try:
+            mine.append((i, True, fn(it)))
+        except Exception as e:  # reported to rank 0, not raised here
+            mine.append((i, False, f"{type(e).__name__}: {e}"))
     gathered = [None] * world if rank == 0 else None
     dist.gather_object(mine, gathered, dst=0)
     if rank != 0:
         return None
     out: list[Any] = [None] * len(items)
-    for part in gathered:
-        for i, r in part:
-            out[i] = r
+    failures: dict[int, tuple[int, str]] = {}
+    for r, part in enumerate(gathered):
+        for i, ok, v in part:
+            if ok:
+                out[i] = v
+            else:
+                failures[i] = (r, v)
+    if failures:
+        raise ReplicaError(failures)
     return out

@@ -5,7 +5,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from beep3_b200.replicas import run_replicated, shard
+from beep3_b200.replicas import ReplicaError, run_replicated, shard
 
 
 def test_shard_round_robin():
@@ -58,3 +58,45 @@ def test_run_replicated_gloo_world2():
 
 def test_single_process_path():
     assert run_replicated([1, 2, 3], lambda v: v + 1, None) == [2, 3, 4]
+
+
+def _failing(v):
+    if v == 3:
+        raise ValueError("pose 3 has no solution")
+    return v + 100
+
+
+def _worker_fail(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        try:
+            res = run_replicated(list(range(6)), _failing, dist)
+            q.put(("ok", rank, res))
+        except ReplicaError as e:
+            q.put(("error", rank, e.failures))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_failing_item_reported_on_rank0_without_hang():
+    """Item 3 (rank 1) raises; both ranks finish the gather and rank 0 gets
+    a ReplicaError naming it, while rank 1 returns normally."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_fail, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    by_rank = {r: (kind, v) for kind, r, v in got}
+    assert by_rank[0][0] == "error" and set(by_rank[0][1]) == {3}
+    assert by_rank[0][1][3][0] == 1 and "no solution" in by_rank[0][1][3][1]
+    assert by_rank[1] == ("ok", None)
