@@ -213,6 +213,17 @@ __device__ __forceinline__ void patch_charges(const double* area, const double* 
   q[11] = (T)(a * h);
 }
 
+// ---------------------------------------------------------------- async copies
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------- P2M
 // The multipole basis of a patch in its childless node (yformmp without the
 // charge: i_l(beta r) P_l^m(cos theta) e^{-i m phi} * scale factors, per
@@ -269,7 +280,8 @@ __global__ void __launch_bounds__(64) p2m_basis_kernel(const __grid_constant__ T
 
 // One block per childless node; thread (g, e) accumulates coefficient e of
 // the group's channels (8 for group 0, 4 for group 1) over the node's
-// patches, charges staged per chunk in shared memory.
+// patches.  Per chunk of 32 patches the basis rows (contiguous) arrive in
+// shared memory by one cp.async burst while the charges are computed.
 template <typename T>
 __global__ void __launch_bounds__(128) p2m_kernel(const P2mItem* __restrict__ items, int E,
                                                   const int32_t* __restrict__ contents,
@@ -280,6 +292,8 @@ __global__ void __launch_bounds__(128) p2m_kernel(const P2mItem* __restrict__ it
                                                   typename C2T<T>::type* __restrict__ M) {
   using C = typename C2T<T>::type;
   __shared__ T q[kP2mChunk][kCh];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bsm = reinterpret_cast<C*>(smem_raw);  // [kP2mChunk][2][E]
   const P2mItem it = items[blockIdx.x];
   const int g = threadIdx.x >= 64 ? 1 : 0, e = threadIdx.x - 64 * g;
   const int c0 = g ? 8 : 0, nc = g ? 4 : 8;
@@ -289,15 +303,22 @@ __global__ void __launch_bounds__(128) p2m_kernel(const P2mItem* __restrict__ it
   for (int base = 0; base < it.count; base += kP2mChunk) {
     const int cnt = min(kP2mChunk, it.count - base);
     __syncthreads();
+    {
+      const char* src = reinterpret_cast<const char*>(basis + (size_t)(it.pos + base) * 2 * E);
+      const int n16 = cnt * 2 * E * (int)sizeof(C) / 16;
+      for (int j = threadIdx.x; j < n16; j += blockDim.x) cp_async16(smem_raw + 16 * j, src + 16 * j);
+      cp_async_commit();
+    }
     if (threadIdx.x < cnt) {
       T qq[kCh];
       patch_charges<T>(area, normal, eps, x, n, contents[it.start + base + threadIdx.x], qq);
 #pragma unroll
       for (int c = 0; c < kCh; ++c) q[threadIdx.x][c] = qq[c];
     }
+    cp_async_wait<0>();
     __syncthreads();
     if (e < E) {
-      const C* b = basis + ((size_t)(it.pos + base) * 2 + g) * E + e;
+      const C* b = bsm + (size_t)g * E + e;
 #pragma unroll 4
       for (int p = 0; p < cnt; ++p) {
         const C v = b[(size_t)p * 2 * E];
@@ -557,6 +578,7 @@ __global__ void __launch_bounds__(kM2xThreads) m2x_kernel(const __grid_constant_
 struct XlTarget {
   int node, acc_row;             // target node; its row block of the ACC scratch
   int first_entry, n_entries;    // interactions sorted by direction
+  int dir_start[7];              // direction d: entries [first + dir_start[d], first + dir_start[d + 1])
 };
 // One diagonal translation: source node, direction, and the translation
 // factor's index combo = up * 343 + (a+3) * 49 + (b+3) * 7 + (c+3) with
@@ -572,75 +594,66 @@ constexpr int kXlThreads = kXlTargets * kPairLanes;
 constexpr int kXlChannels = 4;                    // channels per translate block (one screening group)
 constexpr int kXlUnroll = 8;
 
-// One block per (4 targets of a level, 4 channels); thread (target tl,
-// lane i = plane wave): per direction run of the target's entries, the sum
-// of W[src][dir][ch][i] * factor[combo][i] is kept in registers and stored
-// as ACC[acc_row][ch][dir][i] (re, im); directions without entries store 0.
+constexpr int kXlDirThreads = 6 * kPairLanes;    // one lane group per direction
+
+// One block per (target, 4 channels); thread (direction d, lane i = plane
+// wave) sums W[src][d][ch][i] * factor[combo][i] over the target's entries
+// of direction d, in registers, and stores ACC[acc_row][ch][d][i] (re, im);
+// a direction without entries stores 0.  The six directions of a target run
+// side by side.
 template <typename T>
-__global__ void __launch_bounds__(kXlThreads) xl_translate_kernel(const __grid_constant__ Tables<T> tb, int parent_level,
-                                                                  const XlTarget* __restrict__ targets, int n_targets,
-                                                                  const XlEntry* __restrict__ entries,
-                                                                  const typename C2T<T>::type* __restrict__ W,
-                                                                  typename C2T<T>::type* __restrict__ ACC) {
+__global__ void __launch_bounds__(kXlDirThreads) xl_translate_kernel(const __grid_constant__ Tables<T> tb,
+                                                                     int parent_level,
+                                                                     const XlTarget* __restrict__ targets,
+                                                                     int n_targets,
+                                                                     const XlEntry* __restrict__ entries,
+                                                                     const typename C2T<T>::type* __restrict__ W,
+                                                                     typename C2T<T>::type* __restrict__ ACC) {
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
-  constexpr int U = sizeof(T) == 4 ? kXlUnroll : kXlUnroll / 2;  // loads in flight per thread
+  constexpr int U = sizeof(T) == 4 ? kXlUnroll / 2 : kXlUnroll / 4;  // entries in flight per thread
   const int NPM = tb.np_max;
-  const int tq = blockIdx.x / (kCh / CB);
+  const int t = blockIdx.x / (kCh / CB);
   const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
-  const int tl = threadIdx.x / kPairLanes, i = threadIdx.x - tl * kPairLanes;
-  const int t = tq * kXlTargets + tl;
+  const int d = threadIdx.x / kPairLanes, i = threadIdx.x - d * kPairLanes;
   const int lg = 2 * parent_level + (ch0 >= 8 ? 1 : 0);
   if (t >= n_targets || i >= NPM) return;
   const XlTarget tg = targets[t];
   const int np = tb.nexptotp[lg];
   // ACC[acc_row][ch][dir][i]: 6 * NPM complex per (target, channel)
-  C* out = ACC + ((size_t)tg.acc_row * kCh + ch0) * 6 * NPM + i;
-  if (i >= np) {  // plane waves beyond this level's count are never read
-    for (int c = 0; c < CB; ++c)
-      for (int d = 0; d < 6; ++d) out[((size_t)c * 6 + d) * NPM] = cmk<C>(0, 0);
-    return;
-  }
-  const XlEntry* ent = entries + tg.first_entry;
-  const int ne = tg.n_entries;
-  const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
+  C* out = ACC + (((size_t)tg.acc_row * kCh + ch0) * 6 + d) * NPM + i;
   C a[CB];
 #pragma unroll
   for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
-  int cur = 0;  // next direction to store
-  for (int k0 = 0; k0 < ne; k0 += U) {
-    XlEntry en[U];
-    C tt[U], w[U][CB];
+  if (i < np) {  // plane waves beyond this level's count are never read: they stay 0
+    const XlEntry* ent = entries + tg.first_entry + tg.dir_start[d];
+    const int ne = tg.dir_start[d + 1] - tg.dir_start[d];
+    const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
+    const C* Wd = W + ((size_t)d * kCh + ch0) * NPM + i;
+    for (int k0 = 0; k0 < ne; k0 += U) {
+      int src[U], combo[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) en[u] = ent[min(k0 + u, ne - 1)];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      tt[u] = tc[(size_t)en[u].combo * NPM];
-#pragma unroll
-      for (int c = 0; c < CB; ++c) w[u][c] = W[(((size_t)en[u].src * 6 + en[u].dir) * kCh + ch0 + c) * NPM + i];
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (k0 + u < ne) {
-        while (cur < en[u].dir) {  // close the current direction (and any without entries)
-#pragma unroll
-          for (int c = 0; c < CB; ++c) {
-            out[((size_t)c * 6 + cur) * NPM] = a[c];
-            a[c] = cmk<C>(0, 0);
-          }
-          ++cur;
-        }
-#pragma unroll
-        for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
+      for (int u = 0; u < U; ++u) {
+        const XlEntry en = ent[min(k0 + u, ne - 1)];
+        src[u] = en.src;
+        combo[u] = en.combo;
       }
+      C tt[U], w[U][CB];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        tt[u] = tc[(size_t)combo[u] * NPM];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) w[u][c] = Wd[((size_t)src[u] * 6 * kCh + c) * NPM];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (k0 + u < ne)
+#pragma unroll
+          for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
     }
   }
-  for (; cur < 6; ++cur)
 #pragma unroll
-    for (int c = 0; c < CB; ++c) {
-      out[((size_t)c * 6 + cur) * NPM] = a[c];
-      a[c] = cmk<C>(0, 0);
-    }
+  for (int c = 0; c < CB; ++c) out[(size_t)c * 6 * NPM] = a[c];
 }
 
 // Conversion of one accumulated-wave vector to a local expansion, applied
@@ -1033,15 +1046,28 @@ __global__ void __launch_bounds__(kEvalThreads) l2p_eval_kernel(int nt, const Le
   const int EQ = (nt + 3) * (nt + 4) / 2, EF = (nt + 2) * (nt + 3) / 2;
   C* Ds = reinterpret_cast<C*>(smem_raw);                   // [2][4][EQ]
   T* part = reinterpret_cast<T*>(Ds + 8 * EQ);              // [4 slices][4 sums][kEvalChunk]
+  // FP32: the item's whole basis block (contiguous, 80 KB) is copied into
+  // shared memory in one cp.async burst, so every load is in flight at once
+  constexpr bool kStageQ = sizeof(T) == 4;
+  C* Qs = reinterpret_cast<C*>(part + 16 * kEvalChunk);     // [2][EQ][kEvalChunk]
   const LeafItem it = items[blockIdx.x];
+  const C* Qb = Q + (size_t)blockIdx.x * 2 * EQ * kEvalChunk;
+  if (kStageQ) {
+    const char* src = reinterpret_cast<const char*>(Qb);
+    char* dst = reinterpret_cast<char*>(Qs);
+    const int n16 = 2 * EQ * kEvalChunk * (int)sizeof(C) / 16;
+    for (int j = threadIdx.x; j < n16; j += blockDim.x) cp_async16(dst + 16 * j, src + 16 * j);
+    cp_async_commit();
+  }
   for (int o = threadIdx.x; o < 8 * EQ; o += blockDim.x) Ds[o] = D[(size_t)it.leaf * 8 * EQ + o];
+  if (kStageQ) cp_async_wait<0>();
   __syncthreads();
   const int s = threadIdx.x / kEvalChunk, k = threadIdx.x - s * kEvalChunk;
   const int g = s >> 1, half = EQ / 2;
   const int e0 = (s & 1) ? half : 0, e1 = (s & 1) ? EQ : half;
   T f = 0, h0 = 0, h1 = 0, h2 = 0;
   if (k < it.count) {
-    const C* q = Q + ((size_t)blockIdx.x * 2 + g) * EQ * kEvalChunk + k;
+    const C* q = (kStageQ ? Qs : Qb) + (size_t)g * EQ * kEvalChunk + k;
     const C* F = Ds + g * 4 * EQ;
 #pragma unroll 8
     for (int e = e0; e < e1; ++e) {
@@ -1119,16 +1145,6 @@ __global__ void __launch_bounds__(64) shift_basis_kernel(const __grid_constant__
     col[2 * o + 1] = acc[o].y;
   }
   for (int r = R + threadIdx.x; r < RP; r += blockDim.x) col[r] = 0;
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // Operator form of M2M and L2L as a gather-GEMM.  A tile is up to 16
@@ -1369,7 +1385,7 @@ namespace tc {
 constexpr int kRows = 128, kKC = 32, kThreads = 128;
 // tile widths: multipole -> waves (K = 110, many columns) and waves -> local
 // (K = 684, fewer columns: narrower tiles give more CTAs)
-constexpr int kColsM2x = 128, kColsXl = 64;
+constexpr int kColsM2x = 64, kColsXl = 64;
 constexpr int kPanel = kRows * 16;                  // bytes of one 4-wide k panel of 128 rows
 constexpr int kHalf = kKC / 4 * kPanel;             // bytes of the operator's hi (or lo) part of a chunk: 16 KB
 // dynamic shared memory of a tile NC columns wide: two stages of operator
@@ -1649,7 +1665,7 @@ struct FmmState {
   DevBuf M, L, W;  // expansions and plane waves
   DevBuf p2m_items, xl_targets, xl_entries, leaf_items;
   int n_p2m = 0, n_leaf = 0;
-  size_t smem_shift = 0, smem_m2x = 0, smem_prep = 0, smem_eval = 0, smem_op = 0, smem_xlb = 0;
+  size_t smem_p2m = 0, smem_shift = 0, smem_m2x = 0, smem_prep = 0, smem_eval = 0, smem_op = 0, smem_xlb = 0;
   // operator form of multipole -> plane waves and accumulated waves -> local
   DevBuf m2x_ops;  // [lg][2E][m2x_rp]
   DevBuf xl_ops;   // [lg][12 NPM][xl_rp]
@@ -2088,8 +2104,9 @@ void fmm_setup(Problem& P) {
     for (int t = 0; t < 8; ++t) {
       const int ck = nd.children[t];
       if (ck < 0 || (flags(ck) & TREE_SHADOW)) continue;
-      XlTarget tg{ck, 0, (int)xle.size(), 0};
-      for (int dir = 0; dir < 6; ++dir)
+      XlTarget tg{ck, 0, (int)xle.size(), 0, {0, 0, 0, 0, 0, 0, 0}};
+      for (int dir = 0; dir < 6; ++dir) {
+        tg.dir_start[dir] = (int)xle.size() - tg.first_entry;
         for (int q : by_target_dir[t * 6 + dir]) {
           const RawInteraction& r = table[q];
           const int nbk = nd.neighbours[r.nb];
@@ -2111,7 +2128,9 @@ void fmm_setup(Problem& P) {
           xle.push_back(e);
           is_source[sk] = 1;
         }
+      }
       tg.n_entries = (int)xle.size() - tg.first_entry;
+      tg.dir_start[6] = tg.n_entries;
       if (tg.n_entries == 0) continue;
       written[ck] = 1;
       xlt_lev[nd.level + 1].push_back(tg);
@@ -2307,11 +2326,13 @@ void fmm_setup(Problem& P) {
     S->xl_ldst = upload(c, xl_ldst);
     S->xl_partials.alloc(c, sizeof(float) * (size_t)std::max<long long>(1, xl_part));
   }
+  int prio_lo = 0, prio_hi = 0;  // level streams share the FMM stream's (highest) priority
+  BP_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   S->lstreams.assign(nlev, nullptr);
   S->ev_m.assign(nlev, nullptr);
   S->ev_x.assign(nlev, nullptr);
   for (int lev = 0; lev < nlev; ++lev) {
-    BP_CUDA(cudaStreamCreateWithFlags(&S->lstreams[lev], cudaStreamNonBlocking));
+    BP_CUDA(cudaStreamCreateWithPriority(&S->lstreams[lev], cudaStreamNonBlocking, prio_hi));
     BP_CUDA(cudaEventCreateWithFlags(&S->ev_m[lev], cudaEventDisableTiming));
     BP_CUDA(cudaEventCreateWithFlags(&S->ev_x[lev], cudaEventDisableTiming));
   }
@@ -2326,6 +2347,7 @@ void fmm_setup(Problem& P) {
   const int E = S->E, NT = S->nt;
   if (E > kPairLanes) throw std::invalid_argument("FMM order above 9 is not supported");
   S->smem_shift = 4 * celem * E;
+  S->smem_p2m = celem * (size_t)kP2mChunk * 2 * E;
   S->smem_gemm = (S->fp64 ? 8 : 4) * (size_t)(2 * E) * (((2 * E + 3) & ~3) + kTileCols);
   S->smem_m2x = sizeof(double2) * (size_t)(4 * kM2xChannels * E + 6 * kM2xChannels * 64);  // FP64 tabulation
   S->smem_xlb = sizeof(double2) * (size_t)(6 * S->np_max + 6 * 64);
@@ -2333,7 +2355,8 @@ void fmm_setup(Problem& P) {
                (kOpRows + kOpCols);
   const int EQ = (NT + 3) * (NT + 4) / 2;
   S->smem_prep = celem * 2 * 24 * (size_t)EQ;
-  S->smem_eval = celem * 8 * (size_t)EQ + (S->fp64 ? 8 : 4) * (size_t)16 * kEvalChunk;
+  S->smem_eval = celem * 8 * (size_t)EQ + (S->fp64 ? 8 : 4) * (size_t)16 * kEvalChunk +
+                 (S->fp64 ? 0 : celem * 2 * (size_t)EQ * kEvalChunk);
   S->leaf_exp.alloc(P.ctx, celem * 8 * (size_t)EQ * std::max(1, S->n_leaf));
   S->p2m_basis.alloc(P.ctx, celem * 2 * (size_t)E * std::max(1, p2m_rows));
   S->eval_basis.alloc(P.ctx, celem * 2 * (size_t)EQ * kEvalChunk * std::max(1, S->n_eval));
@@ -2345,11 +2368,13 @@ void fmm_setup(Problem& P) {
     ensure_dynamic_smem((const void*)shift_gemm_kernel<double>, S->smem_gemm);
     ensure_dynamic_smem((const void*)l2p_prep_kernel<double>, S->smem_prep);
     ensure_dynamic_smem((const void*)l2p_eval_kernel<double>, S->smem_eval);
+    ensure_dynamic_smem((const void*)p2m_kernel<double>, S->smem_p2m);
   } else {
     ensure_dynamic_smem((const void*)op_gemm_kernel<float>, S->smem_op);
     ensure_dynamic_smem((const void*)shift_gemm_kernel<float>, S->smem_gemm);
     ensure_dynamic_smem((const void*)l2p_prep_kernel<float>, S->smem_prep);
     ensure_dynamic_smem((const void*)l2p_eval_kernel<float>, S->smem_eval);
+    ensure_dynamic_smem((const void*)p2m_kernel<float>, S->smem_p2m);
   }
   ensure_dynamic_smem((const void*)m2x_kernel<double>, S->smem_m2x);
   if (S->tensor) {
@@ -2454,8 +2479,8 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
     }
     if (S.xlt_count[lev]) {
       begin(4, q);
-      const int nb = (S.xlt_count[lev] + kXlTargets - 1) / kXlTargets * (kCh / kXlChannels);
-      xl_translate_kernel<T><<<nb, kXlThreads, 0, q>>>(tb, lev - 1, S.xl_targets.as<XlTarget>() + S.xlt_first[lev],
+      const int nb = S.xlt_count[lev] * (kCh / kXlChannels);
+      xl_translate_kernel<T><<<nb, kXlDirThreads, 0, q>>>(tb, lev - 1, S.xl_targets.as<XlTarget>() + S.xlt_first[lev],
                                                       S.xlt_count[lev], S.xl_entries.as<XlEntry>(), W,
                                                       S.acc.as<C>());
       BP_LAUNCH_CHECK();
@@ -2496,7 +2521,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   begin(1, s);
   int l_p2m = 0;
   if (S.n_p2m) {
-    p2m_kernel<T><<<S.n_p2m, 128, 0, s>>>(S.p2m_items.as<P2mItem>(), S.E, contents, P.d_area.as<double>(),
+    p2m_kernel<T><<<S.n_p2m, 128, S.smem_p2m, s>>>(S.p2m_items.as<P2mItem>(), S.E, contents, P.d_area.as<double>(),
                                           P.d_normal.as<double>(), P.d_eps.as<double>(), x, P.n,
                                           S.p2m_basis.as<C>(), M);
     BP_LAUNCH_CHECK();

@@ -172,7 +172,12 @@ void matvec_setup(Problem& P) {
   P.d_yfar.alloc(c, bytes);
   P.d_gx.alloc(c, bytes);
   P.d_gy.alloc(c, bytes);
-  BP_CUDA(cudaStreamCreateWithFlags(&P.side, cudaStreamNonBlocking));
+  // the FMM is the matvec's critical path and the near field is a
+  // bandwidth-bound stream that can fill the gaps: the FMM streams get the
+  // highest priority, so their blocks are scheduled first
+  int lo = 0, hi = 0;
+  BP_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  BP_CUDA(cudaStreamCreateWithPriority(&P.side, cudaStreamNonBlocking, hi));
   BP_CUDA(cudaEventCreateWithFlags(&P.ev_fork, cudaEventDisableTiming));
   BP_CUDA(cudaEventCreateWithFlags(&P.ev_join, cudaEventDisableTiming));
 }
@@ -227,7 +232,8 @@ static bool ensure_graph(Problem& P) {
     P.graph_failed = true;
     return false;
   }
-  e = cudaGraphInstantiate(&P.graph, g, 0);
+  // node priorities (taken from the capturing streams) are kept in the graph
+  e = cudaGraphInstantiateWithFlags(&P.graph, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
     cudaGetLastError();

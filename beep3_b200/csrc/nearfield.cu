@@ -42,6 +42,7 @@ constexpr int kAsmRows = 8;      // rows per assembly work item
 constexpr int kAsmThreads = 256;
 constexpr int kApplyRows = 64;   // rows per apply work item
 constexpr int kApplyThreads = 256;
+constexpr int kApplyBlocksPerSm = 8;  // resident apply blocks per SM (persistent grid)
 constexpr double kOneOver4Pi = 0.07957747154594767;  // 1/(4 pi)
 
 template <typename T>
@@ -259,10 +260,14 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
     const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
     const T* __restrict__ coef, const double* __restrict__ diag, int n, const double* __restrict__ x,
-    double* __restrict__ y) {
+    double* __restrict__ y, int n_items) {
   extern __shared__ unsigned char smem_raw[];
   T* sf = reinterpret_cast<T*>(smem_raw);
-  const NfItem it = items[blockIdx.x];
+  // persistent: a few blocks per SM stride over the items, leaving room on
+  // every SM for the far-field kernels that run beside the near field
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  if (item != blockIdx.x) __syncthreads();  // the previous item's readers of sf / sh are done
+  const NfItem it = items[item];
   const int64_t c0 = col_off[it.leaf];
   const int ncols = (int)(col_off[it.leaf + 1] - c0);
   T* sh = sf + ncols;
@@ -282,19 +287,26 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     const V4* rowp = blk + (int64_t)(it.row_begin + r) * ncols;
     T accf = 0, acch = 0;
     int cc = lane;
+    // eight 16-byte (FP32) / 32-byte (FP64) coefficient loads in flight per lane
+    for (; cc + 224 < ncols; cc += 256) {
+      V4 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = ld_stream(rowp + cc + 32 * u);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        accf += v[u].y * sf[cc + 32 * u] - v[u].x * sh[cc + 32 * u];
+        acch += v[u].w * sf[cc + 32 * u] - v[u].z * sh[cc + 32 * u];
+      }
+    }
     for (; cc + 96 < ncols; cc += 128) {
-      const V4 v0 = ld_stream(rowp + cc);
-      const V4 v1 = ld_stream(rowp + cc + 32);
-      const V4 v2 = ld_stream(rowp + cc + 64);
-      const V4 v3 = ld_stream(rowp + cc + 96);
-      accf += v0.y * sf[cc] - v0.x * sh[cc];
-      acch += v0.w * sf[cc] - v0.z * sh[cc];
-      accf += v1.y * sf[cc + 32] - v1.x * sh[cc + 32];
-      acch += v1.w * sf[cc + 32] - v1.z * sh[cc + 32];
-      accf += v2.y * sf[cc + 64] - v2.x * sh[cc + 64];
-      acch += v2.w * sf[cc + 64] - v2.z * sh[cc + 64];
-      accf += v3.y * sf[cc + 96] - v3.x * sh[cc + 96];
-      acch += v3.w * sf[cc + 96] - v3.z * sh[cc + 96];
+      V4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = ld_stream(rowp + cc + 32 * u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        accf += v[u].y * sf[cc + 32 * u] - v[u].x * sh[cc + 32 * u];
+        acch += v[u].w * sf[cc + 32 * u] - v[u].z * sh[cc + 32 * u];
+      }
     }
     for (; cc < ncols; cc += 32) {
       const V4 v = ld_stream(rowp + cc);
@@ -312,6 +324,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
       y[i] = df + (diag[4 * i + 1] * fi - diag[4 * i + 0] * hi);
       y[n + i] = dh + (diag[4 * i + 3] * fi - diag[4 * i + 2] * hi);
     }
+  }
   }
 }
 
@@ -443,7 +456,14 @@ void nf_assemble(Problem& P) {
     ensure_dynamic_smem((const void*)apply_kernel<double>, apply_smem);
   else
     ensure_dynamic_smem((const void*)apply_kernel<float>, apply_smem);
-  nf.h_items = make_items(P, kApplyRows);
+  // rows per apply item: 64, halved (down to 8) while the grid would hold
+  // fewer than 8 blocks per SM, so small problems still fill the GPU
+  int rows_per_item = kApplyRows;
+  nf.h_items = make_items(P, rows_per_item);
+  while (rows_per_item > 8 && (int)nf.h_items.size() < 8 * ctx->sm_count) {
+    rows_per_item /= 2;
+    nf.h_items = make_items(P, rows_per_item);
+  }
   nf.items = upload(ctx, nf.h_items);
   nf.n_items = (int)nf.h_items.size();
   BP_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -455,16 +475,17 @@ void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t strea
   if (nf.n_items == 0) return;
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
   const size_t smem = 2 * elem * (size_t)nf.max_cols;
+  const int grid = std::min(nf.n_items, kApplyBlocksPerSm * P.ctx->sm_count);
   if (P.fp64) {
-    apply_kernel<double><<<nf.n_items, kApplyThreads, smem, stream>>>(
+    apply_kernel<double><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
         nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev,
-        y_dev);
+        y_dev, nf.n_items);
   } else {
-    apply_kernel<float><<<nf.n_items, kApplyThreads, smem, stream>>>(
+    apply_kernel<float><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
         nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev,
-        y_dev);
+        y_dev, nf.n_items);
   }
   BP_LAUNCH_CHECK();
 }
