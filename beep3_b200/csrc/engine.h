@@ -265,7 +265,10 @@ struct StageTimes {
 // nearfield.cu
 void nf_build_structure(Problem& P);
 void nf_assemble(Problem& P);
-void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t stream);
+// y = near field (incl. singular diagonal) of x, plus yfar if not null;
+// returns the number of kernel launches (0 when the problem has no near-field
+// items, in which case y is not written)
+int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_dev, cudaStream_t stream);
 // fmm.cu
 bool fmm_active(const Problem& P);
 // Throws TimeoutError if a tensor-core FMM kernel of this problem gave up on

@@ -589,8 +589,6 @@ struct XlEntry {
   signed char dir, pad;
 };
 constexpr int kCombos = 686;
-constexpr int kXlTargets = 4;                     // targets per translate block
-constexpr int kXlThreads = kXlTargets * kPairLanes;
 constexpr int kXlChannels = 4;                    // channels per translate block (one screening group)
 constexpr int kXlUnroll = 8;
 
@@ -2326,13 +2324,24 @@ void fmm_setup(Problem& P) {
     S->xl_ldst = upload(c, xl_ldst);
     S->xl_partials.alloc(c, sizeof(float) * (size_t)std::max<long long>(1, xl_part));
   }
-  int prio_lo = 0, prio_hi = 0;  // level streams share the FMM stream's (highest) priority
+  // priorities: the upward chain (M2M), L2L and L2P on the FMM stream are the
+  // critical path and keep the highest priority; the coarsest level with
+  // interactions feeds the downward chain first, so each deeper level's
+  // stream (M2X + X2L, not needed until later) is one step lower
+  int prio_lo = 0, prio_hi = 0;
   BP_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  int top_x = nlev;
+  for (int lev = 0; lev < nlev; ++lev)
+    if (S->m2x_tcount[lev] > 0 || S->xlt_count[lev] > 0) {
+      top_x = lev;
+      break;
+    }
   S->lstreams.assign(nlev, nullptr);
   S->ev_m.assign(nlev, nullptr);
   S->ev_x.assign(nlev, nullptr);
   for (int lev = 0; lev < nlev; ++lev) {
-    BP_CUDA(cudaStreamCreateWithPriority(&S->lstreams[lev], cudaStreamNonBlocking, prio_hi));
+    const int prio = std::min(prio_lo, prio_hi + std::max(0, lev - top_x));
+    BP_CUDA(cudaStreamCreateWithPriority(&S->lstreams[lev], cudaStreamNonBlocking, prio));
     BP_CUDA(cudaEventCreateWithFlags(&S->ev_m[lev], cudaEventDisableTiming));
     BP_CUDA(cudaEventCreateWithFlags(&S->ev_x[lev], cudaEventDisableTiming));
   }

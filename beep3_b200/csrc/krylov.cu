@@ -161,20 +161,15 @@ void ensure_dynamic_smem(const void* kernel, size_t bytes) {
   cur = bytes;
 }
 
-__global__ void add_inplace(double* __restrict__ y, const double* __restrict__ a, int64_t len) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] += a[i];
-}
-
 void matvec_setup(Problem& P) {
   Ctx* c = P.ctx;
   const size_t bytes = sizeof(double) * 2 * (size_t)P.n;
   P.d_yfar.alloc(c, bytes);
   P.d_gx.alloc(c, bytes);
   P.d_gy.alloc(c, bytes);
-  // the FMM is the matvec's critical path and the near field is a
-  // bandwidth-bound stream that can fill the gaps: the FMM streams get the
-  // highest priority, so their blocks are scheduled first
+  // the FMM stream carries the far field's critical chain (P2M, M2M, L2L,
+  // L2P) and has the highest priority; the per-level streams it forks (M2X,
+  // X2L) have lower ones
   int lo = 0, hi = 0;
   BP_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
   BP_CUDA(cudaStreamCreateWithPriority(&P.side, cudaStreamNonBlocking, hi));
@@ -189,23 +184,33 @@ static void matvec_launches(Problem& P, const double* x, double* y, cudaStream_t
                             StageTimes* st) {
   const bool far = fmm_active(P);
   const int64_t len = 2 * (int64_t)P.n;
-  if (far && side != main) {
-    BP_CUDA(cudaEventRecord(P.ev_fork, main));
-    BP_CUDA(cudaStreamWaitEvent(side, P.ev_fork, 0));
+  // The far field first, then the near field, which adds it in its store.
+  // They do not run side by side: the near field is an HBM-bound stream of
+  // about a gigabyte that evicts the FMM's L2-resident expansions, operators
+  // and plane waves and raises the memory latency the FMM's small kernels
+  // wait on, so together they take longer than one after the other.
+  if (far) {
+    if (side != main) {
+      // the FMM runs on its own stream (and one stream per level inside)
+      BP_CUDA(cudaEventRecord(P.ev_fork, main));
+      BP_CUDA(cudaStreamWaitEvent(side, P.ev_fork, 0));
+      fmm_apply(P, x, P.d_yfar.as<double>(), st, side);  // assigns every far-field entry
+      BP_CUDA(cudaEventRecord(P.ev_join, side));
+      BP_CUDA(cudaStreamWaitEvent(main, P.ev_join, 0));
+    } else {
+      fmm_apply(P, x, P.d_yfar.as<double>(), st, main);
+    }
   }
   if (st) st->begin(0, main);
-  nf_apply(P, x, y, main);  // writes every y entry
-  if (st) st->end(P.nf.n_items > 0 ? 1 : 0);
-  if (!far) return;
-  fmm_apply(P, x, P.d_yfar.as<double>(), st, side);  // assigns every far-field entry
-  if (side != main) {
-    BP_CUDA(cudaEventRecord(P.ev_join, side));
-    BP_CUDA(cudaStreamWaitEvent(main, P.ev_join, 0));
+  const int launches = nf_apply(P, x, y, far ? P.d_yfar.as<double>() : nullptr, main);  // writes every y entry
+  if (!launches) {  // no near-field work (not produced by the tree builder): y = far field only
+    if (far)
+      BP_CUDA(cudaMemcpyAsync(y, P.d_yfar.get(), sizeof(double) * len, cudaMemcpyDeviceToDevice, main));
+    else
+      BP_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * len, main));
   }
-  if (st) st->begin(0, main);
-  add_inplace<<<grid_for(len), kThreads, 0, main>>>(y, P.d_yfar.as<double>(), len);
-  BP_LAUNCH_CHECK();
-  if (st) st->end(1);
+  if (st) st->end(launches);
+  (void)len;
 }
 
 // Captures matvec_launches(d_gx -> d_gy) as a CUDA graph on first use.

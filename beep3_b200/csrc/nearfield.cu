@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
     const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
     const T* __restrict__ coef, const double* __restrict__ diag, int n, const double* __restrict__ x,
-    double* __restrict__ y, int n_items) {
+    const double* __restrict__ yfar, double* __restrict__ y, int n_items) {
   extern __shared__ unsigned char smem_raw[];
   T* sf = reinterpret_cast<T*>(smem_raw);
   // persistent: a few blocks per SM stride over the items, leaving room on
@@ -321,8 +321,14 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     if (lane == 0) {
       const int i = rows[r0 + r];
       const double fi = x[i], hi = x[n + i];
-      y[i] = df + (diag[4 * i + 1] * fi - diag[4 * i + 0] * hi);
-      y[n + i] = dh + (diag[4 * i + 3] * fi - diag[4 * i + 2] * hi);
+      double yf = df + (diag[4 * i + 1] * fi - diag[4 * i + 0] * hi);
+      double yh = dh + (diag[4 * i + 3] * fi - diag[4 * i + 2] * hi);
+      if (yfar) {  // the far field of the same matvec, added in the store
+        yf += yfar[i];
+        yh += yfar[n + i];
+      }
+      y[i] = yf;
+      y[n + i] = yh;
     }
   }
   }
@@ -470,9 +476,9 @@ void nf_assemble(Problem& P) {
   P.assemble_ms = ms_since(t0);
 }
 
-void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t stream) {
+int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_dev, cudaStream_t stream) {
   NearField& nf = P.nf;
-  if (nf.n_items == 0) return;
+  if (nf.n_items == 0) return 0;
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
   const size_t smem = 2 * elem * (size_t)nf.max_cols;
   const int grid = std::min(nf.n_items, kApplyBlocksPerSm * P.ctx->sm_count);
@@ -480,14 +486,15 @@ void nf_apply(Problem& P, const double* x_dev, double* y_dev, cudaStream_t strea
     apply_kernel<double><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
         nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev,
-        y_dev, nf.n_items);
+        yfar_dev, y_dev, nf.n_items);
   } else {
     apply_kernel<float><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
         nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev,
-        y_dev, nf.n_items);
+        yfar_dev, y_dev, nf.n_items);
   }
   BP_LAUNCH_CHECK();
+  return 1;
 }
 
 }  // namespace bp

@@ -104,8 +104,9 @@ def test_restart_and_device_stream_profile():
     launches = np.zeros(8, np.int32)
     ns = C.c_int32()
     N.check(N.lib().bp_matvec_profile(p, x.data_ptr(), y.data_ptr(), 3, N.ptr(ms), N.ptr(launches), C.byref(ns)))
-    # near field + final add; P2M one launch; L2P one launch (its per-leaf preparation is stage 5)
-    assert ns.value == 8 and launches[0] == 2 and launches[1] == 1 and launches[5] == 1 and launches[7] == 1
+    # near field (the far field is added in its store); P2M one launch; L2P
+    # preparation (stage 5) and evaluation (stage 7) one launch each
+    assert ns.value == 8 and launches[0] == 1 and launches[1] == 1 and launches[5] == 1 and launches[7] == 1
     assert np.all(ms >= 0) and ms.sum() > 0
     y2 = bp.matvec(x.cpu().numpy())
     assert rel_l2(y.cpu().numpy(), y2) < 1e-12
