@@ -34,6 +34,12 @@ L2_BYTES = 126 * 1024 * 1024
 
 
 # --------------------------------------------------------------------------- workloads
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one near-field
+# apply launch, measured with ncu on each workload (a one-pass capture of the
+# same bench command; 976.9 MB of them are algorithmic on the star workload)
+APPLY_TRAFFIC = {"star": 984_270_000}
+
+
 def workload(name: str):
     """Returns (description dict, list of (Mesh, offset, quaternion), kappa, nbsize)."""
     import beep3_b200 as b
@@ -363,7 +369,7 @@ def _run_ours(args, world, rank, local, dist):
         "e2e": {"value": e2e_value, "unit": "matvec/s", "h2d_bytes_per_step": n2 * 8, "d2h_bytes_per_step": n2 * 8},
         "gpu_launches": int(launches.sum()) * args.steps,
         "roofline": {"bound": "hbm", "kernel": "nearfield apply_kernel<float>", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": APPLY_TRAFFIC.get(args.workload),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                      "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": near_ms},
         "stage_ms": {k: round(float(v), 5) for k, v in zip(
