@@ -340,7 +340,8 @@ BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, 
     DeviceGuard g(P->ctx->device);
     const size_t bytes = sizeof(double) * 2 * (size_t)P->n;
     cudaStream_t st = P->ctx->stream;
-    DevBuf b(P->ctx, bytes);
+    DevBuf& b = P->scratch_b;
+    if (b.bytes() < bytes) b.alloc(P->ctx, bytes);
     BP_CUDA(cudaMemcpyAsync(b.get(), rhs, bytes, cudaMemcpyHostToDevice, st));
     BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
     double rr = 0;
@@ -363,7 +364,9 @@ BP_API int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charge
     if (!(eps_solvent > 0)) return fail(BP_ERR_INVALID, "bp_rhs: eps_solvent must be positive");
     DeviceGuard g(P->ctx->device);
     Ctx* c = P->ctx;
-    DevBuf dch(c, sizeof(double) * 4 * (size_t)std::max(1, n_charges));
+    DevBuf& dch = P->scratch_charges;
+    const size_t cbytes = sizeof(double) * 4 * (size_t)std::max(1, n_charges);
+    if (dch.bytes() < cbytes) dch.alloc(c, cbytes);
     if (n_charges)
       BP_CUDA(cudaMemcpyAsync(dch.get(), charges_xyzq, sizeof(double) * 4 * (size_t)n_charges, cudaMemcpyHostToDevice,
                               c->stream));

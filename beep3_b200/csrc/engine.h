@@ -207,6 +207,9 @@ struct Problem {
   bool graph_failed = false;
   // Krylov workspace
   DevBuf d_V, d_w, d_scal;
+  // grow-only scratch of the source terms (charges, per-point values, the
+  // right-hand side of bp_solve): kept so repeated calls allocate nothing
+  DevBuf scratch_charges, scratch_vals, scratch_b;
   int krylov_m = 0;
   double tree_ms = 0, assemble_ms = 0;
   ~Problem() {

@@ -27,12 +27,32 @@ namespace {
 constexpr int kThreads = 256;
 constexpr double kOneOver4Pi = 0.07957747154594767;
 
+// 1/sqrt(d2) for d2 > 0 in double precision: the single-precision estimate
+// refined by two Newton-Raphson steps y <- y (3 - d2 y^2) / 2 (each step
+// roughly squares the relative error: ~2^-22 -> ~2^-44 -> double rounding),
+// far cheaper than the double-precision reciprocal square root.
+__device__ __forceinline__ double rsqrt_newton(double d2) {
+  double y = (double)rsqrtf((float)d2);
+  y = y * (1.5 - 0.5 * d2 * y * y);
+  y = y * (1.5 - 0.5 * d2 * y * y);
+  return y;
+}
+
 // One thread per point; charges staged through shared memory in tiles.
-// out[2*p] = w * phi * scale, out[2*p+1] = w * (grad phi . n) * scale
+// out[2*p] = w * phi * scale, out[2*p+1] = w * (grad phi . n) * scale.
+// kFast (the mixed engine's right-hand side): points and charges are held as
+// two-float (hi + lo) offsets from the block's first point, converted once,
+// so the coordinate differences come out to FP32 rounding without any
+// per-term conversion; the reciprocal distance and the terms are FP32,
+// summed per tile in FP32 and across tiles in FP64 -- about 1e-7 relative
+// per term, in line with the reference, whose right-hand side comes from a
+// 6-figure FMM.
+template <bool kFast>
 __global__ void point_potential_kernel(const double* __restrict__ pts, int npts, int first_pt, int count_pts,
                                        const double* __restrict__ charges, int nc, double scale,
                                        double* __restrict__ out) {
   __shared__ double4 tile[kThreads];
+  __shared__ float4 ftile_hi[kFast ? kThreads : 1], ftile_lo[kFast ? kThreads : 1];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = k < count_pts;
   const int p = first_pt + k;
@@ -43,18 +63,66 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
     z = pts[2 * (size_t)npts + p];
   }
   double phi = 0, gx = 0, gy = 0, gz = 0;
+  // block origin (kFast): the block's first point; two-float offsets
+  const int p0 = first_pt + blockIdx.x * blockDim.x;
+  const double ox = kFast ? pts[p0] : 0.0, oy = kFast ? pts[(size_t)npts + p0] : 0.0,
+               oz = kFast ? pts[2 * (size_t)npts + p0] : 0.0;
+  auto split = [](double v, float& hi, float& lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+  };
+  float pxh = 0.f, pxl = 0.f, pyh = 0.f, pyl = 0.f, pzh = 0.f, pzl = 0.f;
+  if (kFast) {
+    split(x - ox, pxh, pxl);
+    split(y - oy, pyh, pyl);
+    split(z - oz, pzh, pzl);
+  }
   for (int base = 0; base < nc; base += kThreads) {
     const int c = base + threadIdx.x;
-    if (c < nc) tile[threadIdx.x] = make_double4(charges[4 * c], charges[4 * c + 1], charges[4 * c + 2], charges[4 * c + 3]);
+    if (c < nc) {
+      const double cx = charges[4 * c], cy = charges[4 * c + 1], cz = charges[4 * c + 2], cq = charges[4 * c + 3];
+      if (kFast) {
+        float4 h, l;
+        split(cx - ox, h.x, l.x);
+        split(cy - oy, h.y, l.y);
+        split(cz - oz, h.z, l.z);
+        h.w = (float)cq;
+        l.w = 0.f;
+        ftile_hi[threadIdx.x] = h;
+        ftile_lo[threadIdx.x] = l;
+      } else {
+        tile[threadIdx.x] = make_double4(cx, cy, cz, cq);
+      }
+    }
     __syncthreads();
     const int lim = min(kThreads, nc - base);
-    if (active) {
+    if (active && kFast) {
+      float fphi = 0.f, fgx = 0.f, fgy = 0.f, fgz = 0.f;
+      for (int t = 0; t < lim; ++t) {
+        const float4 h = ftile_hi[t], l = ftile_lo[t];
+        const float dx = (pxh - h.x) + (pxl - l.x), dy = (pyh - h.y) + (pyl - l.y), dz = (pzh - h.z) + (pzl - l.z);
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (d2 > 2.220446049250313e-16f) {
+          const float id = rsqrtf(d2);
+          const float pt = h.w * id;
+          const float ft = -pt * id * id;
+          fphi += pt;
+          fgx = fmaf(ft, dx, fgx);
+          fgy = fmaf(ft, dy, fgy);
+          fgz = fmaf(ft, dz, fgz);
+        }
+      }
+      phi += fphi;
+      gx += fgx;
+      gy += fgy;
+      gz += fgz;
+    } else if (active) {
       for (int t = 0; t < lim; ++t) {
         const double4 ch = tile[t];
         const double dx = x - ch.x, dy = y - ch.y, dz = z - ch.z;
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (d2 > 2.220446049250313e-16) {
-          const double id = rsqrt(d2);
+          const double id = rsqrt_newton(d2);
           const double pt = ch.w * id;
           const double ft = -pt * id * id;
           phi += pt;
@@ -92,12 +160,18 @@ __global__ void sum_points_kernel(const int32_t* __restrict__ off, int first, in
 }  // namespace
 
 void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev) {
+  // FP64 engine: exact FP64 sum; mixed engine: the fast FP32 terms
   Ctx* ctx = P.ctx;
   const int nq = (int)(P.h_qual.size() / 7);
-  DevBuf vals(ctx, sizeof(double) * 2 * (size_t)nq);
+  DevBuf& vals = P.scratch_vals;
+  if (vals.bytes() < sizeof(double) * 2 * (size_t)nq) vals.alloc(ctx, sizeof(double) * 2 * (size_t)nq);
   const double scale = kOneOver4Pi / eps_solvent;
-  point_potential_kernel<<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
-      P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
+  if (P.fp64)
+    point_potential_kernel<false><<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+        P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
+  else
+    point_potential_kernel<true><<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+        P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
   BP_LAUNCH_CHECK();
   sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
       P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
@@ -112,7 +186,7 @@ void energy_coefficients_device(Problem& P, int first, int count, const double* 
   const int p0 = P.h_gal_off[first], p1 = P.h_gal_off[first + count];
   DevBuf vals(ctx, sizeof(double) * 2 * (size_t)std::max(1, p1 - p0));
   if (p1 > p0) {
-    point_potential_kernel<<<(p1 - p0 + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+    point_potential_kernel<false><<<(p1 - p0 + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
         P.d_gal.as<double>(), ng, p0, p1 - p0, charges_dev, n_charges, kOneOver4Pi, vals.as<double>());
     BP_LAUNCH_CHECK();
   }
@@ -187,7 +261,7 @@ extern "C" BP_API int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_
     double* scratch = noalloc_scratch_for_current_device();
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     const double scale = kOneOver4Pi / eps_solvent;
-    point_potential_kernel<<<(n_qual_points + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+    point_potential_kernel<false><<<(n_qual_points + kThreads - 1) / kThreads, kThreads, 0, st>>>(
         qual_points_soa_dev, n_qual_points, 0, n_qual_points, charges_xyzq_dev, n_charges, scale, scratch);
     BP_LAUNCH_CHECK();
     sum_points_kernel<<<(n_patches + kThreads - 1) / kThreads, kThreads, 0, st>>>(

@@ -344,7 +344,7 @@ def _run_ours(args, world, rank, local, dist):
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     achieved = alg_bytes / (near_ms * 1e-3) / 1e9
     # solves (RHS + GMRES) and energies, both precisions
-    solve_ms, solve64_ms = [], []
+    solve_ms, solve64_ms, rhs_ms, gmres_ms = [], [], [], []
     for _ in range(3):
         bp.solve(1e-6, 100)
         bp64.solve(1e-6, 100)
@@ -353,6 +353,8 @@ def _run_ours(args, world, rank, local, dist):
         t = time.perf_counter()
         info = bp.solve(1e-6, 100)
         solve_ms.append((time.perf_counter() - t) * 1e3)
+        rhs_ms.append(info.time_rhs_ms)
+        gmres_ms.append(info.time_gmres_ms)
         t = time.perf_counter()
         info64 = bp64.solve(1e-6, 100)
         solve64_ms.append((time.perf_counter() - t) * 1e3)
@@ -379,6 +381,7 @@ def _run_ours(args, world, rank, local, dist):
         "solves_per_s": world * 1e3 / statistics.median(solve_ms),
         "fp64_solves_per_s": world * 1e3 / statistics.median(solve64_ms),
         "solve_latency_ms": {"p50": float(np.percentile(solve_ms, 50)), "p99": float(np.percentile(solve_ms, 99))},
+        "solve_parts_ms": {"rhs": float(np.median(rhs_ms)), "gmres": float(np.median(gmres_ms))},
         "gmres_iterations": {"mixed": info.num_iterations, "fp64": info64.num_iterations},
         "energy_kj_per_mol": {"mixed": e_mixed, "fp64": e_fp64,
                               "rel_err_mixed_vs_fp64": abs(e_mixed - e_fp64) / abs(e_fp64)},

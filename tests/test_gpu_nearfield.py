@@ -52,10 +52,13 @@ def test_info_and_tree(setup):
 
 
 def test_rhs_parity(setup):
+    """FP64 engine: the exact FP64 direct sum.  Mixed engine: FP32 terms
+    summed in FP64, held to 1e-6 -- the reference's own right-hand side comes
+    from a 6-figure FMM."""
     prec, bp, pr = setup
     rhs = bp.set_rhs()
     ro = O.rhs(pr.patches, bp.instances[0].charges, 80.0)
-    assert rel_l2(rhs, ro) < 1e-12
+    assert rel_l2(rhs, ro) < (1e-12 if prec == "fp64" else 1e-6)
 
 
 def test_solve_and_energy(setup, kirkwood_case):
