@@ -965,7 +965,7 @@ __global__ void __launch_bounds__(64) l2p_prep_kernel(const __grid_constant__ Ta
   }
 }
 
-constexpr int kEvalChunk = 64;  // targets per l2p_eval block
+constexpr int kEvalChunk = 32;  // targets per l2p_eval block
 
 // q(n, m) = i_n(beta r) P_n^m(cos theta) e^{i m phi} of every target patch
 // relative to its leaf centre, n <= nt + 2, per screening group: geometry
