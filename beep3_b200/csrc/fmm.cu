@@ -219,6 +219,19 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// one 4- or 8-byte element
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem);
+template <>
+__device__ __forceinline__ void cp_async_elem<float>(float* smem, const float* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <>
+__device__ __forceinline__ void cp_async_elem<double>(double* smem, const double* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -1161,8 +1174,8 @@ struct ShiftCol {
 struct ShiftReduce {
   int parent, first_slot, n_slots;
 };
-constexpr int kTileCols = 16;
-constexpr int kGemmThreads = 128;
+constexpr int kTileCols = 64;   // columns per shift tile: the operator load is shared by all of them
+constexpr int kGemmThreads = (112 / 4) * (kTileCols / 4);  // 4 x 4 outputs per thread, R <= 112
 
 template <typename T>
 __device__ __forceinline__ void load4(const T* p, T (&v)[4]);
@@ -1198,15 +1211,18 @@ __global__ void __launch_bounds__(kGemmThreads) shift_gemm_kernel(int E, const S
     for (int j = threadIdx.x; j < n16; j += blockDim.x) cp_async16(dst + 16 * j, src + 16 * j);
     cp_async_commit();
   }
+  // columns: asynchronous element copies, column-fastest so that the
+  // shared-memory writes of a warp fall in distinct banks
   for (int o = threadIdx.x; o < kTileCols * R; o += blockDim.x) {
-    const int j = o / R, k = o - j * R;
-    T v = 0;
+    const int j = o % kTileCols, k = o / kTileCols;
     if (j < tl.n_cols) {
       const ShiftCol c = cols[tl.first_col + j];
-      v = X[((size_t)c.src * kCh + c.ch) * R + k];
+      cp_async_elem(xs + k * kTileCols + j, X + ((size_t)c.src * kCh + c.ch) * R + k);
+    } else {
+      xs[k * kTileCols + j] = 0;
     }
-    xs[k * kTileCols + j] = v;
   }
+  cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
   const int ngr = RP / 4;
@@ -1273,18 +1289,6 @@ struct OpChunk<double> {
   static constexpr int value = 28;
 };
 
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem);
-template <>
-__device__ __forceinline__ void cp_async_elem<float>(float* smem, const float* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-template <>
-__device__ __forceinline__ void cp_async_elem<double>(double* smem, const double* gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
 
 template <typename T>
 __global__ void __launch_bounds__(kOpThreads) op_gemm_kernel(const GemmTile* __restrict__ tiles,
@@ -2354,7 +2358,7 @@ void fmm_setup(Problem& P) {
   S->eval_items = upload(c, evals);
   S->n_eval = (int)evals.size();
   const int E = S->E, NT = S->nt;
-  if (E > kPairLanes) throw std::invalid_argument("FMM order above 9 is not supported");
+  if (E > kPairLanes || ((2 * E + 3) & ~3) > 112) throw std::invalid_argument("FMM order above 9 is not supported");
   S->smem_shift = 4 * celem * E;
   S->smem_p2m = celem * (size_t)kP2mChunk * 2 * E;
   S->smem_gemm = (S->fp64 ? 8 : 4) * (size_t)(2 * E) * (((2 * E + 3) & ~3) + kTileCols);
