@@ -605,47 +605,51 @@ constexpr int kCombos = 686;
 constexpr int kXlChannels = 4;                    // channels per translate block (one screening group)
 constexpr int kXlUnroll = 8;
 
-constexpr int kXlDirThreads = 6 * kPairLanes;    // one lane group per direction
+constexpr int kXlGroups = 7;                     // lane groups of a translate block
+constexpr int kXlDirThreads = kXlGroups * kPairLanes;
 
-// One block per (target, 4 channels); thread (direction d, lane i = plane
-// wave) sums W[src][d][ch][i] * factor[combo][i] over the target's entries
-// of direction d, in registers, and stores ACC[acc_row][ch][d][i] (re, im);
-// a direction without entries stores 0.  The six directions of a target run
-// side by side.
+// One block per (target, 4 channels); thread (lane group g, lane i = plane
+// wave) sums W[src][d][ch][i] * factor[combo][i] over a range of the
+// target's entries of direction d, in registers.  The up and down lists
+// are about twice as long as north / south and four times east / west, so
+// the seven lane groups share the work evenly: up and down each split in
+// halves (groups 0 + 1, 2 + 3; the second half's sum is added through shared
+// memory), north (4), south (5), and east then west (6).  ACC[acc_row][ch]
+// [d][i] (re, im) is stored for all six directions, 0 for one without
+// entries.
 template <typename T>
-__global__ void __launch_bounds__(kXlDirThreads) xl_translate_kernel(const __grid_constant__ Tables<T> tb,
-                                                                     int parent_level,
-                                                                     const XlTarget* __restrict__ targets,
-                                                                     int n_targets,
-                                                                     const XlEntry* __restrict__ entries,
-                                                                     const typename C2T<T>::type* __restrict__ W,
-                                                                     typename C2T<T>::type* __restrict__ ACC) {
+__global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __grid_constant__ Tables<T> tb,
+                                                                        int parent_level,
+                                                                        const XlTarget* __restrict__ targets,
+                                                                        int n_targets,
+                                                                        const XlEntry* __restrict__ entries,
+                                                                        const typename C2T<T>::type* __restrict__ W,
+                                                                        typename C2T<T>::type* __restrict__ ACC) {
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
   constexpr int U = sizeof(T) == 4 ? kXlUnroll / 2 : kXlUnroll / 4;  // entries in flight per thread
+  __shared__ C part[2][CB][kPairLanes];  // second halves of up and down
   const int NPM = tb.np_max;
   const int t = blockIdx.x / (kCh / CB);
   const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
-  const int d = threadIdx.x / kPairLanes, i = threadIdx.x - d * kPairLanes;
+  const int g = threadIdx.x / kPairLanes, i = threadIdx.x - g * kPairLanes;
   const int lg = 2 * parent_level + (ch0 >= 8 ? 1 : 0);
-  if (t >= n_targets || i >= NPM) return;
-  const XlTarget tg = targets[t];
+  const XlTarget tg = targets[t];  // t < n_targets: the grid has one block set per target
   const int np = tb.nexptotp[lg];
-  // ACC[acc_row][ch][dir][i]: 6 * NPM complex per (target, channel)
-  C* out = ACC + (((size_t)tg.acc_row * kCh + ch0) * 6 + d) * NPM + i;
-  C a[CB];
+  const bool live = i < NPM && i < np;  // plane waves beyond this level's count stay 0
+  const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
+  // sum over entries [b, e) of direction d
+  auto accum = [&](int d, int b, int e, C (&a)[CB]) {
 #pragma unroll
-  for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
-  if (i < np) {  // plane waves beyond this level's count are never read: they stay 0
-    const XlEntry* ent = entries + tg.first_entry + tg.dir_start[d];
-    const int ne = tg.dir_start[d + 1] - tg.dir_start[d];
-    const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
+    for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
+    if (!live) return;
+    const XlEntry* ent = entries + tg.first_entry;
     const C* Wd = W + ((size_t)d * kCh + ch0) * NPM + i;
-    for (int k0 = 0; k0 < ne; k0 += U) {
+    for (int k0 = b; k0 < e; k0 += U) {
       int src[U], combo[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const XlEntry en = ent[min(k0 + u, ne - 1)];
+        const XlEntry en = ent[min(k0 + u, e - 1)];
         src[u] = en.src;
         combo[u] = en.combo;
       }
@@ -658,13 +662,45 @@ __global__ void __launch_bounds__(kXlDirThreads) xl_translate_kernel(const __gri
       }
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        if (k0 + u < ne)
+        if (k0 + u < e)
 #pragma unroll
           for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
     }
-  }
+  };
+  auto store = [&](int d, const C (&a)[CB]) {
+    if (i >= NPM) return;
+    C* out = ACC + (((size_t)tg.acc_row * kCh + ch0) * 6 + d) * NPM + i;
 #pragma unroll
-  for (int c = 0; c < CB; ++c) out[(size_t)c * 6 * NPM] = a[c];
+    for (int c = 0; c < CB; ++c) out[(size_t)c * 6 * NPM] = a[c];
+  };
+  C a[CB];
+  if (g < 4) {  // halves of up (0, 1) and down (2, 3)
+    const int d = g >> 1, b = tg.dir_start[d], e = tg.dir_start[d + 1], mid = b + (e - b + 1) / 2;
+    if (g & 1) {
+      accum(d, mid, e, a);
+#pragma unroll
+      for (int c = 0; c < CB; ++c) part[d][c][i] = a[c];
+    } else {
+      accum(d, b, mid, a);
+    }
+  } else if (g < 6) {
+    const int d = g - 2;
+    accum(d, tg.dir_start[d], tg.dir_start[d + 1], a);
+    store(d, a);
+  } else {
+    accum(4, tg.dir_start[4], tg.dir_start[5], a);
+    store(4, a);
+    accum(5, tg.dir_start[5], tg.dir_start[6], a);
+    store(5, a);
+  }
+  __syncthreads();
+  if (g < 4 && !(g & 1)) {
+    const int d = g >> 1;
+#pragma unroll
+    for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], part[d][c][i]);
+    store(d, a);
+  }
+  (void)n_targets;
 }
 
 // Conversion of one accumulated-wave vector to a local expansion, applied
