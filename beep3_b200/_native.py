@@ -65,6 +65,13 @@ class bp_params(C.Structure):
     ]
 
 
+class bp_instance(C.Structure):
+    _fields_ = [
+        ("mesh", C.c_void_p), ("rotation", C.c_double * 9), ("offset", C.c_double * 3),
+        ("dielectric_ratio", C.c_double),
+    ]
+
+
 class bp_problem_info(C.Structure):
     _fields_ = [
         ("n_patches", C.c_int64), ("n_levels", C.c_int64), ("n_nodes", C.c_int64), ("n_leaves", C.c_int64),
@@ -92,6 +99,9 @@ _SIGS = {
     "bp_geom_copy": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "bp_geom_destroy": [_P],
     "bp_problem_create": [_P, C.POINTER(bp_patches), C.POINTER(bp_params), _PP],
+    "bp_mesh_create": [_P, C.POINTER(bp_patches), _P, _PP],
+    "bp_mesh_destroy": [_P],
+    "bp_problem_create_posed": [_P, C.POINTER(bp_instance), _I, C.POINTER(bp_params), _PP],
     "bp_problem_destroy": [_P],
     "bp_problem_info_get": [_P, C.POINTER(bp_problem_info)],
     "bp_problem_tree": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_int64), _P, _P, _P],

@@ -76,21 +76,32 @@ class MeshInstance:
     rotation: np.ndarray  # quaternion (a, b, c, d)
     eps_protein: float
     eps_solvent: float
-    patches: PatchSet = field(init=False)
     charges: np.ndarray = field(init=False)
 
     def __post_init__(self):
         self.place(self.offset, self.rotation)
 
     def place(self, offset, rotation) -> None:
-        """NodePatch / Charge change_coordinate_frame (src/bem/node_patch.cpp:369-456)."""
+        """NodePatch / Charge change_coordinate_frame (src/bem/node_patch.cpp:369-456).
+        The charges move at once; the patches (host copy) on first use, as
+        the engine places its own copy on the device."""
         self.offset = np.asarray(offset, float)
         self.rotation = np.asarray(rotation, float)
-        R = quaternion_matrix(self.rotation)
-        self.patches = self.mesh.patches.transformed(R, self.mesh.centre, self.offset)
+        self.matrix = quaternion_matrix(self.rotation)
+        self._patches = None
         ch = self.mesh.charges.copy()
-        ch[:, :3] = (ch[:, :3] - self.mesh.centre) @ R.T + self.offset
+        ch[:, :3] = (ch[:, :3] - self.mesh.centre) @ self.matrix.T + self.offset
         self.charges = np.ascontiguousarray(ch)
+
+    @property
+    def patches(self) -> PatchSet:
+        if self._patches is None:
+            self._patches = self.mesh.patches.transformed(self.matrix, self.mesh.centre, self.offset)
+        return self._patches
+
+    @property
+    def n_patches(self) -> int:
+        return self.mesh.patches.n
 
     @property
     def dielectric_ratio(self) -> float:
@@ -132,6 +143,7 @@ class BEEP:
         self.device = int(device)
         self.hbm_budget_bytes = int(hbm_budget_bytes)
         self._ctx = C.c_void_p()
+        self._meshes: dict[int, tuple[Mesh, C.c_void_p]] = {}  # id(mesh) -> device-resident copy
         self._problem = None
         self.bounding_cube = None
         self._manual_cube = False
@@ -179,6 +191,9 @@ class BEEP:
 
     def close(self) -> None:
         self._invalidate()
+        for _, h in self._meshes.values():
+            N.lib().bp_mesh_destroy(h)
+        self._meshes = {}
         if self._ctx:
             N.lib().bp_ctx_destroy(self._ctx)
             self._ctx = C.c_void_p()
@@ -218,7 +233,23 @@ class BEEP:
 
     @property
     def num_patches(self) -> int:
-        return sum(i.patches.n for i in self.instances)
+        return sum(i.n_patches for i in self.instances)
+
+    def _mesh_handle(self, mesh: Mesh) -> C.c_void_p:
+        """The mesh's patches (its own frame) on this context's device,
+        uploaded on first use (bp_mesh_create)."""
+        entry = self._meshes.get(id(mesh))
+        if entry is None:
+            p = mesh.patches
+            pp = N.bp_patches(p.n, N.ptr(p.centroid), N.ptr(p.normal), N.ptr(p.area), None, None,
+                              N.ptr(p.qual_off), N.ptr(p.qual), N.ptr(p.quad_off), N.ptr(p.quad),
+                              N.ptr(p.gal_off), N.ptr(p.gal))
+            h = C.c_void_p()
+            N.check(N.lib().bp_mesh_create(self.context(), C.byref(pp), N.ptr(np.ascontiguousarray(mesh.centre)),
+                                           C.byref(h)))
+            entry = (mesh, h)
+            self._meshes[id(mesh)] = entry
+        return entry[1]
 
     def context(self) -> C.c_void_p:
         """The device context (created on first use)."""
@@ -237,20 +268,26 @@ class BEEP:
         return build_tree(cen, centre, edge, self.nbsize)
 
     def build(self):
-        """Tree + singular integrals + cached near field on the device."""
+        """Tree + singular integrals + cached near field on the device.  The
+        instances' meshes stay on the device between builds; each instance
+        is placed there by its rigid move (bp_problem_create_posed)."""
         if self._problem is not None:
             return self._problem
+        if not self.instances:
+            raise ValueError("no mesh instances")
         self.context()
-        g = self._gather()
-        self._arrays = g
+        self._arrays = {"first": np.cumsum([0] + [i.n_patches for i in self.instances])}
         centre, edge = self.calculate_bounding_cube()
-        pp = N.bp_patches(len(g["area"]), N.ptr(g["centroid"]), N.ptr(g["normal"]), N.ptr(g["area"]),
-                          N.ptr(g["eps"]), N.ptr(g["gc"]), N.ptr(g["qual_off"]), N.ptr(g["qual"]),
-                          N.ptr(g["quad_off"]), N.ptr(g["quad"]), N.ptr(g["gal_off"]), N.ptr(g["gal"]))
+        insts = (N.bp_instance * len(self.instances))()
+        for k, inst in enumerate(self.instances):
+            insts[k].mesh = self._mesh_handle(inst.mesh)
+            insts[k].rotation[:] = [float(v) for v in inst.matrix.ravel()]
+            insts[k].offset[:] = [float(v) for v in inst.offset]
+            insts[k].dielectric_ratio = inst.dielectric_ratio
         prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge, self.nbsize, self.nterms,
                           N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED, 0)
         h = C.c_void_p()
-        N.check(N.lib().bp_problem_create(self._ctx, C.byref(pp), C.byref(prm), C.byref(h)))
+        N.check(N.lib().bp_problem_create_posed(self._ctx, insts, len(self.instances), C.byref(prm), C.byref(h)))
         self._problem = h
         return h
 
@@ -318,7 +355,7 @@ class BEEP:
             # rigid-motion invariant: computed once per library mesh
             p = self.build()
             first = int(self._arrays["first"][idx])
-            n = inst.patches.n
+            n = inst.n_patches
             cf, chh = np.empty(n), np.empty(n)
             ch = np.ascontiguousarray(inst.charges[inst.charges[:, 3] != 0])
             N.check(N.lib().bp_energy_coefficients(p, first, n, N.ptr(ch), len(ch), mesh.patches.total_area,
@@ -337,7 +374,7 @@ class BEEP:
             cf, chh = self._energy_coefficients(idx)
             e = C.c_double()
             first = int(self._arrays["first"][idx])
-            N.check(N.lib().bp_energy(p, first, inst.patches.n, N.ptr(cf), N.ptr(chh), inst.dielectric_ratio,
+            N.check(N.lib().bp_energy(p, first, inst.n_patches, N.ptr(cf), N.ptr(chh), inst.dielectric_ratio,
                                       N.ptr(self.x), C.byref(e)))
             out.append(e.value)
         return float(sum(out)), out

@@ -55,6 +55,61 @@ void check_points(const char* what, int n, const int32_t* off, const double* pts
     if (!std::isfinite(v)) throw std::invalid_argument(std::string(what) + ": non-finite point data");
 }
 
+int32_t check_params(const char* who, const bp_params* prm) {
+  if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
+    return fail(BP_ERR_INVALID, std::string(who) + ": unknown precision");
+  if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, std::string(who) + ": bad kappa");
+  if (prm->nterms != 9 && prm->nterms != 18)
+    return fail(BP_ERR_UNSUPPORTED, std::string(who) + ": FMM order must be 9 or 18 (tabulated quadratures)");
+  return BP_OK;
+}
+
+// The steps after the patch geometry is in place (host arrays and device
+// point lists): tree, per-patch device arrays, near field, FMM, matvec graph.
+void finish_problem(Ctx* c, Problem& P) {
+  auto t0 = std::chrono::steady_clock::now();
+  build_reference_tree(P.h_centroid.data(), P.n, P.params.cube_centre, P.params.cube_edge, P.params.nbsize, P.tree);
+  P.tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  P.d_centroid = upload(c, P.h_centroid);
+  P.d_normal = upload(c, P.h_normal);
+  P.d_area = upload(c, P.h_area);
+  P.d_eps = upload(c, P.h_eps);
+  P.d_qual_off = upload(c, P.h_qual_off);
+  P.d_quad_off = upload(c, P.h_quad_off);
+  P.d_gal_off = upload(c, P.h_gal_off);
+  P.d_x.alloc(c, sizeof(double) * 2 * (size_t)P.n);
+  P.d_y.alloc(c, sizeof(double) * 2 * (size_t)P.n);
+  nf_build_structure(P);
+  nf_assemble(P);
+  if (fmm_active(P)) fmm_setup(P);
+  matvec_setup(P);
+  BP_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// p -> R (p - c) + o and n -> R n of `count` points of a 7-array SoA list
+// (x y z nx ny nz w, row stride src_n) into rows [base, base + count) of a
+// list of row stride dst_n; FP32 copy too when dst_f is set.
+struct Rigid {
+  double R[9], c[3], o[3];
+};
+__global__ void place_points_kernel(const double* __restrict__ src, int src_n, double* __restrict__ dst, int dst_n,
+                                    int base, int count, Rigid rg, float* __restrict__ dst_f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const double x = src[i] - rg.c[0], y = src[src_n + i] - rg.c[1], z = src[2 * (size_t)src_n + i] - rg.c[2];
+  const double nx = src[3 * (size_t)src_n + i], ny = src[4 * (size_t)src_n + i], nz = src[5 * (size_t)src_n + i];
+  double v[7];
+  for (int r = 0; r < 3; ++r) {
+    v[r] = rg.R[3 * r] * x + rg.R[3 * r + 1] * y + rg.R[3 * r + 2] * z + rg.o[r];
+    v[3 + r] = rg.R[3 * r] * nx + rg.R[3 * r + 1] * ny + rg.R[3 * r + 2] * nz;
+  }
+  v[6] = src[6 * (size_t)src_n + i];
+  for (int f = 0; f < 7; ++f) {
+    dst[(size_t)f * dst_n + base + i] = v[f];
+    if (dst_f) dst_f[(size_t)f * dst_n + base + i] = (float)v[f];
+  }
+}
+
 }  // namespace
 }  // namespace bp
 
@@ -88,6 +143,8 @@ BP_API int32_t bp_ctx_destroy(bp_ctx ctx) {
     Ctx* c = as_ctx(ctx);
     if (!c) return BP_OK;
     DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->stream);
+    c->trim();  // the released blocks kept for reuse
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return BP_OK;
@@ -127,11 +184,7 @@ BP_API int32_t bp_problem_create(bp_ctx ctx, const bp_patches* pp, const bp_para
     if (n <= 0) return fail(BP_ERR_INVALID, "bp_problem_create: no patches");
     if (!pp->centroid || !pp->normal || !pp->area || !pp->dielectric_ratio)
       return fail(BP_ERR_INVALID, "bp_problem_create: missing patch arrays");
-    if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
-      return fail(BP_ERR_INVALID, "bp_problem_create: unknown precision");
-    if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, "bp_problem_create: bad kappa");
-    if (prm->nterms != 9 && prm->nterms != 18)
-      return fail(BP_ERR_UNSUPPORTED, "bp_problem_create: FMM order must be 9 or 18 (tabulated quadratures)");
+    if (const int32_t e = check_params("bp_problem_create", prm)) return e;
     DeviceGuard g(c->device);
     auto P = std::make_unique<Problem>();
     P->ctx = c;
@@ -150,35 +203,164 @@ BP_API int32_t bp_problem_create(bp_ctx ctx, const bp_patches* pp, const bp_para
         if (!std::isfinite(P->h_centroid[3 * i + k]) || !std::isfinite(P->h_normal[3 * i + k]))
           return fail(BP_ERR_INVALID, "bp_problem_create: non-finite patch geometry");
     }
-    check_points("qualocation", n, pp->qual_offsets, pp->qual_points, P->h_qual_off, P->h_qual);
-    check_points("quadrature", n, pp->quad_offsets, pp->quad_points, P->h_quad_off, P->h_quad);
-    check_points("galerkin", n, pp->galerkin_offsets, pp->galerkin_points, P->h_gal_off, P->h_gal);
-    // adaptive tree (host)
-    auto t0 = std::chrono::steady_clock::now();
-    build_reference_tree(P->h_centroid.data(), n, prm->cube_centre, prm->cube_edge, prm->nbsize, P->tree);
-    P->tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    // device copies
-    P->d_centroid = upload(c, P->h_centroid);
-    P->d_normal = upload(c, P->h_normal);
-    P->d_area = upload(c, P->h_area);
-    P->d_eps = upload(c, P->h_eps);
-    P->d_qual_off = upload(c, P->h_qual_off);
-    P->d_quad_off = upload(c, P->h_quad_off);
-    P->d_gal_off = upload(c, P->h_gal_off);
-    P->d_qual = upload(c, soa7<double>(P->h_qual));
-    P->d_quad = upload(c, soa7<double>(P->h_quad));
-    P->d_gal = upload(c, soa7<double>(P->h_gal));
-    if (!P->fp64) {
-      P->d_qual_f = upload(c, soa7<float>(P->h_qual));
-      P->d_quad_f = upload(c, soa7<float>(P->h_quad));
+    {
+      std::vector<double> qual, quad, gal;
+      check_points("qualocation", n, pp->qual_offsets, pp->qual_points, P->h_qual_off, qual);
+      check_points("quadrature", n, pp->quad_offsets, pp->quad_points, P->h_quad_off, quad);
+      check_points("galerkin", n, pp->galerkin_offsets, pp->galerkin_points, P->h_gal_off, gal);
+      P->n_qual_pts = P->h_qual_off[n];
+      P->n_quad_pts = P->h_quad_off[n];
+      P->n_gal_pts = P->h_gal_off[n];
+      P->d_qual = upload(c, soa7<double>(qual));
+      P->d_quad = upload(c, soa7<double>(quad));
+      P->d_gal = upload(c, soa7<double>(gal));
+      if (!P->fp64) {
+        P->d_qual_f = upload(c, soa7<float>(qual));
+        P->d_quad_f = upload(c, soa7<float>(quad));
+      }
+      BP_CUDA(cudaStreamSynchronize(c->stream));  // the host staging vectors go out of scope
     }
-    P->d_x.alloc(c, sizeof(double) * 2 * (size_t)n);
-    P->d_y.alloc(c, sizeof(double) * 2 * (size_t)n);
-    nf_build_structure(*P);
-    nf_assemble(*P);
-    if (fmm_active(*P)) fmm_setup(*P);
-    matvec_setup(*P);
+    finish_problem(c, *P);
+    *out = reinterpret_cast<bp_problem>(P.release());
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_mesh_create(bp_ctx ctx, const bp_patches* pp, const double centre[3], bp_mesh* out) {
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c || !pp || !centre || !out) return fail(BP_ERR_INVALID, "bp_mesh_create: null argument");
+    const int n = pp->n_patches;
+    if (n <= 0) return fail(BP_ERR_INVALID, "bp_mesh_create: no patches");
+    if (!pp->centroid || !pp->normal || !pp->area) return fail(BP_ERR_INVALID, "bp_mesh_create: missing patch arrays");
+    DeviceGuard g(c->device);
+    auto m = std::make_unique<DevMesh>();
+    m->ctx = c;
+    m->n = n;
+    for (int k = 0; k < 3; ++k) {
+      if (!std::isfinite(centre[k])) return fail(BP_ERR_INVALID, "bp_mesh_create: non-finite centre");
+      m->centre[k] = centre[k];
+    }
+    m->h_centroid.assign(pp->centroid, pp->centroid + 3 * (size_t)n);
+    m->h_normal.assign(pp->normal, pp->normal + 3 * (size_t)n);
+    m->h_area.assign(pp->area, pp->area + n);
+    m->h_gc.assign(n, 0.5);
+    if (pp->gc) m->h_gc.assign(pp->gc, pp->gc + n);
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(m->h_centroid[3 * i + k]) || !std::isfinite(m->h_normal[3 * i + k]))
+          return fail(BP_ERR_INVALID, "bp_mesh_create: non-finite patch geometry");
+    std::vector<double> qual, quad, gal;
+    check_points("qualocation", n, pp->qual_offsets, pp->qual_points, m->h_qual_off, qual);
+    check_points("quadrature", n, pp->quad_offsets, pp->quad_points, m->h_quad_off, quad);
+    check_points("galerkin", n, pp->galerkin_offsets, pp->galerkin_points, m->h_gal_off, gal);
+    m->n_qual_pts = m->h_qual_off[n];
+    m->n_quad_pts = m->h_quad_off[n];
+    m->n_gal_pts = m->h_gal_off[n];
+    m->d_qual = upload(c, soa7<double>(qual));
+    m->d_quad = upload(c, soa7<double>(quad));
+    m->d_gal = upload(c, soa7<double>(gal));
     BP_CUDA(cudaStreamSynchronize(c->stream));
+    *out = reinterpret_cast<bp_mesh>(m.release());
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_mesh_destroy(bp_mesh mesh) {
+  return guarded_engine([&]() -> int32_t {
+    DevMesh* m = reinterpret_cast<DevMesh*>(mesh);
+    if (!m) return BP_OK;
+    DeviceGuard g(m->ctx->device);
+    cudaStreamSynchronize(m->ctx->stream);
+    delete m;
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int32_t n_inst, const bp_params* prm,
+                                       bp_problem* out) {
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c || !inst || !prm || !out || n_inst <= 0) return fail(BP_ERR_INVALID, "bp_problem_create_posed: bad argument");
+    if (const int32_t e = check_params("bp_problem_create_posed", prm)) return e;
+    long long n_total = 0, nq = 0, nd = 0, ng = 0;
+    for (int q = 0; q < n_inst; ++q) {
+      const DevMesh* m = reinterpret_cast<const DevMesh*>(inst[q].mesh);
+      if (!m || m->ctx != c) return fail(BP_ERR_INVALID, "bp_problem_create_posed: mesh of another context");
+      if (!(inst[q].dielectric_ratio > 0) || !std::isfinite(inst[q].dielectric_ratio))
+        return fail(BP_ERR_INVALID, "bp_problem_create_posed: dielectric ratio must be > 0");
+      for (int k = 0; k < 9; ++k)
+        if (!std::isfinite(inst[q].rotation[k])) return fail(BP_ERR_INVALID, "bp_problem_create_posed: bad rotation");
+      for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(inst[q].offset[k])) return fail(BP_ERR_INVALID, "bp_problem_create_posed: bad offset");
+      n_total += m->n;
+      nq += m->n_qual_pts;
+      nd += m->n_quad_pts;
+      ng += m->n_gal_pts;
+    }
+    if (n_total > (1LL << 30) || nq > (1LL << 31) - 1 || nd > (1LL << 31) - 1 || ng > (1LL << 31) - 1)
+      return fail(BP_ERR_INVALID, "bp_problem_create_posed: too many patches or points");
+    DeviceGuard g(c->device);
+    auto P = std::make_unique<Problem>();
+    P->ctx = c;
+    P->n = (int)n_total;
+    P->params = *prm;
+    P->fp64 = prm->precision == BP_PREC_FP64;
+    P->n_qual_pts = (int)nq;
+    P->n_quad_pts = (int)nd;
+    P->n_gal_pts = (int)ng;
+    P->d_qual.alloc(c, sizeof(double) * 7 * (size_t)nq);
+    P->d_quad.alloc(c, sizeof(double) * 7 * (size_t)nd);
+    P->d_gal.alloc(c, sizeof(double) * 7 * (size_t)ng);
+    if (!P->fp64) {
+      P->d_qual_f.alloc(c, sizeof(float) * 7 * (size_t)nq);
+      P->d_quad_f.alloc(c, sizeof(float) * 7 * (size_t)nd);
+    }
+    P->h_qual_off.assign(1, 0);
+    P->h_quad_off.assign(1, 0);
+    P->h_gal_off.assign(1, 0);
+    int bq = 0, bd = 0, bg = 0;
+    for (int q = 0; q < n_inst; ++q) {
+      const DevMesh& m = *reinterpret_cast<const DevMesh*>(inst[q].mesh);
+      Rigid rg;
+      for (int k = 0; k < 9; ++k) rg.R[k] = inst[q].rotation[k];
+      for (int k = 0; k < 3; ++k) {
+        rg.c[k] = m.centre[k];
+        rg.o[k] = inst[q].offset[k];
+      }
+      // patch centres and normals on the host (the tree is built there)
+      for (int i = 0; i < m.n; ++i) {
+        const double* p = &m.h_centroid[3 * (size_t)i];
+        const double* nv = &m.h_normal[3 * (size_t)i];
+        const double x = p[0] - rg.c[0], y = p[1] - rg.c[1], z = p[2] - rg.c[2];
+        for (int r = 0; r < 3; ++r) {
+          P->h_centroid.push_back(rg.R[3 * r] * x + rg.R[3 * r + 1] * y + rg.R[3 * r + 2] * z + rg.o[r]);
+          P->h_normal.push_back(rg.R[3 * r] * nv[0] + rg.R[3 * r + 1] * nv[1] + rg.R[3 * r + 2] * nv[2]);
+        }
+      }
+      P->h_area.insert(P->h_area.end(), m.h_area.begin(), m.h_area.end());
+      P->h_gc.insert(P->h_gc.end(), m.h_gc.begin(), m.h_gc.end());
+      P->h_eps.insert(P->h_eps.end(), (size_t)m.n, inst[q].dielectric_ratio);
+      for (int i = 1; i <= m.n; ++i) {
+        P->h_qual_off.push_back(bq + m.h_qual_off[i]);
+        P->h_quad_off.push_back(bd + m.h_quad_off[i]);
+        P->h_gal_off.push_back(bg + m.h_gal_off[i]);
+      }
+      // point lists: placed on the device
+      auto place = [&](const DevBuf& src, int src_n, DevBuf& dst, int dst_n, int base, float* dst_f) {
+        if (src_n == 0) return;
+        place_points_kernel<<<(src_n + 255) / 256, 256, 0, c->stream>>>(src.as<double>(), src_n, dst.as<double>(),
+                                                                       dst_n, base, src_n, rg, dst_f);
+        BP_LAUNCH_CHECK();
+      };
+      place(m.d_qual, m.n_qual_pts, P->d_qual, (int)nq, bq, P->fp64 ? nullptr : P->d_qual_f.as<float>());
+      place(m.d_quad, m.n_quad_pts, P->d_quad, (int)nd, bd, P->fp64 ? nullptr : P->d_quad_f.as<float>());
+      place(m.d_gal, m.n_gal_pts, P->d_gal, (int)ng, bg, nullptr);
+      bq += m.n_qual_pts;
+      bd += m.n_quad_pts;
+      bg += m.n_gal_pts;
+    }
+    finish_problem(c, *P);
     *out = reinterpret_cast<bp_problem>(P.release());
     return BP_OK;
   });
@@ -394,7 +576,9 @@ BP_API int32_t bp_energy_coefficients(bp_problem p, int32_t first, int32_t count
     energy_coefficients_device(*P, first, count, dch.as<double>(), n_charges, out.as<double>(),
                                out.as<double>() + count);
     std::vector<double> h(2 * (size_t)count);
-    BP_CUDA(cudaMemcpy(h.data(), out.get(), sizeof(double) * 2 * (size_t)count, cudaMemcpyDeviceToHost));
+    BP_CUDA(cudaMemcpyAsync(h.data(), out.get(), sizeof(double) * 2 * (size_t)count, cudaMemcpyDeviceToHost,
+                            c->stream));
+    BP_CUDA(cudaStreamSynchronize(c->stream));
     // Gauss-law renormalisation of the f coefficients (host, compensated sums)
     double net = 0.0;
     for (int k = 0; k < n_charges; ++k) net += charges_xyzq[4 * k + 3];

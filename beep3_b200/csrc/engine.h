@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <iterator>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -68,12 +70,34 @@ struct Ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   uint64_t budget = 0;
-  uint64_t used = 0;
+  uint64_t used = 0;    // bytes of live device buffers
+  uint64_t cached = 0;  // bytes of released buffers kept for reuse
+  std::multimap<uint64_t, void*> cache;  // block size -> block
   std::mutex mu;
   int sm_count = 148;
+  // released blocks beyond this are freed at once
+  static constexpr uint64_t kCacheMax = 8ull << 30;
 
+  // A released block of at least `bytes` (at most a quarter + 1 MB larger),
+  // now live, or nullptr.  A problem rebuilt on the same context (a new pose)
+  // asks for nearly the same sizes, so it reuses its predecessor's memory
+  // without cudaMalloc / cudaFree, which synchronise the whole device.
+  void* take(uint64_t bytes, uint64_t& block) {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.lower_bound(bytes);
+    if (it == cache.end() || it->first > bytes + bytes / 4 + (1ull << 20)) return nullptr;
+    block = it->first;
+    void* p = it->second;
+    cache.erase(it);
+    cached -= block;
+    used += block;
+    return p;
+  }
+  // Budget for a new block (freeing released blocks first when they stand
+  // in the way).
   void charge(uint64_t bytes) {
     std::lock_guard<std::mutex> lk(mu);
+    if (budget && used + cached + bytes > budget) trim_locked();
     if (budget && used + bytes > budget)
       throw BudgetError("device allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget (" +
                         std::to_string(used) + " of " + std::to_string(budget) + " in use)");
@@ -83,9 +107,35 @@ struct Ctx {
     std::lock_guard<std::mutex> lk(mu);
     used -= bytes;
   }
+  // A live block goes back to the cache.  The context's work is ordered on
+  // its stream, so a later user of the block runs after the earlier ones.
+  void give(void* p, uint64_t block) {
+    std::lock_guard<std::mutex> lk(mu);
+    used -= block;
+    cache.emplace(block, p);
+    cached += block;
+    while (cached > kCacheMax && !cache.empty()) {  // the largest blocks first
+      auto it = std::prev(cache.end());
+      cudaFree(it->second);
+      cached -= it->first;
+      cache.erase(it);
+    }
+  }
+  void trim() {
+    std::lock_guard<std::mutex> lk(mu);
+    trim_locked();
+  }
+
+ private:
+  void trim_locked() {
+    for (auto& kv : cache) cudaFree(kv.second);
+    cache.clear();
+    cached = 0;
+  }
 };
 
-// Device allocation charged to a context's budget; freed on destruction.
+// Device allocation charged to a context's budget; released on destruction
+// (to the context's cache of blocks).
 class DevBuf {
  public:
   DevBuf() = default;
@@ -104,24 +154,32 @@ class DevBuf {
   void alloc(Ctx* ctx, size_t bytes) {
     reset();
     if (bytes == 0) return;
-    ctx->charge(bytes);
-    void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) {
-      ctx->release(bytes);
-      throw CudaError(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    uint64_t block = 0;
+    void* p = ctx->take(bytes, block);
+    if (!p) {
+      ctx->charge(bytes);
+      cudaError_t e = cudaMalloc(&p, bytes);
+      if (e == cudaErrorMemoryAllocation) {  // released blocks may be in the way
+        cudaGetLastError();
+        ctx->trim();
+        e = cudaMalloc(&p, bytes);
+      }
+      if (e != cudaSuccess) {
+        ctx->release(bytes);
+        throw CudaError(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+      }
+      block = bytes;
     }
     ctx_ = ctx;
     ptr_ = p;
     bytes_ = bytes;
+    block_ = block;
   }
   void reset() {
-    if (ptr_) {
-      cudaFree(ptr_);
-      ctx_->release(bytes_);
-    }
+    if (ptr_) ctx_->give(ptr_, block_);
     ptr_ = nullptr;
     bytes_ = 0;
+    block_ = 0;
     ctx_ = nullptr;
   }
   template <typename T>
@@ -136,10 +194,12 @@ class DevBuf {
     std::swap(ctx_, o.ctx_);
     std::swap(ptr_, o.ptr_);
     std::swap(bytes_, o.bytes_);
+    std::swap(block_, o.block_);
   }
   Ctx* ctx_ = nullptr;
   void* ptr_ = nullptr;
-  size_t bytes_ = 0;
+  size_t bytes_ = 0;   // requested
+  uint64_t block_ = 0;  // allocated (a reused block may be larger)
 };
 
 template <typename T>
@@ -173,6 +233,18 @@ struct NearField {
   std::vector<NfItem> h_items;
 };
 
+// A mesh's node patches in its own frame, checked and uploaded once
+// (bp_mesh_create); instances of it are placed on the device.
+struct DevMesh {
+  Ctx* ctx = nullptr;
+  int n = 0;
+  double centre[3] = {0, 0, 0};
+  std::vector<double> h_centroid, h_normal, h_area, h_gc;
+  std::vector<int32_t> h_qual_off, h_quad_off, h_gal_off;
+  int n_qual_pts = 0, n_quad_pts = 0, n_gal_pts = 0;
+  DevBuf d_qual, d_quad, d_gal;  // SoA of double, 7 arrays each
+};
+
 struct Problem;
 struct FmmState;  // far-field state (fmm.cu)
 void fmm_destroy(FmmState*);
@@ -186,7 +258,7 @@ struct Problem {
   // patches (original order)
   std::vector<double> h_centroid, h_normal, h_area, h_eps, h_gc;
   std::vector<int32_t> h_qual_off, h_quad_off, h_gal_off;
-  std::vector<double> h_qual, h_quad, h_gal;
+  int n_qual_pts = 0, n_quad_pts = 0, n_gal_pts = 0;  // point counts of the device point lists
   DevBuf d_centroid, d_normal, d_area, d_eps;               // double
   DevBuf d_qual_off, d_quad_off, d_gal_off;                 // int32
   DevBuf d_qual, d_quad, d_gal;                             // SoA of double, 7 arrays

@@ -418,7 +418,7 @@ void nf_assemble(Problem& P) {
   DevBuf d_gc = upload(ctx, P.h_gc);
   {
     P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
-    const int ng = (int)(P.h_gal.size() / 7);
+    const int ng = P.n_gal_pts;
     const int threads = 256;
     const int blocks = (P.n * 32 + threads - 1) / threads;
     singular_kernel<<<blocks, threads, 0, ctx->stream>>>(P.n, P.d_gal_off.as<int32_t>(), P.d_gal.as<double>(), ng,
@@ -432,8 +432,8 @@ void nf_assemble(Problem& P) {
   DevBuf d_asm_items = upload(ctx, asm_items);
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
   nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
-  const int nq = (int)(P.h_qual.size() / 7);
-  const int np = (int)(P.h_quad.size() / 7);
+  const int nq = P.n_qual_pts;
+  const int np = P.n_quad_pts;
   const size_t smem = elem * 7 * (size_t)max_tq;
   if (smem > 200 * 1024) throw std::invalid_argument("too many qualocation points per patch");
   if (!asm_items.empty()) {

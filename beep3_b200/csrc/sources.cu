@@ -162,7 +162,7 @@ __global__ void sum_points_kernel(const int32_t* __restrict__ off, int first, in
 void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev) {
   // FP64 engine: exact FP64 sum; mixed engine: the fast FP32 terms
   Ctx* ctx = P.ctx;
-  const int nq = (int)(P.h_qual.size() / 7);
+  const int nq = P.n_qual_pts;
   DevBuf& vals = P.scratch_vals;
   if (vals.bytes() < sizeof(double) * 2 * (size_t)nq) vals.alloc(ctx, sizeof(double) * 2 * (size_t)nq);
   const double scale = kOneOver4Pi / eps_solvent;
@@ -182,7 +182,7 @@ void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps
 void energy_coefficients_device(Problem& P, int first, int count, const double* charges_dev, int n_charges,
                                 double* cf_dev, double* ch_dev) {
   Ctx* ctx = P.ctx;
-  const int ng = (int)(P.h_gal.size() / 7);
+  const int ng = P.n_gal_pts;
   const int p0 = P.h_gal_off[first], p1 = P.h_gal_off[first + count];
   DevBuf vals(ctx, sizeof(double) * 2 * (size_t)std::max(1, p1 - p0));
   if (p1 > p0) {

@@ -8,9 +8,10 @@ instances) is solved with GMRES on the device and
     E_int(pose) = E(A + B) - E(A alone) - E(B alone)
 
 in kJ/mol, with E the BEM solvation energy summed over instances
-(BEEP::calculate_energies).  Poses are independent: several run
+(BEEP::calculate_energies).  Poses are independent: several workers run
 concurrently, each on its own engine context and CUDA stream (the calls
-release the GIL), so their kernels overlap on the GPU.
+release the GIL), so their kernels overlap on the GPU; a worker keeps both
+meshes on the device and places B on the device for each of its poses.
 """
 from __future__ import annotations
 
@@ -69,21 +70,44 @@ def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it):
         bp.close()
 
 
+def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, tol, max_it):
+    """Poses idx on one engine context: the two meshes stay on the device and
+    each pose only moves instance B (a new tree, near field and far-field
+    set-up, then the solve)."""
+    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device)
+    out = []
+    try:
+        ident = np.array([1.0, 0.0, 0.0, 0.0])
+        ca = mesh_a.centre
+        bp.insert_mesh_instance(mesh_a, offset=ca, rotation=ident, eps_protein=2.0)
+        bp.insert_mesh_instance(mesh_b, offset=ca + poses[idx[0]].offset, rotation=poses[idx[0]].rotation,
+                                eps_protein=2.0)
+        for k in idx:
+            bp.move_mesh_instance(1, ca + poses[k].offset, poses[k].rotation)
+            info = bp.solve(tol, max_it)
+            e, _ = bp.calculate_energies()
+            out.append((k, e, info.num_iterations))
+    finally:
+        bp.close()
+    return out
+
+
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
                     nbsize: int = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
                     max_iterations: int = 100) -> ScanResult:
     t0 = time.perf_counter()
     ident = np.array([1.0, 0.0, 0.0, 0.0])
     ca = mesh_a.centre
-    with ThreadPoolExecutor(max_workers=workers) as ex:
+    workers = max(1, min(workers, len(poses)))
+    with ThreadPoolExecutor(max_workers=workers + 2) as ex:
         fa = ex.submit(_solve_energy, [(mesh_a, ca, ident)], kappa, precision, nbsize, device, tol, max_iterations)
         fb = ex.submit(_solve_energy, [(mesh_b, mesh_b.centre, ident)], kappa, precision, nbsize, device, tol,
                        max_iterations)
-        fp = [ex.submit(_solve_energy, [(mesh_a, ca, ident), (mesh_b, ca + p.offset, p.rotation)], kappa, precision,
-                        nbsize, device, tol, max_iterations) for p in poses]
+        fw = [ex.submit(_scan_worker, mesh_a, mesh_b, poses, list(range(w, len(poses), workers)), kappa, precision,
+                        nbsize, device, tol, max_iterations) for w in range(workers)]
         e_a, _ = fa.result()
         e_b, _ = fb.result()
-        res = [f.result() for f in fp]
+        res = sorted(r for f in fw for r in f.result())
     dt = time.perf_counter() - t0
-    ec = [r[0] for r in res]
-    return ScanResult([e - e_a - e_b for e in ec], ec, e_a, e_b, dt, [r[1] for r in res])
+    ec = [r[1] for r in res]
+    return ScanResult([e - e_a - e_b for e in ec], ec, e_a, e_b, dt, [r[2] for r in res])

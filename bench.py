@@ -240,6 +240,10 @@ def run_reference(args):
     world, rank, local, dist = dist_setup(args)
     if rank != 0:
         return
+    if args.workload in ("scan", "serve"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the matvec workloads only"}),
+              flush=True)
+        return
     desc, meshes, kappa, nbsize = workload(args.workload)
     import beep3_b200 as b  # geometry preparation (host) only
     bp = b.BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision="mixed")
@@ -295,10 +299,90 @@ def _only_matvec(args, local):
     bp.close()
 
 
+def _scan_mode(args, local):
+    """Batched rigid-body scan: two star molecules (40962 and 10242 patches,
+    different seeds) over random poses (uniform quaternion, centre separation
+    uniform in 45-80 A), each pose's complex solved and its interaction
+    energy taken; poses run concurrently on their own engine contexts."""
+    import beep3_b200 as b
+    from beep3_b200.scan import random_poses, rigid_body_scan
+    va, ta, sa = b.star_surface(6, 20.0, seed=1235)
+    ma = b.Mesh(va, ta, b.charges_in_star(2000, sa, seed=1236))
+    vb, tb, sb = b.star_surface(5, 20.0, seed=2235)
+    mb = b.Mesh(vb, tb, b.charges_in_star(500, sb, seed=2236))
+    poses = random_poses(args.poses, seed=1237)
+    rigid_body_scan(ma, mb, poses[:2], kappa=0.1, workers=args.workers, device=local)  # warm-up
+    res = rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local)
+    e = np.asarray(res.energies)
+    print(json.dumps({
+        "metric": "rigid-body scan poses/s (mixed engine, full solve + interaction energy per pose)",
+        "value": res.poses_per_s, "unit": "poses/s", "n_gpus": 1, "higher_is_better": True,
+        "data": "synthetic", "dtype": "fp32 near field/FMM + fp64 singular/GMRES",
+        "config": {"workload": "batched rigid-body scan: star k=6 (40962 patches, 2000 charges) + star k=5 "
+                               "(10242 patches, 500 charges), kappa 0.1, separation 45-80 A",
+                   "poses": len(poses), "concurrent_poses": args.workers},
+        "seconds": res.seconds, "mean_iterations": float(np.mean(res.iterations)),
+        "interaction_energy_kj_per_mol": {"min": float(e.min()), "max": float(e.max()), "mean": float(e.mean())},
+    }), flush=True)
+
+
+def _serve_mode(args, local):
+    """Served request stream: Poisson arrivals of single-molecule solves,
+    patch counts log-uniform in 2562-163842 (snapped to icosphere levels
+    4-7, radius scaled with the patch count), charges 0.05 x patches, kappa
+    from {0, 0.05, 0.1, 0.15}; admission by HBM budget with worker slots."""
+    import beep3_b200 as b
+    from beep3_b200.server import BemServer, SolveRequest
+    rng = np.random.default_rng(4321)
+    levels = {2562: 4, 10242: 5, 40962: 6, 163842: 7}
+    sizes = np.array(sorted(levels))
+    meshes = {}
+    plan = []
+    for r in range(args.requests):
+        n = float(np.exp(rng.uniform(np.log(2562), np.log(163842))))
+        n_snap = int(sizes[np.argmin(np.abs(np.log(sizes) - np.log(n)))])
+        kappa = float(rng.choice([0.0, 0.05, 0.1, 0.15]))
+        plan.append((n_snap, kappa, float(rng.exponential(1.0 / args.rate))))
+        if n_snap not in meshes:
+            k = levels[n_snap]
+            v, t, shape = b.star_surface(k, 20.0 * (n_snap / 40962) ** 0.5, seed=5000 + k)
+            meshes[n_snap] = b.Mesh(v, t, b.charges_in_star(int(0.05 * n_snap), shape, seed=6000 + k))
+    srv = BemServer(device=local, workers=args.workers)
+    try:
+        srv.submit(SolveRequest(meshes[min(meshes)], 0.1)).result()  # warm-up
+        futs = []
+        t0 = time.perf_counter()
+        for n_snap, kappa, gap in plan:
+            time.sleep(gap)
+            futs.append(srv.submit(SolveRequest(meshes[n_snap], kappa, tag=n_snap)))
+        results = [f.result() for f in futs]
+        wall = max(r.end for r in results) - t0
+    finally:
+        srv.close()
+    lat = np.array([r.latency_ms for r in results])
+    print(json.dumps({
+        "metric": "served solves/s and p50/p99 latency (mixed engine, continuous batching)",
+        "value": len(results) / wall, "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+        "data": "synthetic", "dtype": "fp32 near field/FMM + fp64 singular/GMRES",
+        "config": {"workload": "served stream: Poisson arrivals, star surfaces of 2562-163842 patches "
+                               "(log-uniform), charges 0.05 x patches, kappa in {0, 0.05, 0.1, 0.15}",
+                   "requests": len(results), "rate_per_s": args.rate, "worker_slots": args.workers},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max())},
+        "all_converged": all(r.converged for r in results),
+        "peak_device_bytes_admitted": srv.peak_in_use,
+        "patches": {str(k): int(sum(1 for r in results if r.n_patches == k)) for k in sorted(meshes)},
+    }), flush=True)
+
+
 def _run_ours(args, world, rank, local, dist):
     import torch
     if args.only_matvec:
         _only_matvec(args, local)
+        return
+    if args.workload in ("scan", "serve"):
+        if rank == 0:
+            (_scan_mode if args.workload == "scan" else _serve_mode)(args, local)
         return
     dev = torch.device("cuda", local)
     desc, meshes, kappa, nbsize = workload(args.workload)
@@ -404,7 +488,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="star", choices=["kirkwood", "star", "star-small"])
+    ap.add_argument("--workload", default="star", choices=["kirkwood", "star", "star-small", "scan", "serve"],
+                    help="scan / serve: the batched rigid-body scan and the served request stream")
+    ap.add_argument("--poses", type=int, default=64, help="scan: number of poses")
+    ap.add_argument("--requests", type=int, default=24, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=8.0, help="serve: Poisson arrival rate, requests/s")
+    ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

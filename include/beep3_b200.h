@@ -135,6 +135,35 @@ typedef struct {
  * BEEP::precalc_neighbour_interactions, src/beep/beep.cpp:1585-1641,
  * :768-956). */
 int32_t bp_problem_create(bp_ctx ctx, const bp_patches* patches, const bp_params* params, bp_problem* out);
+
+/* ---------------------------------------------------------------------------
+ * Device-resident meshes and posed problems (rigid-body scans).  A mesh's
+ * node patches, in its own frame, are checked and uploaded once; a problem
+ * is then built from instances of such meshes, each placed by a rigid move
+ * p -> R (p - centre) + offset, n -> R n that runs on the device, so a new
+ * pose costs no host transform and no upload of point lists.  The reference
+ * moves its host patch objects for every pose instead
+ * (MeshInstance::init, src/bem/mesh_instance.cpp:50-85; NodePatch
+ * change_coordinate_frame, src/bem/node_patch.cpp:402-478); these entry
+ * points have no counterpart there.  A mesh must outlive the problems built
+ * from it; its patches' dielectric_ratio entries are ignored (the instance
+ * gives it).
+ */
+typedef struct bp_mesh_s* bp_mesh;
+int32_t bp_mesh_create(bp_ctx ctx, const bp_patches* patches, const double centre[3], bp_mesh* out);
+int32_t bp_mesh_destroy(bp_mesh mesh);
+
+typedef struct {
+  bp_mesh mesh;
+  double rotation[9];       /* row-major R */
+  double offset[3];         /* where the mesh centre goes */
+  double dielectric_ratio;  /* eps_solvent / eps_protein of this instance */
+} bp_instance;
+
+/* bp_problem_create for the instances' patches, concatenated in instance
+ * order. */
+int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* instances, int32_t n_instances,
+                                const bp_params* params, bp_problem* out);
 int32_t bp_problem_destroy(bp_problem p);
 int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info);
 
