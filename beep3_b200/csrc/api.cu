@@ -33,26 +33,45 @@ struct DeviceGuard {
   }
 };
 
-// Structure-of-arrays copy of [n][7] points: 7 arrays of n values.
-template <typename T>
-std::vector<T> soa7(const std::vector<double>& aos) {
-  const size_t n = aos.size() / 7;
-  std::vector<T> out(aos.size());
-  for (size_t i = 0; i < n; ++i)
-    for (int f = 0; f < 7; ++f) out[f * n + i] = (T)aos[7 * i + f];
-  return out;
+// [n][7] points (x y z nx ny nz w) -> 7 arrays of n values, FP32 copy too
+// when soa_f is set; *bad is set when a value is not finite.
+__global__ void aos_to_soa_kernel(const double* __restrict__ aos, int n, double* __restrict__ soa,
+                                  float* __restrict__ soa_f, int* __restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bool ok = true;
+  for (int f = 0; f < 7; ++f) {
+    const double v = aos[7 * (size_t)i + f];
+    ok = ok && isfinite(v);
+    soa[(size_t)f * n + i] = v;
+    if (soa_f) soa_f[(size_t)f * n + i] = (float)v;
+  }
+  if (!ok) atomicOr(bad, 1);
 }
 
-void check_points(const char* what, int n, const int32_t* off, const double* pts, std::vector<int32_t>& h_off,
-                  std::vector<double>& h_pts) {
+// A patch point list: offsets checked on the host, the points uploaded as
+// given and laid out (and checked) on the device.
+void upload_points(Ctx* c, const char* what, int n, const int32_t* off, const double* pts,
+                   std::vector<int32_t>& h_off, int& n_pts, DevBuf& soa, DevBuf* soa_f) {
   if (!off || !pts) throw std::invalid_argument(std::string(what) + ": missing point list");
   h_off.assign(off, off + n + 1);
   if (h_off[0] != 0) throw std::invalid_argument(std::string(what) + ": offsets must start at 0");
   for (int i = 0; i < n; ++i)
     if (h_off[i + 1] <= h_off[i]) throw std::invalid_argument(std::string(what) + ": every patch needs points");
-  h_pts.assign(pts, pts + 7 * (size_t)h_off[n]);
-  for (double v : h_pts)
-    if (!std::isfinite(v)) throw std::invalid_argument(std::string(what) + ": non-finite point data");
+  n_pts = h_off[n];
+  DevBuf aos(c, sizeof(double) * 7 * (size_t)n_pts);
+  DevBuf bad(c, sizeof(int));
+  BP_CUDA(cudaMemcpyAsync(aos.get(), pts, aos.bytes(), cudaMemcpyHostToDevice, c->stream));
+  BP_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(int), c->stream));
+  soa.alloc(c, sizeof(double) * 7 * (size_t)n_pts);
+  if (soa_f) soa_f->alloc(c, sizeof(float) * 7 * (size_t)n_pts);
+  aos_to_soa_kernel<<<(n_pts + 255) / 256, 256, 0, c->stream>>>(aos.as<double>(), n_pts, soa.as<double>(),
+                                                                 soa_f ? soa_f->as<float>() : nullptr, bad.as<int>());
+  BP_LAUNCH_CHECK();
+  int h_bad = 0;
+  BP_CUDA(cudaMemcpyAsync(&h_bad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BP_CUDA(cudaStreamSynchronize(c->stream));
+  if (h_bad) throw std::invalid_argument(std::string(what) + ": non-finite point data");
 }
 
 int32_t check_params(const char* who, const bp_params* prm) {
@@ -203,23 +222,12 @@ BP_API int32_t bp_problem_create(bp_ctx ctx, const bp_patches* pp, const bp_para
         if (!std::isfinite(P->h_centroid[3 * i + k]) || !std::isfinite(P->h_normal[3 * i + k]))
           return fail(BP_ERR_INVALID, "bp_problem_create: non-finite patch geometry");
     }
-    {
-      std::vector<double> qual, quad, gal;
-      check_points("qualocation", n, pp->qual_offsets, pp->qual_points, P->h_qual_off, qual);
-      check_points("quadrature", n, pp->quad_offsets, pp->quad_points, P->h_quad_off, quad);
-      check_points("galerkin", n, pp->galerkin_offsets, pp->galerkin_points, P->h_gal_off, gal);
-      P->n_qual_pts = P->h_qual_off[n];
-      P->n_quad_pts = P->h_quad_off[n];
-      P->n_gal_pts = P->h_gal_off[n];
-      P->d_qual = upload(c, soa7<double>(qual));
-      P->d_quad = upload(c, soa7<double>(quad));
-      P->d_gal = upload(c, soa7<double>(gal));
-      if (!P->fp64) {
-        P->d_qual_f = upload(c, soa7<float>(qual));
-        P->d_quad_f = upload(c, soa7<float>(quad));
-      }
-      BP_CUDA(cudaStreamSynchronize(c->stream));  // the host staging vectors go out of scope
-    }
+    upload_points(c, "qualocation", n, pp->qual_offsets, pp->qual_points, P->h_qual_off, P->n_qual_pts, P->d_qual,
+                  P->fp64 ? nullptr : &P->d_qual_f);
+    upload_points(c, "quadrature", n, pp->quad_offsets, pp->quad_points, P->h_quad_off, P->n_quad_pts, P->d_quad,
+                  P->fp64 ? nullptr : &P->d_quad_f);
+    upload_points(c, "galerkin", n, pp->galerkin_offsets, pp->galerkin_points, P->h_gal_off, P->n_gal_pts, P->d_gal,
+                  nullptr);
     finish_problem(c, *P);
     *out = reinterpret_cast<bp_problem>(P.release());
     return BP_OK;
@@ -250,17 +258,12 @@ BP_API int32_t bp_mesh_create(bp_ctx ctx, const bp_patches* pp, const double cen
       for (int k = 0; k < 3; ++k)
         if (!std::isfinite(m->h_centroid[3 * i + k]) || !std::isfinite(m->h_normal[3 * i + k]))
           return fail(BP_ERR_INVALID, "bp_mesh_create: non-finite patch geometry");
-    std::vector<double> qual, quad, gal;
-    check_points("qualocation", n, pp->qual_offsets, pp->qual_points, m->h_qual_off, qual);
-    check_points("quadrature", n, pp->quad_offsets, pp->quad_points, m->h_quad_off, quad);
-    check_points("galerkin", n, pp->galerkin_offsets, pp->galerkin_points, m->h_gal_off, gal);
-    m->n_qual_pts = m->h_qual_off[n];
-    m->n_quad_pts = m->h_quad_off[n];
-    m->n_gal_pts = m->h_gal_off[n];
-    m->d_qual = upload(c, soa7<double>(qual));
-    m->d_quad = upload(c, soa7<double>(quad));
-    m->d_gal = upload(c, soa7<double>(gal));
-    BP_CUDA(cudaStreamSynchronize(c->stream));
+    upload_points(c, "qualocation", n, pp->qual_offsets, pp->qual_points, m->h_qual_off, m->n_qual_pts, m->d_qual,
+                  nullptr);
+    upload_points(c, "quadrature", n, pp->quad_offsets, pp->quad_points, m->h_quad_off, m->n_quad_pts, m->d_quad,
+                  nullptr);
+    upload_points(c, "galerkin", n, pp->galerkin_offsets, pp->galerkin_points, m->h_gal_off, m->n_gal_pts, m->d_gal,
+                  nullptr);
     *out = reinterpret_cast<bp_mesh>(m.release());
     return BP_OK;
   });
