@@ -94,6 +94,7 @@ _SIGS = {
     "bp_ctx_set_stream": [_P, _P],
     "bp_ctx_memory": [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
     "bp_ctx_synchronize": [_P],
+    "bp_ctx_cache": [_P, C.POINTER(C.c_uint64), _I],
     "bp_geom_create": [_I, _P, _P, _I, _P, _I, _I, _I, _PP],
     "bp_geom_sizes": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)],
     "bp_geom_copy": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -112,6 +112,71 @@ class MeshInstance:
         return self.mesh.radius
 
 
+class EngineContext:
+    """A device context (bp_ctx) with the meshes it holds on the device, for
+    scenarios (BEEP objects) that run one after another on it: the later ones
+    upload no mesh and reuse the device blocks of the earlier ones.  One
+    thread at a time."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_meshes: int = 8):
+        """``max_meshes``: device-resident meshes kept; beyond it the least
+        recently used one not needed by the scenario being built goes."""
+        self.device = int(device)
+        self.max_meshes = int(max_meshes)
+        self._ctx = C.c_void_p()
+        N.check(N.lib().bp_ctx_create(self.device, int(hbm_budget_bytes), C.byref(self._ctx)))
+        # id(mesh) -> [mesh, handle, build in which it was last used]; holding
+        # the mesh keeps its id from being reused while the entry exists
+        self._meshes: dict[int, list] = {}
+        self._build = 0
+
+    def begin_build(self) -> None:
+        """Marks the start of a scenario build (its meshes are not evicted)."""
+        self._build += 1
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._ctx
+
+    def mesh_handle(self, mesh: Mesh) -> C.c_void_p:
+        """The mesh's patches (its own frame) on the device, uploaded on first
+        use (bp_mesh_create)."""
+        entry = self._meshes.get(id(mesh))
+        if entry is None:
+            stale = sorted((e[2], k) for k, e in self._meshes.items() if e[2] < self._build)
+            while len(self._meshes) >= self.max_meshes and stale:
+                N.lib().bp_mesh_destroy(self._meshes.pop(stale.pop(0)[1])[1])
+            p = mesh.patches
+            pp = N.bp_patches(p.n, N.ptr(p.centroid), N.ptr(p.normal), N.ptr(p.area), None, None,
+                              N.ptr(p.qual_off), N.ptr(p.qual), N.ptr(p.quad_off), N.ptr(p.quad),
+                              N.ptr(p.gal_off), N.ptr(p.gal))
+            h = C.c_void_p()
+            N.check(N.lib().bp_mesh_create(self._ctx, C.byref(pp), N.ptr(np.ascontiguousarray(mesh.centre)),
+                                           C.byref(h)))
+            entry = [mesh, h, self._build]
+            self._meshes[id(mesh)] = entry
+        entry[2] = self._build
+        return entry[1]
+
+    def memory(self) -> tuple[int, int]:
+        """(bytes in live device buffers, bytes of released blocks kept for reuse)."""
+        used, budget, cached = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        N.check(N.lib().bp_ctx_memory(self._ctx, C.byref(used), C.byref(budget)))
+        N.check(N.lib().bp_ctx_cache(self._ctx, C.byref(cached), 0))
+        return int(used.value), int(cached.value)
+
+    def release_cache(self) -> None:
+        N.check(N.lib().bp_ctx_cache(self._ctx, None, 1))
+
+    def close(self) -> None:
+        for e in self._meshes.values():
+            N.lib().bp_mesh_destroy(e[1])
+        self._meshes = {}
+        if self._ctx:
+            N.lib().bp_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+
 @dataclass
 class RunInfo:
     num_iterations: int
@@ -131,7 +196,11 @@ class BEEP:
     """Scenario and solver (mirror of libBEEP's BEEP class)."""
 
     def __init__(self, eps_solvent: float = 80.0, kappa: float = 0.1, nbsize: int = DEFAULT_NBSIZE,
-                 nterms: int = 9, precision: str = "fp64", device: int = 0, hbm_budget_bytes: int = 0):
+                 nterms: int = 9, precision: str = "fp64", device: int = 0, hbm_budget_bytes: int = 0,
+                 context: EngineContext | None = None):
+        """``context``: an EngineContext shared with scenarios run before or
+        after this one (its device and budget apply); by default the scenario
+        has its own."""
         self.eps_solvent = float(eps_solvent)
         self.kappa = float(kappa)
         self.nbsize = int(nbsize)
@@ -142,8 +211,10 @@ class BEEP:
         self.instances: list[MeshInstance] = []
         self.device = int(device)
         self.hbm_budget_bytes = int(hbm_budget_bytes)
-        self._ctx = C.c_void_p()
-        self._meshes: dict[int, tuple[Mesh, C.c_void_p]] = {}  # id(mesh) -> device-resident copy
+        self._engine = context
+        self._own_engine = context is None
+        if context is not None:
+            self.device = context.device
         self._problem = None
         self.bounding_cube = None
         self._manual_cube = False
@@ -191,12 +262,9 @@ class BEEP:
 
     def close(self) -> None:
         self._invalidate()
-        for _, h in self._meshes.values():
-            N.lib().bp_mesh_destroy(h)
-        self._meshes = {}
-        if self._ctx:
-            N.lib().bp_ctx_destroy(self._ctx)
-            self._ctx = C.c_void_p()
+        if self._own_engine and self._engine is not None:
+            self._engine.close()
+            self._engine = None
 
     def __del__(self):
         try:
@@ -236,26 +304,18 @@ class BEEP:
         return sum(i.n_patches for i in self.instances)
 
     def _mesh_handle(self, mesh: Mesh) -> C.c_void_p:
-        """The mesh's patches (its own frame) on this context's device,
-        uploaded on first use (bp_mesh_create)."""
-        entry = self._meshes.get(id(mesh))
-        if entry is None:
-            p = mesh.patches
-            pp = N.bp_patches(p.n, N.ptr(p.centroid), N.ptr(p.normal), N.ptr(p.area), None, None,
-                              N.ptr(p.qual_off), N.ptr(p.qual), N.ptr(p.quad_off), N.ptr(p.quad),
-                              N.ptr(p.gal_off), N.ptr(p.gal))
-            h = C.c_void_p()
-            N.check(N.lib().bp_mesh_create(self.context(), C.byref(pp), N.ptr(np.ascontiguousarray(mesh.centre)),
-                                           C.byref(h)))
-            entry = (mesh, h)
-            self._meshes[id(mesh)] = entry
-        return entry[1]
+        return self.engine.mesh_handle(mesh)
+
+    @property
+    def engine(self) -> EngineContext:
+        """The engine context (created on first use unless one was given)."""
+        if self._engine is None:
+            self._engine = EngineContext(self.device, self.hbm_budget_bytes)
+        return self._engine
 
     def context(self) -> C.c_void_p:
-        """The device context (created on first use)."""
-        if not self._ctx:
-            N.check(N.lib().bp_ctx_create(self.device, self.hbm_budget_bytes, C.byref(self._ctx)))
-        return self._ctx
+        """The device context handle."""
+        return self.engine.handle
 
     def gathered(self) -> dict:
         """All instances' patch arrays concatenated in patch order (host)."""
@@ -279,6 +339,7 @@ class BEEP:
         self._arrays = {"first": np.cumsum([0] + [i.n_patches for i in self.instances])}
         centre, edge = self.calculate_bounding_cube()
         insts = (N.bp_instance * len(self.instances))()
+        self.engine.begin_build()
         for k, inst in enumerate(self.instances):
             insts[k].mesh = self._mesh_handle(inst.mesh)
             insts[k].rotation[:] = [float(v) for v in inst.matrix.ravel()]
@@ -287,7 +348,7 @@ class BEEP:
         prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge, self.nbsize, self.nterms,
                           N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED, 0)
         h = C.c_void_p()
-        N.check(N.lib().bp_problem_create_posed(self._ctx, insts, len(self.instances), C.byref(prm), C.byref(h)))
+        N.check(N.lib().bp_problem_create_posed(self.context(), insts, len(self.instances), C.byref(prm), C.byref(h)))
         self._problem = h
         return h
 

@@ -185,6 +185,23 @@ BP_API int32_t bp_ctx_memory(bp_ctx ctx, uint64_t* used, uint64_t* budget) {
   return BP_OK;
 }
 
+BP_API int32_t bp_ctx_cache(bp_ctx ctx, uint64_t* cached, int32_t release) {
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c) return fail(BP_ERR_INVALID, "bp_ctx_cache: null context");
+    if (release) {
+      DeviceGuard g(c->device);
+      BP_CUDA(cudaStreamSynchronize(c->stream));
+      c->trim();
+    }
+    if (cached) {
+      std::lock_guard<std::mutex> lk(c->mu);
+      *cached = c->cached;
+    }
+    return BP_OK;
+  });
+}
+
 BP_API int32_t bp_ctx_synchronize(bp_ctx ctx) {
   return guarded_engine([&]() -> int32_t {
     Ctx* c = as_ctx(ctx);

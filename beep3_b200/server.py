@@ -7,8 +7,12 @@ concurrently, each on its own engine context (own CUDA stream), so their
 kernels overlap on the device while later requests wait in the queue.
 Device state (tree, near-field coefficients, FMM expansions, Krylov basis)
 stays resident for the lifetime of a request and is released at completion,
-which frees budget for the next admission.  Latency is measured from
-arrival to completion.
+which frees budget for the next admission.  Each worker slot keeps one
+engine context for the requests it runs in turn, so a molecule seen before
+is not uploaded again and a request reuses the device blocks its slot's
+previous request released (those blocks are returned to the driver when an
+admission needs their room).  Latency is measured from arrival to
+completion.
 
 The engine's kernels are deterministic (no atomics in any reduction), so a
 request's result does not depend on what else is running.
@@ -23,7 +27,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .beep import BEEP, DEFAULT_NBSIZE, Mesh
+from .beep import BEEP, DEFAULT_NBSIZE, EngineContext, Mesh
 
 
 @dataclass
@@ -89,6 +93,7 @@ class BemServer:
         self._in_use = 0
         self._slots = workers
         self._threads: list[threading.Thread] = []
+        self._contexts: list[EngineContext] = []  # idle engine contexts of the slots
         self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         self._closed = False
         self.peak_in_use = 0
@@ -105,6 +110,9 @@ class BemServer:
         self._dispatcher.join()
         for t in self._threads:
             t.join()
+        for c in self._contexts:
+            c.close()
+        self._contexts = []
 
     # -------------------------------------------------------------- internals
     def _dispatch(self) -> None:
@@ -121,14 +129,24 @@ class BemServer:
                 self._slots -= 1
                 self._in_use += need
                 self.peak_in_use = max(self.peak_in_use, self._in_use)
+                if self.runner == self._engine_solve:
+                    # blocks the idle slots keep for reuse count against the budget
+                    kept = sum(c.memory()[1] for c in self._contexts)
+                    if self._in_use + kept > self.budget:
+                        for c in self._contexts:
+                            c.release_cache()
             t = threading.Thread(target=self._run, args=(req, fut, need), daemon=True)
             self._threads.append(t)
             t.start()
 
     def _engine_solve(self, req: SolveRequest, need: int) -> SolveResult:
         start = time.perf_counter()
+        with self._lock:
+            ectx = self._contexts.pop() if self._contexts else None
+        if ectx is None:
+            ectx = EngineContext(self.device)
         bp = BEEP(eps_solvent=req.eps_solvent, kappa=req.kappa, nbsize=self.nbsize, precision=self.precision,
-                  device=self.device)
+                  context=ectx)
         try:
             bp.insert_mesh_instance(req.mesh, eps_protein=req.eps_protein)
             info = bp.solve(req.tol, req.max_iterations, restart=self.restart)
@@ -137,7 +155,9 @@ class BemServer:
             return SolveResult(req.tag, e, info.num_iterations, info.converged, bp.num_patches, dev_bytes,
                                req.arrival, start, time.perf_counter())
         finally:
-            bp.close()
+            bp.close()  # the problem; the context goes back to the idle slots
+            with self._lock:
+                self._contexts.append(ectx)
 
     def _run(self, req: SolveRequest, fut: Future, need: int) -> None:
         try:

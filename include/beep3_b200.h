@@ -66,6 +66,11 @@ int32_t bp_ctx_create(int32_t device, uint64_t hbm_budget_bytes, bp_ctx* out);
 int32_t bp_ctx_destroy(bp_ctx ctx);
 int32_t bp_ctx_set_stream(bp_ctx ctx, void* cuda_stream); /* cudaStream_t; NULL = the context's own */
 int32_t bp_ctx_memory(bp_ctx ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
+/* Device blocks of destroyed problems that the context keeps for the next
+ * problem of similar size (no cudaMalloc / cudaFree between poses): their
+ * bytes, and with release != 0 their return to the driver.  No counterpart in
+ * the reference (its OpenCL buffers are allocated per work blob). */
+int32_t bp_ctx_cache(bp_ctx ctx, uint64_t* cached_bytes, int32_t release);
 int32_t bp_ctx_synchronize(bp_ctx ctx);
 
 /* ---------------------------------------------------------------------------

@@ -59,7 +59,7 @@ def test_posed_equals_host_transformed(precision, tol):
         finally:
             N.lib().bp_problem_destroy(h)
         assert rel_l2(y2, y2h) < tol
-        assert len(bp._meshes) == 2
+        assert len(bp.engine._meshes) == 2
     finally:
         bp.close()
 
@@ -85,3 +85,36 @@ def test_posed_rejects_bad_instances():
         assert N.lib().bp_problem_create_posed(bp.context(), inst, 1, C.byref(prm), C.byref(h)) == N.BP_ERR_INVALID
     finally:
         bp.close()
+
+
+def test_shared_context_reuses_and_evicts_meshes():
+    """Scenarios run in turn on one EngineContext: a mesh seen before is not
+    uploaded again, at most max_meshes stay resident, and every scenario gives
+    the result it gives on a context of its own."""
+    meshes = []
+    for s in range(3):
+        V, T, shape = b.star_surface(3, 10.0 + 2 * s, seed=31 + s)
+        meshes.append(b.Mesh(V, T, b.charges_in_star(10, shape, seed=41 + s)))
+    ectx = b.EngineContext(0, max_meshes=2)
+    try:
+        for m in meshes + meshes[:1]:
+            own = b.BEEP(kappa=0.1, nbsize=300, precision="mixed")
+            shared = b.BEEP(kappa=0.1, nbsize=300, precision="mixed", context=ectx)
+            try:
+                for bp in (own, shared):
+                    bp.insert_mesh_instance(m)
+                    bp.solve(1e-6, 50)
+                e_own, _ = own.calculate_energies()
+                e_shared, _ = shared.calculate_energies()
+                assert e_shared == e_own
+            finally:
+                own.close()
+                shared.close()
+            assert len(ectx._meshes) <= 2
+            assert id(m) in ectx._meshes
+        used, cached = ectx.memory()
+        assert cached > 0  # the last problem's blocks are kept for the next one
+        ectx.release_cache()
+        assert ectx.memory()[1] == 0
+    finally:
+        ectx.close()
