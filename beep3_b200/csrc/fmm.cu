@@ -1996,49 +1996,54 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   BP_CUDA(cudaStreamSynchronize(st));
 }
 
-// Operator [lg][k][row] (rows padded to RP, R valid) as tensor-core blocks
-// [lg][row tile of 128][k chunk of 32][hi, lo][8 panels of 4 k][128 rows][4]
-// with hi = the FP32 value with its 13 low mantissa bits cleared and
-// lo = value - hi.
-static std::vector<float> pack_tensor(const std::vector<double>& ops, int nlg, int K, int RP, int R, int& n_mt,
-                                      int& n_ch) {
-  n_mt = (R + tc::kRows - 1) / tc::kRows;
-  n_ch = (K + tc::kKC - 1) / tc::kKC;
-  const size_t blk = 2 * tc::kHalf / sizeof(float);
-  std::vector<float> out((size_t)nlg * n_mt * n_ch * blk, 0.f);
-  for (int lg = 0; lg < nlg; ++lg)
-    for (int mt = 0; mt < n_mt; ++mt)
-      for (int ch = 0; ch < n_ch; ++ch) {
-        float* b = out.data() + ((size_t)(lg * n_mt + mt) * n_ch + ch) * blk;
-        for (int q = 0; q < tc::kKC / 4; ++q)
-          for (int r = 0; r < tc::kRows; ++r)
-            for (int u = 0; u < 4; ++u) {
-              const int row = mt * tc::kRows + r, k = ch * tc::kKC + 4 * q + u;
-              if (row >= R || k >= K) continue;
-              const float a = (float)ops[((size_t)lg * K + k) * RP + row];
-              uint32_t bits;
-              std::memcpy(&bits, &a, 4);
-              bits &= 0xFFFFE000u;
-              float hi;
-              std::memcpy(&hi, &bits, 4);
-              const size_t o = (size_t)q * tc::kRows * 4 + (size_t)r * 4 + u;
-              b[o] = hi;
-              b[blk / 2 + o] = a - hi;
-            }
-      }
-  return out;
+// M->X operator columns of one level from the tabulated waves of the unit
+// multipoles: ops[lg][b][dir * 2 NPM + 2 i + re/im] = W[b][dir][ch0][i]
+// (ch0 = 0 / 8 for the two screening groups); padding rows stay 0.
+__global__ void m2x_columns_kernel(const double2* __restrict__ W, int R2, int NPM, int lev, int rp,
+                                   double* __restrict__ ops) {
+  const int total = 2 * R2 * 6 * NPM;
+  for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
+    const int i = o % NPM, dir = (o / NPM) % 6, b = (o / (6 * NPM)) % R2, g = o / (6 * NPM * R2);
+    const double2 w = W[(((size_t)b * 6 + dir) * kCh + (g ? 8 : 0)) * NPM + i];
+    double* col = ops + ((size_t)(2 * (lev - 1) + g) * R2 + b) * rp + (size_t)dir * 2 * NPM + 2 * i;
+    col[0] = w.x;
+    col[1] = w.y;
+  }
 }
 
-// Tabulates, in FP64, the multipole -> plane-wave operator (m2x_kernel on
-// unit multipoles, one per real component) and the accumulated-wave ->
-// local operator (xl_convert_basis_kernel on unit waves) of every level and
-// screening group, stored k-major ([lg][k][row], rows padded) in the
-// engine's precision.
+// ops[lg][k][row] (rows padded to RP) -> the tensor-core blocks
+// [lg][row tile][k chunk][hi, lo][8 panels][128 rows][4] of op_gemm_tc_kernel;
+// hi = the FP32 value with its 13 low mantissa bits cleared, lo = rest.
+__global__ void pack_tensor_kernel(const double* __restrict__ ops, int nlg, int K, int RP, int R, int n_mt, int n_ch,
+                                   float* __restrict__ out) {
+  constexpr int kBlk = 2 * tc::kHalf / 4;  // floats per [hi, lo] block
+  const long long total = (long long)nlg * n_mt * n_ch * (kBlk / 2);
+  for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+       o += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(o % (kBlk / 2));  // q * 512 + r * 4 + u
+    const long long blk = o / (kBlk / 2);
+    const int ch = (int)(blk % n_ch), mt = (int)((blk / n_ch) % n_mt), lg = (int)(blk / ((long long)n_ch * n_mt));
+    const int q = e / (tc::kRows * 4), r = (e / 4) % tc::kRows, u = e % 4;
+    const int row = mt * tc::kRows + r, k = ch * tc::kKC + 4 * q + u;
+    float a = 0.f;
+    if (row < R && k < K) a = (float)ops[((size_t)lg * K + k) * RP + row];
+    const float h = __uint_as_float(__float_as_uint(a) & 0xFFFFE000u);
+    float* b = out + blk * kBlk;
+    b[e] = h;
+    b[kBlk / 2 + e] = a - h;
+  }
+}
+
+// The dense M->X and waves->local operators of every level, tabulated in
+// FP64 on the device by applying the structured kernels to unit vectors, and
+// left on the device: packed for the tensor cores (FP32 engine) or as they
+// are (FP64 engine).
 static void build_wave_operators(Problem& P, FmmState& S) {
   Ctx* c = P.ctx;
   cudaStream_t st = c->stream;
   const int E = S.E, R2 = 2 * E, NPM = S.np_max, KW = 12 * NPM, nlev = S.nlev, nlg = 2 * nlev;
-  std::vector<double> m2x((size_t)nlg * R2 * S.m2x_rp, 0.0);
+  DevBuf m2x(c, sizeof(double) * (size_t)nlg * R2 * S.m2x_rp);
+  BP_CUDA(cudaMemsetAsync(m2x.get(), 0, m2x.bytes(), st));
   {
     std::vector<double2> hm((size_t)R2 * kCh * E, make_double2(0.0, 0.0));
     for (int b = 0; b < R2; ++b)
@@ -2049,50 +2054,40 @@ static void build_wave_operators(Problem& P, FmmState& S) {
       }
     DevBuf Mb = upload(c, hm);
     DevBuf Wb(c, sizeof(double2) * (size_t)R2 * 6 * kCh * NPM);
-    std::vector<double2> hw((size_t)R2 * 6 * kCh * NPM);
+    std::vector<M2xItem> items((size_t)nlev * R2);
+    for (int lev = 1; lev < nlev; ++lev)
+      for (int b = 0; b < R2; ++b) items[(size_t)lev * R2 + b] = M2xItem{b, lev};
+    DevBuf di = upload(c, items);
     for (int lev = 1; lev < nlev; ++lev) {
-      std::vector<M2xItem> items(R2);
-      for (int b = 0; b < R2; ++b) items[b] = M2xItem{b, lev};
-      DevBuf di = upload(c, items);
       BP_CUDA(cudaMemsetAsync(Wb.get(), 0, Wb.bytes(), st));
       m2x_kernel<double><<<R2 * (kCh / kM2xChannels), kM2xThreads, S.smem_m2x, st>>>(
-          S.tb_d, di.as<M2xItem>(), Mb.as<double2>(), Wb.as<double2>());
+          S.tb_d, di.as<M2xItem>() + (size_t)lev * R2, Mb.as<double2>(), Wb.as<double2>());
       BP_LAUNCH_CHECK();
-      BP_CUDA(cudaMemcpyAsync(hw.data(), Wb.get(), Wb.bytes(), cudaMemcpyDeviceToHost, st));
-      BP_CUDA(cudaStreamSynchronize(st));
-      for (int g = 0; g < 2; ++g) {
-        const int ch = g ? 8 : 0, lg = 2 * (lev - 1) + g;
-        for (int b = 0; b < R2; ++b)
-          for (int dir = 0; dir < 6; ++dir)
-            for (int i = 0; i < NPM; ++i) {
-              const double2 w = hw[(((size_t)b * 6 + dir) * kCh + ch) * NPM + i];
-              double* col = m2x.data() + ((size_t)lg * R2 + b) * S.m2x_rp + (size_t)dir * 2 * NPM + 2 * i;
-              col[0] = w.x;
-              col[1] = w.y;
-            }
-      }
+      m2x_columns_kernel<<<128, 256, 0, st>>>(Wb.as<double2>(), R2, NPM, lev, S.m2x_rp, m2x.as<double>());
+      BP_LAUNCH_CHECK();
     }
+    BP_CUDA(cudaStreamSynchronize(st));  // the host staging vectors go out of scope
   }
-  std::vector<double> xl((size_t)nlg * KW * S.xl_rp, 0.0);
-  {
-    DevBuf Ob(c, sizeof(double) * xl.size());
-    BP_CUDA(cudaMemsetAsync(Ob.get(), 0, Ob.bytes(), st));
-    for (int pl = 0; pl + 1 < nlev; ++pl) {
-      xl_convert_basis_kernel<double><<<2 * KW, kPairLanes, S.smem_xlb, st>>>(S.tb_d, pl, S.xl_rp, Ob.as<double>());
-      BP_LAUNCH_CHECK();
-    }
-    BP_CUDA(cudaMemcpyAsync(xl.data(), Ob.get(), Ob.bytes(), cudaMemcpyDeviceToHost, st));
-    BP_CUDA(cudaStreamSynchronize(st));
+  DevBuf xl(c, sizeof(double) * (size_t)nlg * KW * S.xl_rp);
+  BP_CUDA(cudaMemsetAsync(xl.get(), 0, xl.bytes(), st));
+  for (int pl = 0; pl + 1 < nlev; ++pl) {
+    xl_convert_basis_kernel<double><<<2 * KW, kPairLanes, S.smem_xlb, st>>>(S.tb_d, pl, S.xl_rp, xl.as<double>());
+    BP_LAUNCH_CHECK();
   }
   if (S.tensor) {
-    S.m2x_tc = upload(c, pack_tensor(m2x, nlg, R2, S.m2x_rp, KW, S.m2x_mt, S.m2x_nc));
-    S.xl_tc = upload(c, pack_tensor(xl, nlg, KW, S.xl_rp, R2, S.xl_mt, S.xl_nc));
-  } else if (S.fp64) {
-    S.m2x_ops = upload(c, m2x);
-    S.xl_ops = upload(c, xl);
-  } else {
-    S.m2x_ops = upload(c, std::vector<float>(m2x.begin(), m2x.end()));
-    S.xl_ops = upload(c, std::vector<float>(xl.begin(), xl.end()));
+    auto pack = [&](const DevBuf& ops, int K, int RP, int R, int& n_mt, int& n_ch, DevBuf& out) {
+      n_mt = (R + tc::kRows - 1) / tc::kRows;
+      n_ch = (K + tc::kKC - 1) / tc::kKC;
+      out.alloc(c, sizeof(float) * (size_t)nlg * n_mt * n_ch * (2 * tc::kHalf / 4));
+      pack_tensor_kernel<<<4 * c->sm_count, 256, 0, st>>>(ops.as<double>(), nlg, K, RP, R, n_mt, n_ch,
+                                                          out.as<float>());
+      BP_LAUNCH_CHECK();
+    };
+    pack(m2x, R2, S.m2x_rp, KW, S.m2x_mt, S.m2x_nc, S.m2x_tc);
+    pack(xl, KW, S.xl_rp, R2, S.xl_mt, S.xl_nc, S.xl_tc);
+  } else {  // the FP64 engine (the FP32 engine always takes the tensor cores)
+    S.m2x_ops = std::move(m2x);
+    S.xl_ops = std::move(xl);
   }
   BP_CUDA(cudaStreamSynchronize(st));
 }

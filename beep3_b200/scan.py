@@ -70,11 +70,11 @@ def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it):
         bp.close()
 
 
-def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, tol, max_it):
+def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, tol, max_it, context=None):
     """Poses idx on one engine context: the two meshes stay on the device and
     each pose only moves instance B (a new tree, near field and far-field
     set-up, then the solve)."""
-    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device)
+    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
     out = []
     try:
         ident = np.array([1.0, 0.0, 0.0, 0.0])
@@ -94,17 +94,23 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
 
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
                     nbsize: int = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
-                    max_iterations: int = 100) -> ScanResult:
+                    max_iterations: int = 100, contexts: list | None = None) -> ScanResult:
+    """``contexts``: EngineContexts for the workers (at least ``workers``), kept
+    by the caller across scans so that the meshes and device blocks stay on
+    the device; by default each worker has its own for this scan."""
     t0 = time.perf_counter()
     ident = np.array([1.0, 0.0, 0.0, 0.0])
     ca = mesh_a.centre
     workers = max(1, min(workers, len(poses)))
+    if contexts is not None and len(contexts) < workers:
+        raise ValueError("fewer engine contexts than workers")
     with ThreadPoolExecutor(max_workers=workers + 2) as ex:
         fa = ex.submit(_solve_energy, [(mesh_a, ca, ident)], kappa, precision, nbsize, device, tol, max_iterations)
         fb = ex.submit(_solve_energy, [(mesh_b, mesh_b.centre, ident)], kappa, precision, nbsize, device, tol,
                        max_iterations)
         fw = [ex.submit(_scan_worker, mesh_a, mesh_b, poses, list(range(w, len(poses), workers)), kappa, precision,
-                        nbsize, device, tol, max_iterations) for w in range(workers)]
+                        nbsize, device, tol, max_iterations, contexts[w] if contexts else None)
+              for w in range(workers)]
         e_a, _ = fa.result()
         e_b, _ = fb.result()
         res = sorted(r for f in fw for r in f.result())
