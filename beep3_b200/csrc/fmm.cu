@@ -1794,17 +1794,11 @@ std::vector<RawInteraction> interaction_table() {
 }
 
 template <typename T>
-void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb, DevBuf& buf) {
+void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb, DevBuf& buf, const GlobalTables& G,
+                 const std::vector<LevelTables>& LT) {
   using C = typename C2T<T>::type;
   const int nt = S.nt, E = S.E, nlev = S.nlev;
-  GlobalTables G;
-  G.build(nt);
-  std::vector<LevelTables> LT(2 * nlev);
   const double beta = std::max(P.params.kappa, P.params.beta0);
-  for (int l = 0; l < nlev; ++l) {
-    LT[2 * l].build(nt, beta, l, P.params.cube_edge);
-    LT[2 * l + 1].build(nt, P.params.beta0, l, P.params.cube_edge);
-  }
   S.nl = LT[0].nl;
   int npm = 0;
   for (auto& t : LT) npm = std::max(npm, t.nexptotp);
@@ -1937,6 +1931,36 @@ void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb, DevBuf& buf) {
 // kind, level, screening group and octant, R = 2E reals) and of the L2P
 // preparation (one sparse matrix per leaf level) by applying the structured
 // kernels to unit vectors.
+// CSR of a dense operator stored by columns (D[b][rows]): one warp per row
+// counts its nonzeros, then writes them in column order.
+template <typename T>
+__global__ void csr_count_kernel(const T* __restrict__ D, int nb, int rows, int* __restrict__ counts) {
+  const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  int n = 0;
+  for (int b = lane; b < nb; b += 32) n += D[(size_t)b * rows + r] != T(0);
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if (lane == 0) counts[r] = n;
+}
+template <typename T>
+__global__ void csr_fill_kernel(const T* __restrict__ D, int nb, int rows, const int* __restrict__ rowptr,
+                                int* __restrict__ cols, T* __restrict__ vals) {
+  const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  int pos = rowptr[r];
+  for (int b0 = 0; b0 < nb; b0 += 32) {
+    const int b = b0 + lane;
+    const T v = b < nb ? D[(size_t)b * rows + r] : T(0);
+    const unsigned m = __ballot_sync(0xffffffffu, v != T(0));
+    if (v != T(0)) {
+      const int k = pos + __popc(m & ((1u << lane) - 1u));
+      cols[k] = b;
+      vals[k] = v;
+    }
+    pos += __popc(m);
+  }
+}
+
 template <typename T>
 static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const std::vector<LeafItem>& leaves) {
   using C = typename C2T<T>::type;
@@ -1949,49 +1973,58 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   S.shift_ops.alloc(c, sizeof(T) * (size_t)n_ops * R * ((R + 3) & ~3));
   shift_basis_kernel<T><<<n_ops * R, 64, S.smem_shift, st>>>(tb, nlev, S.shift_ops.as<T>());
   BP_LAUNCH_CHECK();
-  // L2P preparation operator per level that holds leaves
+  // L2P preparation operator per level that holds leaves: tabulated on unit
+  // inputs (dense columns [b][rows]) and compacted to CSR on the device, the
+  // nonzeros of a row in column order
   const int nb = kCh * R, rows = 8 * 2 * EQ;
   std::vector<int> levels_with_leaves(nlev, 0);
   for (const LeafItem& lf : leaves) levels_with_leaves[lf.level] = 1;
   DevBuf Lb(c, sizeof(C) * (size_t)nb * kCh * E);
-  DevBuf Db(c, sizeof(C) * (size_t)nb * 8 * EQ);
   prep_basis_inputs<T><<<nb, 128, 0, st>>>(E, nb, Lb.as<C>());
   BP_LAUNCH_CHECK();
-  std::vector<int> rowptr((size_t)nlev * (rows + 1), 0), cols;
-  std::vector<T> vals;
-  std::vector<T> host((size_t)nb * rows);
+  std::vector<DevBuf> Db(nlev);
+  DevBuf counts(c, sizeof(int) * (size_t)nlev * rows);
+  BP_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), st));
+  std::vector<LeafItem> bi(nb);
+  for (int b = 0; b < nb; ++b) bi[b] = LeafItem{b, 0, 0, 0, b, {0, 0, 0}};
+  std::vector<DevBuf> d_bi(nlev);
+  for (int lev = 0; lev < nlev; ++lev) {
+    if (!levels_with_leaves[lev]) continue;
+    for (int b = 0; b < nb; ++b) bi[b].level = lev;
+    d_bi[lev] = upload(c, bi);
+    Db[lev].alloc(c, sizeof(C) * (size_t)nb * 8 * EQ);
+    l2p_prep_kernel<T><<<nb, 64, S.smem_prep, st>>>(tb, d_bi[lev].as<LeafItem>(), Lb.as<C>(), Db[lev].as<C>());
+    BP_LAUNCH_CHECK();
+    csr_count_kernel<T><<<(rows + 7) / 8, 256, 0, st>>>(Db[lev].as<T>(), nb, rows, counts.as<int>() + (size_t)lev * rows);
+    BP_LAUNCH_CHECK();
+  }
+  std::vector<int> h_counts((size_t)nlev * rows);
+  BP_CUDA(cudaMemcpyAsync(h_counts.data(), counts.get(), counts.bytes(), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  std::vector<int> rowptr((size_t)nlev * (rows + 1), 0);
+  int nnz = 0;
   for (int lev = 0; lev < nlev; ++lev) {
     int* rp = rowptr.data() + (size_t)lev * (rows + 1);
-    if (!levels_with_leaves[lev]) {
-      for (int r = 0; r <= rows; ++r) rp[r] = (int)vals.size();
-      continue;
-    }
-    std::vector<LeafItem> bi(nb);
-    for (int b = 0; b < nb; ++b) bi[b] = LeafItem{b, lev, 0, 0, b, {0, 0, 0}};
-    DevBuf d_bi = upload(c, bi);
-    l2p_prep_kernel<T><<<nb, 64, S.smem_prep, st>>>(tb, d_bi.as<LeafItem>(), Lb.as<C>(), Db.as<C>());
-    BP_LAUNCH_CHECK();
-    BP_CUDA(cudaMemcpyAsync(host.data(), Db.get(), sizeof(T) * host.size(), cudaMemcpyDeviceToHost, st));
-    BP_CUDA(cudaStreamSynchronize(st));
     for (int r = 0; r < rows; ++r) {
-      rp[r] = (int)vals.size();
-      for (int b = 0; b < nb; ++b) {
-        const T v = host[(size_t)b * rows + r];
-        if (v != T(0)) {
-          cols.push_back(b);
-          vals.push_back(v);
-        }
-      }
+      rp[r] = nnz;
+      nnz += h_counts[(size_t)lev * rows + r];
     }
-    rp[rows] = (int)vals.size();
-  }
-  if (vals.empty()) {
-    vals.push_back(0);
-    cols.push_back(0);
+    rp[rows] = nnz;
   }
   S.prep_rowptr = upload(c, rowptr);
-  S.prep_cols = upload(c, cols);
-  S.prep_vals = upload(c, vals);
+  S.prep_cols.alloc(c, sizeof(int) * (size_t)std::max(1, nnz));
+  S.prep_vals.alloc(c, sizeof(T) * (size_t)std::max(1, nnz));
+  if (nnz == 0) {
+    BP_CUDA(cudaMemsetAsync(S.prep_cols.get(), 0, sizeof(int), st));
+    BP_CUDA(cudaMemsetAsync(S.prep_vals.get(), 0, sizeof(T), st));
+  }
+  for (int lev = 0; lev < nlev; ++lev) {
+    if (!levels_with_leaves[lev]) continue;
+    csr_fill_kernel<T><<<(rows + 7) / 8, 256, 0, st>>>(Db[lev].as<T>(), nb, rows,
+                                                       S.prep_rowptr.as<int>() + (size_t)lev * (rows + 1),
+                                                       S.prep_cols.as<int>(), S.prep_vals.as<T>());
+    BP_LAUNCH_CHECK();
+  }
   S.smem_csr = sizeof(T) * (size_t)kCh * R;
   BP_CUDA(cudaStreamSynchronize(st));
 }
@@ -2107,8 +2140,19 @@ void fmm_setup(Problem& P) {
   S->nlev = T.n_levels;
   S->fp64 = P.fp64;
   // FP64 tables always: they tabulate the dense operators of both engines
-  fill_tables<double>(*S, P, S->tb_d, S->fp64 ? S->tables_buf : S->tables_buf_d);
-  if (!S->fp64) fill_tables<float>(*S, P, S->tb_f, S->tables_buf);
+  {
+    // host tables (FP64) once; both engines' device copies are made from them
+    GlobalTables G;
+    G.build(S->nt);
+    std::vector<LevelTables> LT(2 * S->nlev);
+    const double beta = std::max(P.params.kappa, P.params.beta0);
+    for (int l = 0; l < S->nlev; ++l) {
+      LT[2 * l].build(S->nt, beta, l, P.params.cube_edge);
+      LT[2 * l + 1].build(S->nt, P.params.beta0, l, P.params.cube_edge);
+    }
+    fill_tables<double>(*S, P, S->tb_d, S->fp64 ? S->tables_buf : S->tables_buf_d, G, LT);
+    if (!S->fp64) fill_tables<float>(*S, P, S->tb_f, S->tables_buf, G, LT);
+  }
   if (S->np_max > kPairLanes) throw std::invalid_argument("FMM order too large for the plane-wave thread layout");
   const int nn = (int)T.nodes.size();
   const size_t celem = S->fp64 ? sizeof(double2) : sizeof(float2);
