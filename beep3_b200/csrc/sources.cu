@@ -39,20 +39,12 @@ __device__ __forceinline__ double rsqrt_newton(double d2) {
 }
 
 // One thread per point; charges staged through shared memory in tiles.
-// out[2*p] = w * phi * scale, out[2*p+1] = w * (grad phi . n) * scale.
-// kFast (the mixed engine's right-hand side): points and charges are held as
-// two-float (hi + lo) offsets from the block's first point, converted once,
-// so the coordinate differences come out to FP32 rounding without any
-// per-term conversion; the reciprocal distance and the terms are FP32,
-// summed per tile in FP32 and across tiles in FP64 -- about 1e-7 relative
-// per term, in line with the reference, whose right-hand side comes from a
-// 6-figure FMM.
-template <bool kFast>
+// out[2*p] = w * phi * scale, out[2*p+1] = w * (grad phi . n) * scale,
+// exact in FP64.
 __global__ void point_potential_kernel(const double* __restrict__ pts, int npts, int first_pt, int count_pts,
                                        const double* __restrict__ charges, int nc, double scale,
                                        double* __restrict__ out) {
   __shared__ double4 tile[kThreads];
-  __shared__ float4 ftile_hi[kFast ? kThreads : 1], ftile_lo[kFast ? kThreads : 1];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = k < count_pts;
   const int p = first_pt + k;
@@ -63,60 +55,12 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
     z = pts[2 * (size_t)npts + p];
   }
   double phi = 0, gx = 0, gy = 0, gz = 0;
-  // block origin (kFast): the block's first point; two-float offsets
-  const int p0 = first_pt + blockIdx.x * blockDim.x;
-  const double ox = kFast ? pts[p0] : 0.0, oy = kFast ? pts[(size_t)npts + p0] : 0.0,
-               oz = kFast ? pts[2 * (size_t)npts + p0] : 0.0;
-  auto split = [](double v, float& hi, float& lo) {
-    hi = (float)v;
-    lo = (float)(v - (double)hi);
-  };
-  float pxh = 0.f, pxl = 0.f, pyh = 0.f, pyl = 0.f, pzh = 0.f, pzl = 0.f;
-  if (kFast) {
-    split(x - ox, pxh, pxl);
-    split(y - oy, pyh, pyl);
-    split(z - oz, pzh, pzl);
-  }
   for (int base = 0; base < nc; base += kThreads) {
     const int c = base + threadIdx.x;
-    if (c < nc) {
-      const double cx = charges[4 * c], cy = charges[4 * c + 1], cz = charges[4 * c + 2], cq = charges[4 * c + 3];
-      if (kFast) {
-        float4 h, l;
-        split(cx - ox, h.x, l.x);
-        split(cy - oy, h.y, l.y);
-        split(cz - oz, h.z, l.z);
-        h.w = (float)cq;
-        l.w = 0.f;
-        ftile_hi[threadIdx.x] = h;
-        ftile_lo[threadIdx.x] = l;
-      } else {
-        tile[threadIdx.x] = make_double4(cx, cy, cz, cq);
-      }
-    }
+    if (c < nc) tile[threadIdx.x] = make_double4(charges[4 * c], charges[4 * c + 1], charges[4 * c + 2], charges[4 * c + 3]);
     __syncthreads();
     const int lim = min(kThreads, nc - base);
-    if (active && kFast) {
-      float fphi = 0.f, fgx = 0.f, fgy = 0.f, fgz = 0.f;
-      for (int t = 0; t < lim; ++t) {
-        const float4 h = ftile_hi[t], l = ftile_lo[t];
-        const float dx = (pxh - h.x) + (pxl - l.x), dy = (pyh - h.y) + (pyl - l.y), dz = (pzh - h.z) + (pzl - l.z);
-        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        if (d2 > 2.220446049250313e-16f) {
-          const float id = rsqrtf(d2);
-          const float pt = h.w * id;
-          const float ft = -pt * id * id;
-          fphi += pt;
-          fgx = fmaf(ft, dx, fgx);
-          fgy = fmaf(ft, dy, fgy);
-          fgz = fmaf(ft, dz, fgz);
-        }
-      }
-      phi += fphi;
-      gx += fgx;
-      gy += fgy;
-      gz += fgz;
-    } else if (active) {
+    if (active)
       for (int t = 0; t < lim; ++t) {
         const double4 ch = tile[t];
         const double dx = x - ch.x, dy = y - ch.y, dz = z - ch.z;
@@ -131,7 +75,6 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
           gz += ft * dz;
         }
       }
-    }
     __syncthreads();
   }
   if (active) {
@@ -139,6 +82,93 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
     const double nx = pts[3 * (size_t)npts + p], ny = pts[4 * (size_t)npts + p], nz = pts[5 * (size_t)npts + p];
     out[2 * k] = w * phi * scale;
     out[2 * k + 1] = w * (gx * nx + gy * ny + gz * nz) * scale;
+  }
+}
+
+// The mixed engine's right-hand side terms: the same sums with FP32 terms.
+// Points and charges are held as two-float (hi + lo) offsets from the
+// block's first point, converted once, so the coordinate differences come
+// out to FP32 rounding without any per-term conversion; the reciprocal
+// distance and the terms are FP32, summed per tile in FP32 and across tiles
+// in FP64 -- about 1e-7 relative per term, in line with the reference, whose
+// right-hand side comes from a 6-figure FMM.  Each thread takes two points
+// (kPtsPerThread), so every charge read from shared memory serves both, and
+// a coincident charge and point give a zero term by a select, not a branch.
+constexpr int kPtsPerThread = 2;
+__global__ void __launch_bounds__(kThreads) point_potential_fast_kernel(const double* __restrict__ pts, int npts,
+                                                                        const double* __restrict__ charges, int nc,
+                                                                        double scale, double* __restrict__ out) {
+  __shared__ float4 th[kThreads], tl[kThreads];
+  constexpr int P = kPtsPerThread;
+  const int p0 = blockIdx.x * (P * kThreads);  // the block's first point: origin of the offsets
+  const double ox = pts[min(p0, npts - 1)], oy = pts[(size_t)npts + min(p0, npts - 1)],
+               oz = pts[2 * (size_t)npts + min(p0, npts - 1)];
+  auto split = [](double v, float& hi, float& lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+  };
+  float xh[P], xl[P], yh[P], yl[P], zh[P], zl[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const int p = min(p0 + j * kThreads + (int)threadIdx.x, npts - 1);
+    split(pts[p] - ox, xh[j], xl[j]);
+    split(pts[(size_t)npts + p] - oy, yh[j], yl[j]);
+    split(pts[2 * (size_t)npts + p] - oz, zh[j], zl[j]);
+  }
+  double phi[P], gx[P], gy[P], gz[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) phi[j] = gx[j] = gy[j] = gz[j] = 0.0;
+  for (int base = 0; base < nc; base += kThreads) {
+    const int c = base + threadIdx.x;
+    if (c < nc) {
+      float4 h, l;
+      split(charges[4 * c] - ox, h.x, l.x);
+      split(charges[4 * c + 1] - oy, h.y, l.y);
+      split(charges[4 * c + 2] - oz, h.z, l.z);
+      h.w = (float)charges[4 * c + 3];
+      l.w = 0.f;
+      th[threadIdx.x] = h;
+      tl[threadIdx.x] = l;
+    }
+    __syncthreads();
+    const int lim = min(kThreads, nc - base);
+    float fphi[P], fgx[P], fgy[P], fgz[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) fphi[j] = fgx[j] = fgy[j] = fgz[j] = 0.f;
+#pragma unroll 4
+    for (int t = 0; t < lim; ++t) {
+      const float4 h = th[t], l = tl[t];
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const float dx = (xh[j] - h.x) + (xl[j] - l.x), dy = (yh[j] - h.y) + (yl[j] - l.y),
+                    dz = (zh[j] - h.z) + (zl[j] - l.z);
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float id = d2 > 2.220446049250313e-16f ? rsqrtf(d2) : 0.f;
+        const float pt = h.w * id;
+        const float ft = -pt * id * id;
+        fphi[j] += pt;
+        fgx[j] = fmaf(ft, dx, fgx[j]);
+        fgy[j] = fmaf(ft, dy, fgy[j]);
+        fgz[j] = fmaf(ft, dz, fgz[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      phi[j] += fphi[j];
+      gx[j] += fgx[j];
+      gy[j] += fgy[j];
+      gz[j] += fgz[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const int p = p0 + j * kThreads + (int)threadIdx.x;
+    if (p >= npts) continue;
+    const double w = pts[6 * (size_t)npts + p];
+    const double nx = pts[3 * (size_t)npts + p], ny = pts[4 * (size_t)npts + p], nz = pts[5 * (size_t)npts + p];
+    out[2 * (size_t)p] = w * phi[j] * scale;
+    out[2 * (size_t)p + 1] = w * (gx[j] * nx + gy[j] * ny + gz[j] * nz) * scale;
   }
 }
 
@@ -167,11 +197,12 @@ void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps
   if (vals.bytes() < sizeof(double) * 2 * (size_t)nq) vals.alloc(ctx, sizeof(double) * 2 * (size_t)nq);
   const double scale = kOneOver4Pi / eps_solvent;
   if (P.fp64)
-    point_potential_kernel<false><<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+    point_potential_kernel<<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
         P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
   else
-    point_potential_kernel<true><<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
-        P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
+    point_potential_fast_kernel<<<(nq + kPtsPerThread * kThreads - 1) / (kPtsPerThread * kThreads), kThreads, 0,
+                                  ctx->stream>>>(P.d_qual.as<double>(), nq, charges_dev, n_charges, scale,
+                                                 vals.as<double>());
   BP_LAUNCH_CHECK();
   sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
       P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
@@ -186,7 +217,7 @@ void energy_coefficients_device(Problem& P, int first, int count, const double* 
   const int p0 = P.h_gal_off[first], p1 = P.h_gal_off[first + count];
   DevBuf vals(ctx, sizeof(double) * 2 * (size_t)std::max(1, p1 - p0));
   if (p1 > p0) {
-    point_potential_kernel<false><<<(p1 - p0 + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
+    point_potential_kernel<<<(p1 - p0 + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
         P.d_gal.as<double>(), ng, p0, p1 - p0, charges_dev, n_charges, kOneOver4Pi, vals.as<double>());
     BP_LAUNCH_CHECK();
   }
@@ -261,7 +292,7 @@ extern "C" BP_API int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_
     double* scratch = noalloc_scratch_for_current_device();
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     const double scale = kOneOver4Pi / eps_solvent;
-    point_potential_kernel<false><<<(n_qual_points + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+    point_potential_kernel<<<(n_qual_points + kThreads - 1) / kThreads, kThreads, 0, st>>>(
         qual_points_soa_dev, n_qual_points, 0, n_qual_points, charges_xyzq_dev, n_charges, scale, scratch);
     BP_LAUNCH_CHECK();
     sum_points_kernel<<<(n_patches + kThreads - 1) / kThreads, kThreads, 0, st>>>(
