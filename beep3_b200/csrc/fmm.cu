@@ -603,7 +603,7 @@ struct XlEntry {
 };
 constexpr int kCombos = 686;
 constexpr int kXlChannels = 4;                    // channels per translate block (one screening group)
-constexpr int kXlUnroll = 8;
+constexpr int kXlUnroll = 2;
 
 constexpr int kXlGroups = 7;                     // lane groups of a translate block
 constexpr int kXlDirThreads = kXlGroups * kPairLanes;
@@ -627,7 +627,7 @@ __global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __
                                                                         typename C2T<T>::type* __restrict__ ACC) {
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
-  constexpr int U = sizeof(T) == 4 ? kXlUnroll / 2 : kXlUnroll / 4;  // entries in flight per thread
+  constexpr int U = kXlUnroll;  // entries in flight per thread (measured: 2 beats 4, 6 and 8 spill)
   __shared__ C part[2][CB][kPairLanes];  // second halves of up and down
   const int NPM = tb.np_max;
   const int t = blockIdx.x / (kCh / CB);
