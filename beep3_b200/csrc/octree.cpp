@@ -31,6 +31,7 @@
 #include <deque>
 #include <map>
 #include <stdexcept>
+#include <unordered_map>
 
 namespace bp {
 
@@ -67,6 +68,8 @@ class RefTree {
     nodes_.push_back(root);
     levels_.emplace_back();
     levels_[0][0] = 0;
+    index_.emplace_back();
+    index_[0][0] = 0;
     for (int i = 0; i < n; ++i) add(i);
   }
 
@@ -135,6 +138,7 @@ class RefTree {
       for (uint64_t k : empties) {
         nodes_[levels_[level][k]].removed = true;
         levels_[level].erase(k);
+        index_[level].erase(k);
       }
     }
   }
@@ -185,8 +189,8 @@ class RefTree {
         long x = (long)tn.ix + dx, y = (long)tn.iy + dy, z = (long)tn.iz + dz;
         tn.neighbours[nb] = -1;
         if (x < 0 || y < 0 || z < 0 || x >= (long)E || y >= (long)E || z >= (long)E) continue;
-        auto it = levels_[tn.level].find(key((uint32_t)x, (uint32_t)y, (uint32_t)z, tn.level));
-        if (it != levels_[tn.level].end()) tn.neighbours[nb] = remap[it->second];
+        auto it = index_[tn.level].find(key((uint32_t)x, (uint32_t)y, (uint32_t)z, tn.level));
+        if (it != index_[tn.level].end()) tn.neighbours[nb] = remap[it->second];
       }
     }
     // FMM slots (bottom-up, map order)
@@ -206,7 +210,9 @@ class RefTree {
   int nbsize_;
   double edge_;
   std::vector<Node> nodes_;
-  std::vector<std::map<uint64_t, int>> levels_;
+  std::vector<std::map<uint64_t, int>> levels_;  // ordered: the node order of a level
+  std::vector<std::unordered_map<uint64_t, int>> index_;  // the same nodes, for lookups
+  std::vector<uint8_t> cid_;  // scratch: child of each item of the node being split
 
   static int child_id(const Node& nd) {
     return 1 + (nd.ix & 1) + 2 * (nd.iy & 1) + 4 * (nd.iz & 1);
@@ -246,21 +252,25 @@ class RefTree {
     if (level >= (int)levels_.size()) return -1;
     long E = 1l << level;
     if (x < 0 || y < 0 || z < 0 || x >= E || y >= E || z >= E) return -1;
-    auto it = levels_[level].find(key((uint32_t)x, (uint32_t)y, (uint32_t)z, level));
-    return it == levels_[level].end() ? -1 : it->second;
+    auto it = index_[level].find(key((uint32_t)x, (uint32_t)y, (uint32_t)z, level));
+    return it == index_[level].end() ? -1 : it->second;
   }
 
   void subdivide(int id) {
     if (nodes_[id].has_children) return;
     nodes_[id].has_children = true;
     int new_level = nodes_[id].level + 1;
-    while ((int)levels_.size() <= new_level) levels_.emplace_back();
-    for (int cid = 1; cid <= 8; ++cid) {
-      const Node& par = nodes_[id];
-      Node ch;
+    while ((int)levels_.size() <= new_level) {
+      levels_.emplace_back();
+      index_.emplace_back();
+    }
+    const int first = (int)nodes_.size();
+    nodes_.resize(first + 8);
+    const Node& par = nodes_[id];
+    for (int o = 0; o < 8; ++o) {
+      Node& ch = nodes_[first + o];
       ch.level = new_level;
       ch.edge = par.edge / 2.0;
-      int o = cid - 1;
       ch.ix = par.ix * 2 + (o & 1);
       ch.iy = par.iy * 2 + ((o >> 1) & 1);
       ch.iz = par.iz * 2 + (o >> 2);
@@ -268,12 +278,29 @@ class RefTree {
       ch.c[1] = par.c[1] + (((o >> 1) & 1) ? ch.edge / 2.0 : -ch.edge / 2.0);
       ch.c[2] = par.c[2] + ((o >> 2) ? ch.edge / 2.0 : -ch.edge / 2.0);
       ch.parent = id;
-      for (int item : par.contents)
-        if (child_for(par, item) == cid) ch.contents.push_back(item);
-      int nid = (int)nodes_.size();
-      nodes_.push_back(std::move(ch));
-      nodes_[id].children[cid - 1] = nid;
-      levels_[new_level][key(nodes_[nid].ix, nodes_[nid].iy, nodes_[nid].iz, new_level)] = nid;
+    }
+    // children take the parent's items in its insertion order
+    const size_t m = par.contents.size();
+    cid_.resize(m);
+    size_t count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t i = 0; i < m; ++i) {
+      const double* p = pts_ + 3 * (size_t)par.contents[i];
+      const int o = (p[0] > par.c[0]) + 2 * (p[1] > par.c[1]) + 4 * (p[2] > par.c[2]);
+      cid_[i] = (uint8_t)o;
+      ++count[o];
+    }
+    int* out[8];
+    for (int o = 0; o < 8; ++o) {
+      nodes_[first + o].contents.resize(count[o]);
+      out[o] = nodes_[first + o].contents.data();
+    }
+    for (size_t i = 0; i < m; ++i) *out[cid_[i]]++ = par.contents[i];
+    for (int o = 0; o < 8; ++o) {
+      nodes_[id].children[o] = first + o;
+      const Node& ch = nodes_[first + o];
+      const uint64_t k = key(ch.ix, ch.iy, ch.iz, new_level);
+      levels_[new_level].emplace(k, first + o);
+      index_[new_level].emplace(k, first + o);
     }
   }
 
