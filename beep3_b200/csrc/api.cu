@@ -100,9 +100,13 @@ void finish_problem(Ctx* c, Problem& P) {
   P.d_y.alloc(c, sizeof(double) * 2 * (size_t)P.n);
   nf_build_structure(P);
   nf_assemble(P);
-  if (fmm_active(P)) fmm_setup(P);
+  if (fmm_active(P)) fmm_setup(P);  // host work overlaps the assembly kernels
+  nf_join(P);
   matvec_setup(P);
   BP_CUDA(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  BP_CUDA(cudaEventElapsedTime(&ms, P.asm_t0, P.asm_t1));
+  P.assemble_ms = ms;
 }
 
 // p -> R (p - c) + o and n -> R n of `count` points of a 7-array SoA list

@@ -284,7 +284,19 @@ struct Problem {
   DevBuf scratch_charges, scratch_vals, scratch_b;
   int krylov_m = 0;
   double tree_ms = 0, assemble_ms = 0;
+  // the near-field assembly runs on a stream of its own while the far field
+  // is set up; its inputs stay allocated until it is joined (nf_join)
+  cudaStream_t asm_stream = nullptr;
+  cudaEvent_t asm_in = nullptr, asm_t0 = nullptr, asm_t1 = nullptr;
+  DevBuf asm_gc, asm_items;
   ~Problem() {
+    if (asm_stream) {
+      cudaStreamSynchronize(asm_stream);
+      cudaStreamDestroy(asm_stream);
+    }
+    if (asm_in) cudaEventDestroy(asm_in);
+    if (asm_t0) cudaEventDestroy(asm_t0);
+    if (asm_t1) cudaEventDestroy(asm_t1);
     if (graph) cudaGraphExecDestroy(graph);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
@@ -339,7 +351,8 @@ struct StageTimes {
 
 // nearfield.cu
 void nf_build_structure(Problem& P);
-void nf_assemble(Problem& P);
+void nf_assemble(Problem& P);  // launches the assembly on P.asm_stream
+void nf_join(Problem& P);      // orders the context's stream after it
 // y = near field (incl. singular diagonal) of x, plus yfar if not null;
 // returns the number of kernel launches (0 when the problem has no near-field
 // items, in which case y is not written)

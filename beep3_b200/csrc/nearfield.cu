@@ -28,7 +28,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <stdexcept>
 
@@ -164,10 +163,25 @@ __global__ void singular_kernel(int n, const int32_t* __restrict__ off, const do
   }
 }
 
+// One staged qualocation point: position, normal and weight, stored 8 wide
+// so that a point is two 16-byte (FP32) or four 16-byte (FP64) shared loads.
+__device__ __forceinline__ void load_qpoint(const float* s, int q, float (&v)[7]) {
+  const float4 a = reinterpret_cast<const float4*>(s)[2 * q];
+  const float4 b = reinterpret_cast<const float4*>(s)[2 * q + 1];
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z;
+}
+__device__ __forceinline__ void load_qpoint(const double* s, int q, double (&v)[7]) {
+  const double2* p = reinterpret_cast<const double2*>(s) + 4 * q;
+  const double2 a = p[0], b = p[1], c = p[2], d = p[3];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x;
+}
+
 // Coefficient assembly.  A work item is <= kAsmRows rows of one leaf; their
 // qualocation points are staged in shared memory; each thread walks the
 // leaf's columns and produces the (A,B,C,D) of every staged row for its
-// column, so one row's stores are contiguous across the block.
+// column, so one row's stores are contiguous across the block.  A column
+// with one quadrature point (quadrature rule 0) keeps it in registers for
+// all of its rows x qualocation points.
 template <typename T>
 __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
     const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
@@ -175,17 +189,15 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
     const int32_t* __restrict__ qoff, const T* __restrict__ qual, int nq, const int32_t* __restrict__ poff,
     const T* __restrict__ quad, int np, const double* __restrict__ eps, T kappa, const double* __restrict__ diag,
     T* __restrict__ coef) {
-  extern __shared__ unsigned char smem_raw[];
-  T* sq = reinterpret_cast<T*>(smem_raw);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sq = reinterpret_cast<T*>(smem_raw);  // [qual_total][8]
   __shared__ int s_start[kAsmRows + 1];
   __shared__ int s_row[kAsmRows];
   const NfItem it = items[blockIdx.x];
   const int64_t r0 = row_off[it.leaf] + it.row_begin;
   const int64_t c0 = col_off[it.leaf];
   const int ncols = (int)(col_off[it.leaf + 1] - c0);
-  const int64_t nrows_leaf = row_off[it.leaf + 1] - row_off[it.leaf];
   const int64_t block = coef_off[it.leaf];
-  const int tq = it.qual_total;
   if (threadIdx.x == 0) {
     int acc = 0;
     for (int r = 0; r < it.row_count; ++r) {
@@ -202,7 +214,9 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
     const int base = qoff[i];
     const int cnt = s_start[r + 1] - s_start[r];
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      for (int f = 0; f < 7; ++f) sq[f * tq + s_start[r] + k] = qual[(size_t)f * nq + base + k];
+      T* dst = sq + 8 * (s_start[r] + k);
+      for (int f = 0; f < 7; ++f) dst[f] = qual[(size_t)f * nq + base + k];
+      dst[7] = T(0);
     }
   }
   __syncthreads();
@@ -213,6 +227,10 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
     const int j = cols[c0 + cc];
     const T ie = T(1.0 / eps[j]);
     const int ps = poff[j], pe = poff[j + 1];
+    const bool one_point = pe - ps == 1;
+    T p1[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (one_point)
+      for (int f = 0; f < 7; ++f) p1[f] = quad[(size_t)f * np + ps];
     for (int r = 0; r < it.row_count; ++r) {
       const int i = s_row[r];
       const int64_t o = block + (int64_t)(it.row_begin + r) * ncols + cc;
@@ -227,20 +245,34 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
       }
       T A = 0, B = 0, C = 0, D = 0;
       const int qs = s_start[r], qe = s_start[r + 1];
-      for (int q = qs; q < qe; ++q) {
-        const T qx = sq[q], qy = sq[tq + q], qz = sq[2 * tq + q];
-        const T qnx = sq[3 * tq + q], qny = sq[4 * tq + q], qnz = sq[5 * tq + q];
-        T a = 0, b = 0, c = 0, d = 0;
-        for (int p = ps; p < pe; ++p) {
-          pair_term<T>(qx, qy, qz, qnx, qny, qnz, quad[p], quad[(size_t)np + p], quad[2 * (size_t)np + p],
-                       quad[3 * (size_t)np + p], quad[4 * (size_t)np + p], quad[5 * (size_t)np + p],
-                       quad[6 * (size_t)np + p], kappa, ie, with_d, a, b, c, d);
+      if (one_point) {
+#pragma unroll 4
+        for (int q = qs; q < qe; ++q) {
+          T u[7];
+          load_qpoint(sq, q, u);
+          T a = 0, b = 0, c = 0, d = 0;
+          pair_term<T>(u[0], u[1], u[2], u[3], u[4], u[5], p1[0], p1[1], p1[2], p1[3], p1[4], p1[5], p1[6], kappa,
+                       ie, with_d, a, b, c, d);
+          A += a * u[6];
+          B += b * u[6];
+          C += c * u[6];
+          D += d * u[6];
         }
-        const T wq = sq[6 * tq + q];
-        A += a * wq;
-        B += b * wq;
-        C += c * wq;
-        D += d * wq;
+      } else {
+        for (int q = qs; q < qe; ++q) {
+          T u[7];
+          load_qpoint(sq, q, u);
+          T a = 0, b = 0, c = 0, d = 0;
+          for (int p = ps; p < pe; ++p) {
+            pair_term<T>(u[0], u[1], u[2], u[3], u[4], u[5], quad[p], quad[(size_t)np + p],
+                         quad[2 * (size_t)np + p], quad[3 * (size_t)np + p], quad[4 * (size_t)np + p],
+                         quad[5 * (size_t)np + p], quad[6 * (size_t)np + p], kappa, ie, with_d, a, b, c, d);
+          }
+          A += a * u[6];
+          B += b * u[6];
+          C += c * u[6];
+          D += d * u[6];
+        }
       }
       v.x = A;
       v.y = B;
@@ -249,7 +281,6 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
       out[o] = v;
     }
   }
-  (void)nrows_leaf;
 }
 
 // y_f[i] = sum_j B_ij f_j - A_ij h_j ; y_h[i] = sum_j D_ij f_j - C_ij h_j
@@ -334,10 +365,6 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
   }
 }
 
-double ms_since(std::chrono::steady_clock::time_point t0) {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-}
-
 }  // namespace
 
 void nf_build_structure(Problem& P) {
@@ -411,42 +438,53 @@ static std::vector<NfItem> make_items(const Problem& P, int chunk) {
 }
 
 void nf_assemble(Problem& P) {
-  auto t0 = std::chrono::steady_clock::now();
   Ctx* ctx = P.ctx;
   NearField& nf = P.nf;
-  // geometric correction per patch
-  DevBuf d_gc = upload(ctx, P.h_gc);
-  {
-    P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
-    const int ng = P.n_gal_pts;
-    const int threads = 256;
-    const int blocks = (P.n * 32 + threads - 1) / threads;
-    singular_kernel<<<blocks, threads, 0, ctx->stream>>>(P.n, P.d_gal_off.as<int32_t>(), P.d_gal.as<double>(), ng,
-                                                        P.d_eps.as<double>(), d_gc.as<double>(), P.params.kappa,
-                                                        P.d_diag.as<double>());
-    BP_LAUNCH_CHECK();
+  if (!P.asm_stream) {
+    BP_CUDA(cudaStreamCreateWithFlags(&P.asm_stream, cudaStreamNonBlocking));
+    BP_CUDA(cudaEventCreateWithFlags(&P.asm_in, cudaEventDisableTiming));
+    BP_CUDA(cudaEventCreate(&P.asm_t0));
+    BP_CUDA(cudaEventCreate(&P.asm_t1));
   }
   std::vector<NfItem> asm_items = make_items(P, kAsmRows);
   int max_tq = 0;
   for (auto& it : asm_items) max_tq = std::max(max_tq, it.qual_total);
-  DevBuf d_asm_items = upload(ctx, asm_items);
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
-  nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
   const int nq = P.n_qual_pts;
   const int np = P.n_quad_pts;
-  const size_t smem = elem * 7 * (size_t)max_tq;
+  const size_t smem = elem * 8 * (size_t)max_tq;
   if (smem > 200 * 1024) throw std::invalid_argument("too many qualocation points per patch");
+  // inputs and outputs are placed on the context's stream; the kernels run
+  // on the assembly stream once they are
+  P.asm_gc = upload(ctx, P.h_gc);  // geometric correction per patch
+  P.asm_items = upload(ctx, asm_items);
+  P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
+  nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
+  BP_CUDA(cudaEventRecord(P.asm_in, ctx->stream));
+  const cudaStream_t st = P.asm_stream;
+  BP_CUDA(cudaStreamWaitEvent(st, P.asm_in, 0));
+  BP_CUDA(cudaEventRecord(P.asm_t0, st));
+  {
+    const int ng = P.n_gal_pts;
+    const int threads = 256;
+    const int blocks = (P.n * 32 + threads - 1) / threads;
+    singular_kernel<<<blocks, threads, 0, st>>>(P.n, P.d_gal_off.as<int32_t>(), P.d_gal.as<double>(), ng,
+                                               P.d_eps.as<double>(), P.asm_gc.as<double>(), P.params.kappa,
+                                               P.d_diag.as<double>());
+    BP_LAUNCH_CHECK();
+  }
+  const DevBuf& d_asm_items = P.asm_items;
   if (!asm_items.empty()) {
     if (P.fp64) {
       ensure_dynamic_smem((const void*)assemble_kernel<double>, smem);
-      assemble_kernel<double><<<(int)asm_items.size(), kAsmThreads, smem, ctx->stream>>>(
+      assemble_kernel<double><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
           d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual.as<double>(), nq,
           P.d_quad_off.as<int32_t>(), P.d_quad.as<double>(), np, P.d_eps.as<double>(), P.params.kappa,
           P.d_diag.as<double>(), nf.coef.as<double>());
     } else {
       ensure_dynamic_smem((const void*)assemble_kernel<float>, smem);
-      assemble_kernel<float><<<(int)asm_items.size(), kAsmThreads, smem, ctx->stream>>>(
+      assemble_kernel<float><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
           d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(), nq,
           P.d_quad_off.as<int32_t>(), P.d_quad_f.as<float>(), np, P.d_eps.as<double>(), (float)P.params.kappa,
@@ -454,6 +492,7 @@ void nf_assemble(Problem& P) {
     }
     BP_LAUNCH_CHECK();
   }
+  BP_CUDA(cudaEventRecord(P.asm_t1, st));
   // apply work items; the apply kernel's shared memory holds the x values of
   // a leaf's columns
   const size_t apply_smem = 2 * elem * (size_t)nf.max_cols;
@@ -472,8 +511,14 @@ void nf_assemble(Problem& P) {
   }
   nf.items = upload(ctx, nf.h_items);
   nf.n_items = (int)nf.h_items.size();
-  BP_CUDA(cudaStreamSynchronize(ctx->stream));
-  P.assemble_ms = ms_since(t0);
+}
+
+void nf_join(Problem& P) {
+  if (!P.asm_stream) return;
+  BP_CUDA(cudaStreamWaitEvent(P.ctx->stream, P.asm_t1, 0));
+  // later users of these blocks run on the context's stream, after the join
+  P.asm_gc.reset();
+  P.asm_items.reset();
 }
 
 int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_dev, cudaStream_t stream) {

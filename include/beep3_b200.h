@@ -132,7 +132,7 @@ typedef struct {
   int64_t fmm_active;        /* 1 when the tree is deep enough for the far field */
   uint64_t device_bytes;
   double tree_ms;
-  double assemble_ms;        /* singular + near-field coefficient assembly */
+  double assemble_ms;        /* device time of the singular + near-field assembly kernels */
 } bp_problem_info;
 
 /* Builds the adaptive octree, the singular self-patch integrals and the
