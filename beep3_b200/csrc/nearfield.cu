@@ -108,6 +108,53 @@ __device__ __forceinline__ void pair_term(T qx, T qy, T qz, T qnx, T qny, T qnz,
   }
 }
 
+// The same four kernels without the quadrature weight, rearranged to share
+// factors: with g = 1/(4 pi r), e = exp(-kappa r) and t = 1/r^2,
+//   G - u                     = g (1 - e)
+//   grad G . d / |d|^2 terms  : g3 = g t,  u3 = e g (t + kappa/r)
+//   Hessian terms             : gr5 = g3 t, pu = e g t (3 kappa/r + kappa^2 + 3 t)
+// (the expressions of pair_term, factored).  `ek` is the exponent scale:
+// -kappa log2(e) for FP32, where e = 2^(ek r) (exp2f), and -kappa for FP64.
+__device__ __forceinline__ float exp_scaled(float ek, float r) { return exp2f(ek * r); }
+__device__ __forceinline__ double exp_scaled(double ek, double r) { return exp(ek * r); }
+template <typename T>
+__device__ __forceinline__ T exp_scale(T kappa);
+template <>
+__device__ __forceinline__ float exp_scale<float>(float kappa) {
+  return -kappa * 1.4426950408889634f;  // log2(e)
+}
+template <>
+__device__ __forceinline__ double exp_scale<double>(double kappa) {
+  return -kappa;
+}
+
+template <typename T>
+__device__ __forceinline__ void pair_term_unit(T qx, T qy, T qz, T qnx, T qny, T qnz, T px, T py, T pz, T pnx,
+                                               T pny, T pnz, T kappa, T ek, T ie, bool with_d, T& a, T& b, T& c,
+                                               T& d) {
+  const T dx = px - qx, dy = py - qy, dz = pz - qz;
+  const T r2 = dx * dx + dy * dy + dz * dz;
+  if (fabs(r2) < T(1e-9)) return;
+  const T ir = fast_rsqrt(r2);
+  const T r = r2 * ir;
+  const T e = exp_scaled(ek, r);
+  const T g = T(kOneOver4Pi) * ir;
+  const T eg = e * g;
+  const T t = ir * ir;
+  const T g3 = g * t;
+  const T u3 = eg * (t + kappa * ir);
+  const T ndx = pnx * dx + pny * dy + pnz * dz;   // n_p . dx
+  const T n0dx = qnx * dx + qny * dy + qnz * dz;  // n_q . dx
+  a += g - eg;
+  b += (u3 - ie * g3) * ndx;
+  c += (g3 - ie * u3) * n0dx;
+  if (with_d) {
+    const T pu = eg * t * (kappa * (T(3) * ir + kappa) + T(3) * t);
+    const T nn0 = pnx * qnx + pny * qny + pnz * qnz;
+    d -= ndx * n0dx * (T(3) * g3 * t - pu) - nn0 * (g3 - u3);
+  }
+}
+
 // Singular self-patch integrals in FP64, one warp per patch
 // (src/bem/bem_kernels.h:18-132): all ordered pairs of distinct galerkin
 // points of the patch, normalised by the sum of the outer weights; then the
@@ -221,6 +268,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
   }
   __syncthreads();
   const bool with_d = kappa != T(0);
+  const T ek = exp_scale<T>(kappa);
   using V4 = typename Vec4<T>::type;
   V4* out = reinterpret_cast<V4*>(coef);
   for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) {
@@ -245,19 +293,23 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
       }
       T A = 0, B = 0, C = 0, D = 0;
       const int qs = s_start[r], qe = s_start[r + 1];
-      if (one_point) {
+      if (one_point) {  // the column's weight multiplies the row's sums
 #pragma unroll 4
         for (int q = qs; q < qe; ++q) {
           T u[7];
           load_qpoint(sq, q, u);
           T a = 0, b = 0, c = 0, d = 0;
-          pair_term<T>(u[0], u[1], u[2], u[3], u[4], u[5], p1[0], p1[1], p1[2], p1[3], p1[4], p1[5], p1[6], kappa,
-                       ie, with_d, a, b, c, d);
+          pair_term_unit<T>(u[0], u[1], u[2], u[3], u[4], u[5], p1[0], p1[1], p1[2], p1[3], p1[4], p1[5], kappa, ek,
+                            ie, with_d, a, b, c, d);
           A += a * u[6];
           B += b * u[6];
           C += c * u[6];
           D += d * u[6];
         }
+        A *= p1[6];
+        B *= p1[6];
+        C *= p1[6];
+        D *= p1[6];
       } else {
         for (int q = qs; q < qe; ++q) {
           T u[7];

@@ -58,8 +58,8 @@ def random_poses(n: int, seed: int, rmin: float = 45.0, rmax: float = 80.0) -> l
     return out
 
 
-def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it):
-    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device)
+def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it, context=None):
+    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
     try:
         for mesh, off, q in instances:
             bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
@@ -70,13 +70,20 @@ def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it):
         bp.close()
 
 
-def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, tol, max_it, context=None):
+def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, tol, max_it, context=None,
+                 isolated=()):
     """Poses idx on one engine context: the two meshes stay on the device and
     each pose only moves instance B (a new tree, near field and far-field
-    set-up, then the solve)."""
+    set-up, then the solve).  The single-molecule problems in ``isolated``
+    are solved first, on the same context.  Returns (pose results, their
+    energies)."""
     bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
     out = []
     try:
+        iso = [_solve_energy(inst, kappa, precision, nbsize, device, tol, max_it, context=bp.engine)[0]
+               for inst in isolated]
+        if not idx:
+            return out, iso
         ident = np.array([1.0, 0.0, 0.0, 0.0])
         ca = mesh_a.centre
         bp.insert_mesh_instance(mesh_a, offset=ca, rotation=ident, eps_protein=2.0)
@@ -89,7 +96,7 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
             out.append((k, e, info.num_iterations))
     finally:
         bp.close()
-    return out
+    return out, iso
 
 
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
@@ -104,16 +111,19 @@ def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float 
     workers = max(1, min(workers, len(poses)))
     if contexts is not None and len(contexts) < workers:
         raise ValueError("fewer engine contexts than workers")
-    with ThreadPoolExecutor(max_workers=workers + 2) as ex:
-        fa = ex.submit(_solve_energy, [(mesh_a, ca, ident)], kappa, precision, nbsize, device, tol, max_iterations)
-        fb = ex.submit(_solve_energy, [(mesh_b, mesh_b.centre, ident)], kappa, precision, nbsize, device, tol,
-                       max_iterations)
+    # the isolated molecules are solved by workers 0 and 1 (0 alone when it is
+    # the only one) on their contexts, before their poses
+    isolated = [[] for _ in range(workers)]
+    isolated[0].append([(mesh_a, ca, ident)])
+    isolated[1 % workers].append([(mesh_b, mesh_b.centre, ident)])
+    with ThreadPoolExecutor(max_workers=workers) as ex:
         fw = [ex.submit(_scan_worker, mesh_a, mesh_b, poses, list(range(w, len(poses), workers)), kappa, precision,
-                        nbsize, device, tol, max_iterations, contexts[w] if contexts else None)
+                        nbsize, device, tol, max_iterations, contexts[w] if contexts else None, isolated[w])
               for w in range(workers)]
-        e_a, _ = fa.result()
-        e_b, _ = fb.result()
-        res = sorted(r for f in fw for r in f.result())
+        outs = [f.result() for f in fw]
+    e_a = outs[0][1][0]
+    e_b = outs[1 % workers][1][-1]
+    res = sorted(r for o in outs for r in o[0])
     dt = time.perf_counter() - t0
     ec = [r[1] for r in res]
     return ScanResult([e - e_a - e_b for e in ec], ec, e_a, e_b, dt, [r[2] for r in res])

@@ -315,8 +315,10 @@ def _scan_mode(args, local):
     # device blocks of a pose stay on the device for the next
     ctxs = [b.EngineContext(local) for _ in range(args.workers)]
     try:
-        rigid_body_scan(ma, mb, random_poses(args.workers, seed=99), kappa=0.1, workers=args.workers, device=local,
-                        contexts=ctxs)  # warm-up
+        # warm-up: a scan of as many other poses, so that every context has
+        # seen problems of the sizes the timed scan builds
+        rigid_body_scan(ma, mb, random_poses(args.poses, seed=99), kappa=0.1, workers=args.workers, device=local,
+                        contexts=ctxs)
         res = rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs)
     finally:
         for c in ctxs:
