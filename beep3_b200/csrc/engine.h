@@ -72,11 +72,16 @@ struct Ctx {
   uint64_t budget = 0;
   uint64_t used = 0;    // bytes of live device buffers
   uint64_t cached = 0;  // bytes of released buffers kept for reuse
-  std::multimap<uint64_t, void*> cache;  // block size -> block
+  struct Cached {
+    void* p;
+    uint64_t stamp;  // order of release
+  };
+  std::multimap<uint64_t, Cached> cache;  // block size -> block
+  uint64_t releases = 0;
   std::mutex mu;
   int sm_count = 148;
-  // released blocks beyond this are freed at once
-  static constexpr uint64_t kCacheMax = 8ull << 30;
+  // released blocks beyond this are freed at once, the longest unused first
+  static constexpr uint64_t kCacheMax = 16ull << 30;
 
   // A released block of at least `bytes` (at most a quarter + 1 MB larger),
   // now live, or nullptr.  A problem rebuilt on the same context (a new pose)
@@ -87,7 +92,7 @@ struct Ctx {
     auto it = cache.lower_bound(bytes);
     if (it == cache.end() || it->first > bytes + bytes / 4 + (1ull << 20)) return nullptr;
     block = it->first;
-    void* p = it->second;
+    void* p = it->second.p;
     cache.erase(it);
     cached -= block;
     used += block;
@@ -112,13 +117,17 @@ struct Ctx {
   void give(void* p, uint64_t block) {
     std::lock_guard<std::mutex> lk(mu);
     used -= block;
-    cache.emplace(block, p);
+    cache.emplace(block, Cached{p, ++releases});
     cached += block;
-    while (cached > kCacheMax && !cache.empty()) {  // the largest blocks first
-      auto it = std::prev(cache.end());
-      cudaFree(it->second);
-      cached -= it->first;
-      cache.erase(it);
+    // a problem rebuilt on the context asks for the sizes it released last,
+    // so the blocks released longest ago go first
+    while (cached > kCacheMax && !cache.empty()) {
+      auto oldest = cache.begin();
+      for (auto it = cache.begin(); it != cache.end(); ++it)
+        if (it->second.stamp < oldest->second.stamp) oldest = it;
+      cudaFree(oldest->second.p);
+      cached -= oldest->first;
+      cache.erase(oldest);
     }
   }
   void trim() {
@@ -128,7 +137,7 @@ struct Ctx {
 
  private:
   void trim_locked() {
-    for (auto& kv : cache) cudaFree(kv.second);
+    for (auto& kv : cache) cudaFree(kv.second.p);
     cache.clear();
     cached = 0;
   }
