@@ -115,6 +115,7 @@ _SIGS = {
     "bp_solve": [_P, _P, _P, _D, _I, _I, C.POINTER(_I), C.POINTER(_D)],
     "bp_solve_device": [_P, _P, _P, _D, _I, _I, C.POINTER(_I), C.POINTER(_D)],
     "bp_rhs": [_P, _P, _I, _D, _P],
+    "bp_rhs_posed": [_P, _P, _P, _D, _P],
     "bp_rhs_noalloc": [_I, _P, _P, _I, _P, _I, _D, _P, _P],
     "bp_energy_coefficients": [_P, _I, _I, _P, _I, _D, _P, _P],
     "bp_energy": [_P, _I, _I, _P, _P, _D, _P, C.POINTER(_D)],

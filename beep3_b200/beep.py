@@ -213,6 +213,8 @@ class BEEP:
         self.hbm_budget_bytes = int(hbm_budget_bytes)
         self._engine = context
         self._own_engine = context is None
+        # rigid-body scans: keep each mesh's own-charge potential across moves
+        self.cache_own_potentials = False
         if context is not None:
             self.device = context.device
         self._problem = None
@@ -373,12 +375,25 @@ class BEEP:
         return y
 
     def set_rhs(self) -> np.ndarray:
-        """BEEP::set_rhs with a direct Coulomb sum over all instances' charges."""
+        """BEEP::set_rhs with a direct Coulomb sum over all instances' charges.
+        With ``cache_own_potentials`` set, each instance's potential at its
+        own patches is computed once per mesh and kept with it across rigid
+        moves (bp_rhs_posed); only the other instances' charges are summed
+        per call."""
         p = self.build()
-        ch = np.ascontiguousarray(np.concatenate([i.charges for i in self.instances]))
-        ch = np.ascontiguousarray(ch[ch[:, 3] != 0])
+        if not self.cache_own_potentials:
+            ch = np.ascontiguousarray(np.concatenate([i.charges for i in self.instances]))
+            ch = np.ascontiguousarray(ch[ch[:, 3] != 0])
+            rhs = np.empty(2 * self.num_patches)
+            N.check(N.lib().bp_rhs(p, N.ptr(ch), len(ch), self.eps_solvent, N.ptr(rhs)))
+            self.rhs = rhs
+            return rhs
+        own = [np.ascontiguousarray(i.mesh.charges[i.mesh.charges[:, 3] != 0]) for i in self.instances]
+        ptrs = (C.c_void_p * len(own))(*[a.ctypes.data for a in own])
+        counts = (C.c_int32 * len(own))(*[len(a) for a in own])
         rhs = np.empty(2 * self.num_patches)
-        N.check(N.lib().bp_rhs(p, N.ptr(ch), len(ch), self.eps_solvent, N.ptr(rhs)))
+        N.check(N.lib().bp_rhs_posed(p, C.cast(ptrs, C.c_void_p), C.cast(counts, C.c_void_p), self.eps_solvent,
+                                     N.ptr(rhs)))
         self.rhs = rhs
         return rhs
 

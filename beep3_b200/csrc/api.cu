@@ -352,6 +352,16 @@ BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int3
         rg.c[k] = m.centre[k];
         rg.o[k] = inst[q].offset[k];
       }
+      Placement pl;
+      pl.mesh = reinterpret_cast<DevMesh*>(inst[q].mesh);
+      for (int k = 0; k < 9; ++k) pl.R[k] = rg.R[k];
+      for (int k = 0; k < 3; ++k) {
+        pl.c[k] = rg.c[k];
+        pl.o[k] = rg.o[k];
+      }
+      pl.q_begin = bq;
+      pl.q_count = m.n_qual_pts;
+      P->placements.push_back(pl);
       // patch centres and normals on the host (the tree is built there)
       for (int i = 0; i < m.n; ++i) {
         const double* p = &m.h_centroid[3 * (size_t)i];
@@ -577,6 +587,26 @@ BP_API int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charge
       BP_CUDA(cudaMemcpyAsync(dch.get(), charges_xyzq, sizeof(double) * 4 * (size_t)n_charges, cudaMemcpyHostToDevice,
                               c->stream));
     rhs_device(*P, dch.as<double>(), n_charges, eps_solvent, P->d_y.as<double>());
+    BP_CUDA(cudaMemcpyAsync(rhs, P->d_y.get(), sizeof(double) * 2 * (size_t)P->n, cudaMemcpyDeviceToHost, c->stream));
+    BP_CUDA(cudaStreamSynchronize(c->stream));
+    return BP_OK;
+  });
+}
+
+BP_API int32_t bp_rhs_posed(bp_problem p, const double* const* charges_xyzq, const int32_t* n_charges,
+                            double eps_solvent, double* rhs) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P || !rhs || !charges_xyzq || !n_charges) return fail(BP_ERR_INVALID, "bp_rhs_posed: bad argument");
+    if (P->placements.empty())
+      return fail(BP_ERR_INVALID, "bp_rhs_posed: the problem was not made by bp_problem_create_posed");
+    if (!(eps_solvent > 0)) return fail(BP_ERR_INVALID, "bp_rhs_posed: eps_solvent must be positive");
+    for (size_t k = 0; k < P->placements.size(); ++k)
+      if (n_charges[k] < 0 || (n_charges[k] > 0 && !charges_xyzq[k]))
+        return fail(BP_ERR_INVALID, "bp_rhs_posed: bad charge list of instance " + std::to_string(k));
+    DeviceGuard g(P->ctx->device);
+    Ctx* c = P->ctx;
+    rhs_posed_device(*P, charges_xyzq, n_charges, eps_solvent, P->d_y.as<double>());
     BP_CUDA(cudaMemcpyAsync(rhs, P->d_y.get(), sizeof(double) * 2 * (size_t)P->n, cudaMemcpyDeviceToHost, c->stream));
     BP_CUDA(cudaStreamSynchronize(c->stream));
     return BP_OK;

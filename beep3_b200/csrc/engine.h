@@ -252,6 +252,25 @@ struct DevMesh {
   std::vector<int32_t> h_qual_off, h_quad_off, h_gal_off;
   int n_qual_pts = 0, n_quad_pts = 0, n_gal_pts = 0;
   DevBuf d_qual, d_quad, d_gal;  // SoA of double, 7 arrays each
+  // potential of a charge list given in the mesh's frame at the mesh's
+  // qualocation points (2 doubles per point), kept for rigid moves
+  struct SelfPotential {
+    std::vector<double> charges;  // x, y, z, q in the mesh's frame
+    double scale = 0;
+    bool fp64 = true;
+    DevBuf vals;
+  };
+  std::vector<SelfPotential> self_potential;  // most recently used last
+  static constexpr size_t kSelfPotentials = 4;
+  std::mutex mu;
+};
+
+// Where an instance of a device-resident mesh sits in a posed problem:
+// p -> R (p - c) + o, its qualocation points at [q_begin, q_begin + q_count).
+struct Placement {
+  DevMesh* mesh = nullptr;
+  double R[9], c[3], o[3];
+  int q_begin = 0, q_count = 0;
 };
 
 struct Problem;
@@ -264,6 +283,7 @@ struct Problem {
   bp_params params{};
   bool fp64 = true;
   TreeInfo tree;
+  std::vector<Placement> placements;  // set by bp_problem_create_posed
   // patches (original order)
   std::vector<double> h_centroid, h_normal, h_area, h_eps, h_gc;
   std::vector<int32_t> h_qual_off, h_quad_off, h_gal_off;
@@ -381,6 +401,10 @@ int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int
                  double* rel_resid);
 // sources.cu
 void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev);
+// right-hand side of a posed problem from each instance's charges in its
+// mesh's frame (host arrays); own-charge potentials cached on the meshes
+void rhs_posed_device(Problem& P, const double* const* charges_host, const int32_t* n_charges, double eps_solvent,
+                      double* rhs_dev);
 void energy_coefficients_device(Problem& P, int first, int count, const double* charges_dev, int n_charges,
                                 double* cf_dev, double* ch_dev);
 

@@ -14,6 +14,9 @@
 // (Mesh::renormalise_energy_precalcs, src/bem/mesh.cpp:905-925).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+
 #include <mutex>
 #include <string>
 #include <vector>
@@ -39,11 +42,12 @@ __device__ __forceinline__ double rsqrt_newton(double d2) {
 }
 
 // One thread per point; charges staged through shared memory in tiles.
-// out[2*p] = w * phi * scale, out[2*p+1] = w * (grad phi . n) * scale,
-// exact in FP64.
+// For point p = first_pt + k: out[2k] = w * phi * scale, out[2k+1] =
+// w * (grad phi . n) * scale, exact in FP64, plus add[2k], add[2k+1] when
+// add is set.
 __global__ void point_potential_kernel(const double* __restrict__ pts, int npts, int first_pt, int count_pts,
                                        const double* __restrict__ charges, int nc, double scale,
-                                       double* __restrict__ out) {
+                                       double* __restrict__ out, const double* __restrict__ add) {
   __shared__ double4 tile[kThreads];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = k < count_pts;
@@ -80,8 +84,9 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
   if (active) {
     const double w = pts[6 * (size_t)npts + p];
     const double nx = pts[3 * (size_t)npts + p], ny = pts[4 * (size_t)npts + p], nz = pts[5 * (size_t)npts + p];
-    out[2 * k] = w * phi * scale;
-    out[2 * k + 1] = w * (gx * nx + gy * ny + gz * nz) * scale;
+    const double a0 = add ? add[2 * k] : 0.0, a1 = add ? add[2 * k + 1] : 0.0;
+    out[2 * k] = w * phi * scale + a0;
+    out[2 * k + 1] = w * (gx * nx + gy * ny + gz * nz) * scale + a1;
   }
 }
 
@@ -95,14 +100,18 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
 // (kPtsPerThread), so every charge read from shared memory serves both, and
 // a coincident charge and point give a zero term by a select, not a branch.
 constexpr int kPtsPerThread = 2;
+// Points first_pt .. first_pt + count_pts - 1 of the list (stride npts);
+// outputs and the optional addend are indexed from first_pt.
 __global__ void __launch_bounds__(kThreads) point_potential_fast_kernel(const double* __restrict__ pts, int npts,
+                                                                        int first_pt, int count_pts,
                                                                         const double* __restrict__ charges, int nc,
-                                                                        double scale, double* __restrict__ out) {
+                                                                        double scale, double* __restrict__ out,
+                                                                        const double* __restrict__ add) {
   __shared__ float4 th[kThreads], tl[kThreads];
   constexpr int P = kPtsPerThread;
   const int p0 = blockIdx.x * (P * kThreads);  // the block's first point: origin of the offsets
-  const double ox = pts[min(p0, npts - 1)], oy = pts[(size_t)npts + min(p0, npts - 1)],
-               oz = pts[2 * (size_t)npts + min(p0, npts - 1)];
+  const int po = first_pt + min(p0, count_pts - 1);
+  const double ox = pts[po], oy = pts[(size_t)npts + po], oz = pts[2 * (size_t)npts + po];
   auto split = [](double v, float& hi, float& lo) {
     hi = (float)v;
     lo = (float)(v - (double)hi);
@@ -110,7 +119,7 @@ __global__ void __launch_bounds__(kThreads) point_potential_fast_kernel(const do
   float xh[P], xl[P], yh[P], yl[P], zh[P], zl[P];
 #pragma unroll
   for (int j = 0; j < P; ++j) {
-    const int p = min(p0 + j * kThreads + (int)threadIdx.x, npts - 1);
+    const int p = first_pt + min(p0 + j * kThreads + (int)threadIdx.x, count_pts - 1);
     split(pts[p] - ox, xh[j], xl[j]);
     split(pts[(size_t)npts + p] - oy, yh[j], yl[j]);
     split(pts[2 * (size_t)npts + p] - oz, zh[j], zl[j]);
@@ -163,12 +172,14 @@ __global__ void __launch_bounds__(kThreads) point_potential_fast_kernel(const do
   }
 #pragma unroll
   for (int j = 0; j < P; ++j) {
-    const int p = p0 + j * kThreads + (int)threadIdx.x;
-    if (p >= npts) continue;
+    const int k = p0 + j * kThreads + (int)threadIdx.x;
+    if (k >= count_pts) continue;
+    const int p = first_pt + k;
     const double w = pts[6 * (size_t)npts + p];
     const double nx = pts[3 * (size_t)npts + p], ny = pts[4 * (size_t)npts + p], nz = pts[5 * (size_t)npts + p];
-    out[2 * (size_t)p] = w * phi[j] * scale;
-    out[2 * (size_t)p + 1] = w * (gx[j] * nx + gy[j] * ny + gz[j] * nz) * scale;
+    const double a0 = add ? add[2 * (size_t)k] : 0.0, a1 = add ? add[2 * (size_t)k + 1] : 0.0;
+    out[2 * (size_t)k] = w * phi[j] * scale + a0;
+    out[2 * (size_t)k + 1] = w * (gx[j] * nx + gy[j] * ny + gz[j] * nz) * scale + a1;
   }
 }
 
@@ -198,16 +209,114 @@ void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps
   const double scale = kOneOver4Pi / eps_solvent;
   if (P.fp64)
     point_potential_kernel<<<(nq + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
-        P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>());
+        P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale, vals.as<double>(), nullptr);
   else
     point_potential_fast_kernel<<<(nq + kPtsPerThread * kThreads - 1) / (kPtsPerThread * kThreads), kThreads, 0,
-                                  ctx->stream>>>(P.d_qual.as<double>(), nq, charges_dev, n_charges, scale,
-                                                 vals.as<double>());
+                                  ctx->stream>>>(P.d_qual.as<double>(), nq, 0, nq, charges_dev, n_charges, scale,
+                                                 vals.as<double>(), nullptr);
   BP_LAUNCH_CHECK();
   sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
       P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
   BP_LAUNCH_CHECK();
   BP_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+namespace {
+
+// Per-point values of points [first, first + count) of a SoA list (stride
+// npts) into out (indexed from first), plus add when set: the FP64 or the
+// fast kernel.
+void launch_point_potential(bool fp64, const double* pts, int npts, int first, int count, const double* charges,
+                            int nc, double scale, double* out, const double* add, cudaStream_t st) {
+  if (count <= 0) return;
+  if (fp64)
+    point_potential_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, st>>>(pts, npts, first, count, charges,
+                                                                                 nc, scale, out, add);
+  else
+    point_potential_fast_kernel<<<(count + kPtsPerThread * kThreads - 1) / (kPtsPerThread * kThreads), kThreads, 0,
+                                  st>>>(pts, npts, first, count, charges, nc, scale, out, add);
+  BP_LAUNCH_CHECK();
+}
+
+// The potential of a charge list (mesh frame) at the mesh's qualocation
+// points, from the mesh's cache or computed into it.  Rotation and
+// translation leave distances and normal derivatives unchanged, so the
+// values serve every placement of the mesh.
+const double* mesh_self_potential(DevMesh& m, const double* charges, int nc, double scale, bool fp64,
+                                  cudaStream_t st) {
+  std::lock_guard<std::mutex> lk(m.mu);
+  auto& list = m.self_potential;
+  for (size_t k = 0; k < list.size(); ++k) {
+    const DevMesh::SelfPotential& e = list[k];
+    if (e.fp64 == fp64 && e.scale == scale && e.charges.size() == 4 * (size_t)nc &&
+        (nc == 0 || std::memcmp(e.charges.data(), charges, sizeof(double) * 4 * (size_t)nc) == 0)) {
+      std::rotate(list.begin() + k, list.begin() + k + 1, list.end());  // most recently used last
+      return list.back().vals.as<double>();
+    }
+  }
+  if (list.size() >= DevMesh::kSelfPotentials) list.erase(list.begin());
+  DevMesh::SelfPotential e;
+  e.charges.assign(charges, charges + 4 * (size_t)nc);
+  e.scale = scale;
+  e.fp64 = fp64;
+  e.vals.alloc(m.ctx, sizeof(double) * 2 * (size_t)std::max(1, m.n_qual_pts));
+  DevBuf dch(m.ctx, sizeof(double) * 4 * (size_t)std::max(1, nc));
+  if (nc) BP_CUDA(cudaMemcpyAsync(dch.get(), charges, sizeof(double) * 4 * (size_t)nc, cudaMemcpyHostToDevice, st));
+  launch_point_potential(fp64, m.d_qual.as<double>(), m.n_qual_pts, 0, m.n_qual_pts, dch.as<double>(), nc, scale,
+                         e.vals.as<double>(), nullptr, st);
+  list.push_back(std::move(e));
+  return list.back().vals.as<double>();
+}
+
+}  // namespace
+
+void rhs_posed_device(Problem& P, const double* const* charges_host, const int32_t* n_charges, double eps_solvent,
+                      double* rhs_dev) {
+  Ctx* ctx = P.ctx;
+  cudaStream_t st = ctx->stream;
+  const int ni = (int)P.placements.size();
+  const double scale = kOneOver4Pi / eps_solvent;
+  // every instance's charges in the problem's frame
+  std::vector<size_t> wstart(ni + 1, 0);
+  for (int k = 0; k < ni; ++k) wstart[k + 1] = wstart[k] + (size_t)n_charges[k];
+  std::vector<double> world(4 * wstart[ni]);
+  for (int k = 0; k < ni; ++k) {
+    const Placement& pl = P.placements[k];
+    for (int i = 0; i < n_charges[k]; ++i) {
+      const double* ch = charges_host[k] + 4 * (size_t)i;
+      const double x = ch[0] - pl.c[0], y = ch[1] - pl.c[1], z = ch[2] - pl.c[2];
+      double* w = &world[4 * (wstart[k] + i)];
+      for (int r = 0; r < 3; ++r) w[r] = pl.R[3 * r] * x + pl.R[3 * r + 1] * y + pl.R[3 * r + 2] * z + pl.o[r];
+      w[3] = ch[3];
+    }
+  }
+  // per instance the other instances' charges, one list after another
+  std::vector<size_t> ostart(ni + 1, 0);
+  std::vector<double> others;
+  for (int k = 0; k < ni; ++k) {
+    for (int j = 0; j < ni; ++j)
+      if (j != k) others.insert(others.end(), world.begin() + 4 * wstart[j], world.begin() + 4 * wstart[j + 1]);
+    ostart[k + 1] = others.size() / 4;
+  }
+  DevBuf& dch = P.scratch_charges;
+  const size_t cbytes = sizeof(double) * std::max<size_t>(4, others.size());
+  if (dch.bytes() < cbytes) dch.alloc(ctx, cbytes);
+  if (!others.empty())
+    BP_CUDA(cudaMemcpyAsync(dch.get(), others.data(), sizeof(double) * others.size(), cudaMemcpyHostToDevice, st));
+  const int nq = P.n_qual_pts;
+  DevBuf& vals = P.scratch_vals;
+  if (vals.bytes() < sizeof(double) * 2 * (size_t)nq) vals.alloc(ctx, sizeof(double) * 2 * (size_t)nq);
+  for (int k = 0; k < ni; ++k) {
+    const Placement& pl = P.placements[k];
+    const double* self = mesh_self_potential(*pl.mesh, charges_host[k], n_charges[k], scale, P.fp64, st);
+    launch_point_potential(P.fp64, P.d_qual.as<double>(), nq, pl.q_begin, pl.q_count,
+                           dch.as<double>() + 4 * ostart[k], (int)(ostart[k + 1] - ostart[k]), scale,
+                           vals.as<double>() + 2 * (size_t)pl.q_begin, self, st);
+  }
+  sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+      P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
+  BP_LAUNCH_CHECK();
+  BP_CUDA(cudaStreamSynchronize(st));
 }
 
 void energy_coefficients_device(Problem& P, int first, int count, const double* charges_dev, int n_charges,
@@ -218,7 +327,7 @@ void energy_coefficients_device(Problem& P, int first, int count, const double* 
   DevBuf vals(ctx, sizeof(double) * 2 * (size_t)std::max(1, p1 - p0));
   if (p1 > p0) {
     point_potential_kernel<<<(p1 - p0 + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
-        P.d_gal.as<double>(), ng, p0, p1 - p0, charges_dev, n_charges, kOneOver4Pi, vals.as<double>());
+        P.d_gal.as<double>(), ng, p0, p1 - p0, charges_dev, n_charges, kOneOver4Pi, vals.as<double>(), nullptr);
     BP_LAUNCH_CHECK();
   }
   // vals[2p] -> ec_h (potential), vals[2p+1] -> ec_f (normal field)
@@ -293,7 +402,7 @@ extern "C" BP_API int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     const double scale = kOneOver4Pi / eps_solvent;
     point_potential_kernel<<<(n_qual_points + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-        qual_points_soa_dev, n_qual_points, 0, n_qual_points, charges_xyzq_dev, n_charges, scale, scratch);
+        qual_points_soa_dev, n_qual_points, 0, n_qual_points, charges_xyzq_dev, n_charges, scale, scratch, nullptr);
     BP_LAUNCH_CHECK();
     sum_points_kernel<<<(n_patches + kThreads - 1) / kThreads, kThreads, 0, st>>>(
         qual_offsets_dev, 0, n_patches, 0, scratch, rhs_dev, rhs_dev + n_patches);

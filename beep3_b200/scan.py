@@ -78,6 +78,7 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
     are solved first, on the same context.  Returns (pose results, their
     energies)."""
     bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
+    bp.cache_own_potentials = True  # instance B only moves: its own potential, and A's, stay
     out = []
     try:
         iso = [_solve_energy(inst, kappa, precision, nbsize, device, tol, max_it, context=bp.engine)[0]

@@ -225,6 +225,17 @@ int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_dev, doub
  * Coulomb potential and field of all charges at every qualocation point,
  * weighted and scaled by 1/(4 pi eps_solvent).  charges_xyzq: [n][4]. */
 int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charges, double eps_solvent, double* rhs);
+/* The same for a problem made by bp_problem_create_posed, from each
+ * instance's charges in its mesh's own frame (the frame of the points given
+ * to bp_mesh_create): charges_xyzq[k] holds n_charges[k] charges of
+ * instance k.  The potential of an instance's own charges at its own
+ * qualocation points does not change when the instance moves, so it is
+ * computed once per mesh, charge list, eps_solvent and precision and kept
+ * with the mesh (the 4 most recent); each call sums the other instances'
+ * charges only.  Equal to bp_rhs with every charge placed in the problem's
+ * frame, up to rounding. */
+int32_t bp_rhs_posed(bp_problem p, const double* const* charges_xyzq, const int32_t* n_charges, double eps_solvent,
+                     double* rhs);
 
 /* Right-hand side without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- host applications

@@ -118,3 +118,31 @@ def test_shared_context_reuses_and_evicts_meshes():
         assert ectx.memory()[1] == 0
     finally:
         ectx.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 2e-6)])
+def test_posed_rhs_equals_direct_sum(precision, tol):
+    """bp_rhs_posed (own-charge potentials kept with the meshes) against
+    bp_rhs over all charges placed in the problem's frame, before and after a
+    move; the second pose reuses the cached own-charge potentials."""
+    V, T, shape = b.star_surface(4, 15.0, seed=51)
+    ma = b.Mesh(V, T, b.charges_in_star(60, shape, seed=52))
+    V2, T2, shape2 = b.star_surface(3, 10.0, seed=53)
+    mb = b.Mesh(V2, T2, b.charges_in_star(25, shape2, seed=54))
+    q = b.random_quaternion(np.random.default_rng(55))
+    bp = b.BEEP(kappa=0.1, nbsize=300, precision=precision)
+    bp.cache_own_potentials = True
+    try:
+        bp.insert_mesh_instance(ma)
+        bp.insert_mesh_instance(mb, offset=ma.centre + np.array([28.0, -4.0, 6.0]), rotation=q, eps_protein=4.0)
+        for pose in range(2):
+            if pose:
+                bp.move_mesh_instance(1, ma.centre + np.array([-22.0, 15.0, 3.0]), q[[0, 3, 1, 2]])
+            r_posed = bp.set_rhs().copy()
+            ch = np.ascontiguousarray(np.concatenate([i.charges for i in bp.instances]))
+            r_direct = np.empty_like(r_posed)
+            N.check(N.lib().bp_rhs(bp.build(), N.ptr(ch), len(ch), bp.eps_solvent, N.ptr(r_direct)))
+            assert rel_l2(r_posed, r_direct) < tol
+            assert np.array_equal(bp.set_rhs(), r_posed)  # cached own-charge potentials: same values
+    finally:
+        bp.close()
