@@ -52,3 +52,13 @@ def test_energy_entry_point_validates():
     L = N.lib()
     e = C.c_double()
     assert L.bp_energy(None, 0, 1, None, None, 40.0, None, C.byref(e)) == N.BP_ERR_INVALID
+
+
+def test_posed_rhs_entry_point_validates():
+    L = N.lib()
+    rhs = np.zeros(2)
+    counts = (C.c_int32 * 1)(0)
+    ptrs = (C.c_void_p * 1)(None)
+    assert L.bp_rhs_posed(None, C.cast(ptrs, C.c_void_p), C.cast(counts, C.c_void_p), 80.0,
+                          N.ptr(rhs)) == N.BP_ERR_INVALID
+    assert b"bad argument" in L.bp_last_error()
