@@ -294,6 +294,13 @@ BP_API int32_t bp_mesh_destroy(bp_mesh mesh) {
   return guarded_engine([&]() -> int32_t {
     DevMesh* m = reinterpret_cast<DevMesh*>(mesh);
     if (!m) return BP_OK;
+    {
+      std::lock_guard<std::mutex> lk(m->mu);
+      if (m->users > 0) {  // the last posed problem placed from it deletes it
+        m->destroy_pending = true;
+        return BP_OK;
+      }
+    }
     DeviceGuard g(m->ctx->device);
     cudaStreamSynchronize(m->ctx->stream);
     delete m;
@@ -362,6 +369,7 @@ BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int3
       pl.q_begin = bq;
       pl.q_count = m.n_qual_pts;
       P->placements.push_back(pl);
+      mesh_acquire(pl.mesh);
       // patch centres and normals on the host (the tree is built there)
       for (int i = 0; i < m.n; ++i) {
         const double* p = &m.h_centroid[3 * (size_t)i];

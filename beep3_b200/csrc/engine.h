@@ -262,8 +262,23 @@ struct DevMesh {
   };
   std::vector<SelfPotential> self_potential;  // most recently used last
   static constexpr size_t kSelfPotentials = 4;
+  // posed problems placed from this mesh keep it: bp_mesh_destroy while any
+  // exists leaves the deletion to the last of them
+  int users = 0;
+  bool destroy_pending = false;
   std::mutex mu;
 };
+
+inline void mesh_acquire(DevMesh* m) {
+  std::lock_guard<std::mutex> lk(m->mu);
+  ++m->users;
+}
+// True when the caller must delete the mesh (its destruction was asked for
+// and this was its last user).
+inline bool mesh_release(DevMesh* m) {
+  std::lock_guard<std::mutex> lk(m->mu);
+  return --m->users == 0 && m->destroy_pending;
+}
 
 // Where an instance of a device-resident mesh sits in a posed problem:
 // p -> R (p - c) + o, its qualocation points at [q_begin, q_begin + q_count).
@@ -326,6 +341,8 @@ struct Problem {
     if (asm_in) cudaEventDestroy(asm_in);
     if (asm_t0) cudaEventDestroy(asm_t0);
     if (asm_t1) cudaEventDestroy(asm_t1);
+    for (const Placement& pl : placements)
+      if (mesh_release(pl.mesh)) delete pl.mesh;
     if (graph) cudaGraphExecDestroy(graph);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);

@@ -150,9 +150,10 @@ int32_t bp_problem_create(bp_ctx ctx, const bp_patches* patches, const bp_params
  * moves its host patch objects for every pose instead
  * (MeshInstance::init, src/bem/mesh_instance.cpp:50-85; NodePatch
  * change_coordinate_frame, src/bem/node_patch.cpp:402-478); these entry
- * points have no counterpart there.  A mesh must outlive the problems built
- * from it; its patches' dielectric_ratio entries are ignored (the instance
- * gives it).
+ * points have no counterpart there.  Problems built from a mesh keep it:
+ * bp_mesh_destroy while one exists defers the deletion to the last of them
+ * (bp_rhs_posed reads the mesh).  Its patches' dielectric_ratio entries are
+ * ignored (the instance gives it).  The context must outlive its meshes.
  */
 typedef struct bp_mesh_s* bp_mesh;
 int32_t bp_mesh_create(bp_ctx ctx, const bp_patches* patches, const double centre[3], bp_mesh* out);

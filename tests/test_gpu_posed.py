@@ -146,3 +146,43 @@ def test_posed_rhs_equals_direct_sum(precision, tol):
             assert np.array_equal(bp.set_rhs(), r_posed)  # cached own-charge potentials: same values
     finally:
         bp.close()
+
+
+def test_mesh_destroyed_before_its_problem():
+    """bp_mesh_destroy while a posed problem built from the mesh is alive
+    defers the deletion; the problem's posed right-hand side still reads the
+    mesh, and destroying the problem then frees it."""
+    V, T, shape = b.star_surface(3, 10.0, seed=61)
+    m = b.Mesh(V, T, b.charges_in_star(15, shape, seed=62))
+    ectx = b.EngineContext(0)
+    try:
+        bp = b.BEEP(kappa=0.1, nbsize=300, precision="fp64", context=ectx)
+        bp.insert_mesh_instance(m)
+        h_mesh = ectx.mesh_handle(m)
+        prm_centre, edge = bp.calculate_bounding_cube()
+        inst = (N.bp_instance * 1)()
+        inst[0].mesh = h_mesh
+        inst[0].rotation[:] = [1, 0, 0, 0, 1, 0, 0, 0, 1]
+        inst[0].offset[:] = list(m.centre)
+        inst[0].dielectric_ratio = 40.0
+        prm = N.bp_params(0.1, BETA0, (C.c_double * 3)(*prm_centre), edge, 300, 9, N.BP_PREC_FP64, 0)
+        h = C.c_void_p()
+        N.check(N.lib().bp_problem_create_posed(ectx.handle, inst, 1, C.byref(prm), C.byref(h)))
+        try:
+            del ectx._meshes[id(m)]
+            N.check(N.lib().bp_mesh_destroy(h_mesh))  # deferred: the problem holds the mesh
+            own = np.ascontiguousarray(m.charges[m.charges[:, 3] != 0])
+            ptrs = (C.c_void_p * 1)(own.ctypes.data)
+            counts = (C.c_int32 * 1)(len(own))
+            r_posed = np.empty(2 * m.patches.n)
+            N.check(N.lib().bp_rhs_posed(h, C.cast(ptrs, C.c_void_p), C.cast(counts, C.c_void_p), 80.0,
+                                         N.ptr(r_posed)))
+            world = np.ascontiguousarray(m.charges[m.charges[:, 3] != 0])  # identity placement
+            r_direct = np.empty_like(r_posed)
+            N.check(N.lib().bp_rhs(h, N.ptr(world), len(world), 80.0, N.ptr(r_direct)))
+            assert rel_l2(r_posed, r_direct) < 1e-13
+        finally:
+            N.check(N.lib().bp_problem_destroy(h))  # the last user: frees the mesh
+        bp.close()
+    finally:
+        ectx.close()
