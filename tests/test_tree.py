@@ -65,3 +65,23 @@ def test_tree_invariants(k, nbsize):
     assert work / n <= nbsize * 1.05
     # children of split non-shadow nodes' neighbours exist (full neighbourhoods)
     assert t["n_levels"] >= 3
+
+
+@pytest.mark.parametrize("nbsize", [60, 100, 200])
+def test_tree_ties_on_split_planes(nbsize):
+    """Points on a lattice whose planes are the nodes' split planes (the
+    child choice p > centre sends ties to the lower child), with duplicates:
+    the C++ tree has the restatement's nodes, parents, children and
+    contents.  Leaf flags and local-expansion slots are left out: on a
+    lattice many leaves tie on their neighbourhood count, and which of them
+    the refinement splits follows the sort's order of ties (std::sort in the
+    engine, as in the reference; a stable sort in the restatement)."""
+    g = np.arange(-8.0, 8.01, 2.0)
+    pts = np.array([[x, y, z] for x in g for y in g for z in g])
+    pts = np.concatenate([pts, pts[::7]])  # duplicated points
+    t = build_tree(pts, np.zeros(3), 16.0, nbsize)
+    r = OT.build(pts, np.zeros(3), 16.0, nbsize)
+    assert t["n_levels"] == r["n_levels"]
+    cols = [0, 1, 2, 3, 5, 6, 7, 8] + list(range(10, 18))
+    np.testing.assert_array_equal(t["info"][:, cols], r["info"][:, cols])
+    np.testing.assert_array_equal(t["contents"], r["contents"])
