@@ -63,7 +63,15 @@ __device__ __forceinline__ double4 ld_stream(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
-__device__ __forceinline__ float fast_rsqrt(float x) { return rsqrtf(x); }
+// FP32: the hardware approximations with denormals flushed (PTX
+// rsqrt.approx.ftz / ex2.approx.ftz).  The arguments here are normal
+// numbers (r^2 >= 1e-9 and exponents above -126), where flushing changes
+// nothing and saves the denormal handling of rsqrtf / exp2f.
+__device__ __forceinline__ float fast_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ double fast_rsqrt(double x) { return rsqrt(x); }
 __device__ __forceinline__ float fexp(float x) { return expf(x); }
 __device__ __forceinline__ double fexp(double x) { return exp(x); }
@@ -115,7 +123,11 @@ __device__ __forceinline__ void pair_term(T qx, T qy, T qz, T qnx, T qny, T qnz,
 //   Hessian terms             : gr5 = g3 t, pu = e g t (3 kappa/r + kappa^2 + 3 t)
 // (the expressions of pair_term, factored).  `ek` is the exponent scale:
 // -kappa log2(e) for FP32, where e = 2^(ek r) (exp2f), and -kappa for FP64.
-__device__ __forceinline__ float exp_scaled(float ek, float r) { return exp2f(ek * r); }
+__device__ __forceinline__ float exp_scaled(float ek, float r) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(ek * r));
+  return y;
+}
 __device__ __forceinline__ double exp_scaled(double ek, double r) { return exp(ek * r); }
 template <typename T>
 __device__ __forceinline__ T exp_scale(T kappa);
