@@ -173,7 +173,8 @@ class EngineContext:
             N.lib().bp_mesh_destroy(e[1])
         self._meshes = {}
         if self._ctx:
-            N.lib().bp_ctx_destroy(self._ctx)
+            # refused (and the context kept) while a problem made on it is alive
+            N.check(N.lib().bp_ctx_destroy(self._ctx))
             self._ctx = C.c_void_p()
 
 

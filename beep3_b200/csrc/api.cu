@@ -165,6 +165,10 @@ BP_API int32_t bp_ctx_destroy(bp_ctx ctx) {
   return guarded_engine([&]() -> int32_t {
     Ctx* c = as_ctx(ctx);
     if (!c) return BP_OK;
+    if (c->live_problems.load() > 0 || c->live_meshes.load() > 0)
+      return fail(BP_ERR_INVALID, "bp_ctx_destroy: " + std::to_string(c->live_problems.load()) + " problem(s) and " +
+                                      std::to_string(c->live_meshes.load()) +
+                                      " mesh(es) of this context are still alive; destroy them first");
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
     c->trim();  // the released blocks kept for reuse
@@ -175,10 +179,19 @@ BP_API int32_t bp_ctx_destroy(bp_ctx ctx) {
 }
 
 BP_API int32_t bp_ctx_set_stream(bp_ctx ctx, void* stream) {
-  Ctx* c = as_ctx(ctx);
-  if (!c) return fail(BP_ERR_INVALID, "bp_ctx_set_stream: null context");
-  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
-  return BP_OK;
+  return guarded_engine([&]() -> int32_t {
+    Ctx* c = as_ctx(ctx);
+    if (!c) return fail(BP_ERR_INVALID, "bp_ctx_set_stream: null context");
+    cudaStream_t next = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+    if (next == c->stream) return BP_OK;
+    // device blocks released by work still pending on the old stream go back
+    // to the context's cache; work on the new stream may take them, so the
+    // old stream's work must be finished first
+    DeviceGuard g(c->device);
+    BP_CUDA(cudaStreamSynchronize(c->stream));
+    c->stream = next;
+    return BP_OK;
+  });
 }
 
 BP_API int32_t bp_ctx_memory(bp_ctx ctx, uint64_t* used, uint64_t* budget) {
@@ -228,6 +241,7 @@ BP_API int32_t bp_problem_create(bp_ctx ctx, const bp_patches* pp, const bp_para
     DeviceGuard g(c->device);
     auto P = std::make_unique<Problem>();
     P->ctx = c;
+    P->live.attach(c->live_problems);
     P->n = n;
     P->params = *prm;
     P->fp64 = prm->precision == BP_PREC_FP64;
@@ -265,6 +279,7 @@ BP_API int32_t bp_mesh_create(bp_ctx ctx, const bp_patches* pp, const double cen
     DeviceGuard g(c->device);
     auto m = std::make_unique<DevMesh>();
     m->ctx = c;
+    m->live.attach(c->live_meshes);
     m->n = n;
     for (int k = 0; k < 3; ++k) {
       if (!std::isfinite(centre[k])) return fail(BP_ERR_INVALID, "bp_mesh_create: non-finite centre");
@@ -334,6 +349,7 @@ BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int3
     DeviceGuard g(c->device);
     auto P = std::make_unique<Problem>();
     P->ctx = c;
+    P->live.attach(c->live_problems);
     P->n = (int)n_total;
     P->params = *prm;
     P->fp64 = prm->precision == BP_PREC_FP64;

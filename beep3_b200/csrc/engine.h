@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <iterator>
 #include <map>
@@ -80,6 +81,9 @@ struct Ctx {
   uint64_t releases = 0;
   std::mutex mu;
   int sm_count = 148;
+  // problems and meshes made on the context and not yet deleted: the
+  // context may not be destroyed under them
+  std::atomic<int> live_problems{0}, live_meshes{0};
   // released blocks beyond this are freed at once, the longest unused first
   static constexpr uint64_t kCacheMax = 16ull << 30;
 
@@ -140,6 +144,23 @@ struct Ctx {
     for (auto& kv : cache) cudaFree(kv.second.p);
     cache.clear();
     cached = 0;
+  }
+};
+
+// Counts one live object on its context from attach() until destruction.
+// Declared as the first member of the object, so it is destroyed last, after
+// the object's device buffers have gone back to the context.
+struct LiveToken {
+  std::atomic<int>* counter = nullptr;
+  void attach(std::atomic<int>& c) {
+    counter = &c;
+    ++c;
+  }
+  LiveToken() = default;
+  LiveToken(const LiveToken&) = delete;
+  LiveToken& operator=(const LiveToken&) = delete;
+  ~LiveToken() {
+    if (counter) --*counter;
   }
 };
 
@@ -245,6 +266,7 @@ struct NearField {
 // A mesh's node patches in its own frame, checked and uploaded once
 // (bp_mesh_create); instances of it are placed on the device.
 struct DevMesh {
+  LiveToken live;  // first member: destroyed last
   Ctx* ctx = nullptr;
   int n = 0;
   double centre[3] = {0, 0, 0};
@@ -293,6 +315,7 @@ struct FmmState;  // far-field state (fmm.cu)
 void fmm_destroy(FmmState*);
 
 struct Problem {
+  LiveToken live;  // first member: destroyed last
   Ctx* ctx = nullptr;
   int n = 0;
   bp_params params{};

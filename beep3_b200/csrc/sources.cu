@@ -84,9 +84,10 @@ __global__ void point_potential_kernel(const double* __restrict__ pts, int npts,
   if (active) {
     const double w = pts[6 * (size_t)npts + p];
     const double nx = pts[3 * (size_t)npts + p], ny = pts[4 * (size_t)npts + p], nz = pts[5 * (size_t)npts + p];
-    const double a0 = add ? add[2 * k] : 0.0, a1 = add ? add[2 * k + 1] : 0.0;
-    out[2 * k] = w * phi * scale + a0;
-    out[2 * k + 1] = w * (gx * nx + gy * ny + gz * nz) * scale + a1;
+    const size_t o = 2 * (size_t)k;
+    const double a0 = add ? add[o] : 0.0, a1 = add ? add[o + 1] : 0.0;
+    out[o] = w * phi * scale + a0;
+    out[o + 1] = w * (gx * nx + gy * ny + gz * nz) * scale + a1;
   }
 }
 
@@ -184,15 +185,19 @@ __global__ void __launch_bounds__(kThreads) point_potential_fast_kernel(const do
 }
 
 // Per-patch sums of the per-point values (fixed order: deterministic).
-__global__ void sum_points_kernel(const int32_t* __restrict__ off, int first, int count, int pt_base,
+// vals holds n_vals points starting at point pt_base; a patch's offsets are
+// clamped to that range, so offsets that do not describe the list (not
+// non-decreasing, or past its end) never read outside it.
+__global__ void sum_points_kernel(const int32_t* __restrict__ off, int first, int count, int pt_base, int n_vals,
                                   const double* __restrict__ vals, double* __restrict__ a, double* __restrict__ b) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= count) return;
   const int i = first + k;
+  const int lo = max(off[i] - pt_base, 0), hi = min(off[i + 1] - pt_base, n_vals);
   double s0 = 0, s1 = 0;
-  for (int p = off[i]; p < off[i + 1]; ++p) {
-    s0 += vals[2 * (p - pt_base)];
-    s1 += vals[2 * (p - pt_base) + 1];
+  for (int p = lo; p < hi; ++p) {
+    s0 += vals[2 * (size_t)p];
+    s1 += vals[2 * (size_t)p + 1];
   }
   a[k] = s0;
   b[k] = s1;
@@ -216,7 +221,7 @@ void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps
                                                  vals.as<double>(), nullptr);
   BP_LAUNCH_CHECK();
   sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
-      P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
+      P.d_qual_off.as<int32_t>(), 0, P.n, 0, nq, vals.as<double>(), rhs_dev, rhs_dev + P.n);
   BP_LAUNCH_CHECK();
   BP_CUDA(cudaStreamSynchronize(ctx->stream));
 }
@@ -314,7 +319,7 @@ void rhs_posed_device(Problem& P, const double* const* charges_host, const int32
                            vals.as<double>() + 2 * (size_t)pl.q_begin, self, st);
   }
   sum_points_kernel<<<(P.n + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-      P.d_qual_off.as<int32_t>(), 0, P.n, 0, vals.as<double>(), rhs_dev, rhs_dev + P.n);
+      P.d_qual_off.as<int32_t>(), 0, P.n, 0, nq, vals.as<double>(), rhs_dev, rhs_dev + P.n);
   BP_LAUNCH_CHECK();
   BP_CUDA(cudaStreamSynchronize(st));
 }
@@ -332,7 +337,7 @@ void energy_coefficients_device(Problem& P, int first, int count, const double* 
   }
   // vals[2p] -> ec_h (potential), vals[2p+1] -> ec_f (normal field)
   sum_points_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(
-      P.d_gal_off.as<int32_t>(), first, count, p0, vals.as<double>(), ch_dev, cf_dev);
+      P.d_gal_off.as<int32_t>(), first, count, p0, p1 - p0, vals.as<double>(), ch_dev, cf_dev);
   BP_LAUNCH_CHECK();
   BP_CUDA(cudaStreamSynchronize(ctx->stream));
 }
@@ -398,6 +403,21 @@ extern "C" BP_API int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_
       return fail(BP_ERR_INVALID, "bp_rhs_noalloc: " + std::to_string(n_qual_points) +
                                       " qualocation points exceed the fixed scratch of " +
                                       std::to_string(kNoAllocMaxPoints) + " points");
+    // the scratch array used is the current device's: every buffer must be
+    // on that device
+    int dev = -1;
+    BP_CUDA(cudaGetDevice(&dev));
+    const void* bufs[4] = {qual_offsets_dev, qual_points_soa_dev, rhs_dev, n_charges > 0 ? charges_xyzq_dev : nullptr};
+    for (const void* b : bufs) {
+      if (!b) continue;
+      cudaPointerAttributes at{};
+      if (cudaPointerGetAttributes(&at, b) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BP_ERR_INVALID, "bp_rhs_noalloc: a buffer is not CUDA memory");
+      }
+      if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != dev)
+        return fail(BP_ERR_INVALID, "bp_rhs_noalloc: every buffer must be device memory of the current device");
+    }
     double* scratch = noalloc_scratch_for_current_device();
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     const double scale = kOneOver4Pi / eps_solvent;
@@ -405,7 +425,7 @@ extern "C" BP_API int32_t bp_rhs_noalloc(int32_t n_patches, const int32_t* qual_
         qual_points_soa_dev, n_qual_points, 0, n_qual_points, charges_xyzq_dev, n_charges, scale, scratch, nullptr);
     BP_LAUNCH_CHECK();
     sum_points_kernel<<<(n_patches + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-        qual_offsets_dev, 0, n_patches, 0, scratch, rhs_dev, rhs_dev + n_patches);
+        qual_offsets_dev, 0, n_patches, 0, n_qual_points, scratch, rhs_dev, rhs_dev + n_patches);
     BP_LAUNCH_CHECK();
     return BP_OK;
   });

@@ -1,8 +1,11 @@
 """Serving loop: continuous batching of BEM solves on one GPU.
 
 Requests (one molecule each: surface + charges + kappa) arrive over time.
-A request is admitted as soon as a worker slot is free and its estimated
-device footprint fits in the server's HBM budget; admitted requests run
+A request is admitted as soon as a worker slot is free and its device
+footprint fits in the server's HBM budget: the footprint measured on an
+earlier request of the same size and settings (the engine context's live
+device bytes once the problem is built and solved), or, for a size not seen
+yet, an upper estimate as the first guess; admitted requests run
 concurrently, each on its own engine context (own CUDA stream), so their
 kernels overlap on the device while later requests wait in the queue.
 Device state (tree, near-field coefficients, FMM expansions, Krylov basis)
@@ -97,6 +100,8 @@ class BemServer:
         self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         self._closed = False
         self.peak_in_use = 0
+        # measured device bytes per (patches, precision, nbsize, kappa > 0)
+        self.measured_bytes: dict[tuple, int] = {}
         self._dispatcher.start()
 
     # -------------------------------------------------------------- public
@@ -114,6 +119,16 @@ class BemServer:
             c.close()
         self._contexts = []
 
+    def _key(self, req: SolveRequest) -> tuple:
+        return (req.mesh.n_patches, self.precision, self.nbsize, req.kappa > 0)
+
+    def footprint(self, req: SolveRequest) -> int:
+        """Device bytes reserved for a request: the largest measured on an
+        earlier request of the same key, else the estimator's guess."""
+        with self._lock:
+            m = self.measured_bytes.get(self._key(req))
+        return int(m) if m is not None else int(self.estimator(req))
+
     # -------------------------------------------------------------- internals
     def _dispatch(self) -> None:
         while True:
@@ -121,7 +136,7 @@ class BemServer:
             if item is None:
                 return
             req, fut = item
-            need = min(int(self.estimator(req)), self.budget)
+            need = min(self.footprint(req), self.budget)
             with self._lock:
                 # FIFO admission: wait for a slot and for budget to free up
                 while self._slots == 0 or self._in_use + need > self.budget:
@@ -160,15 +175,21 @@ class BemServer:
                 self._contexts.append(ectx)
 
     def _run(self, req: SolveRequest, fut: Future, need: int) -> None:
+        res = None
         try:
-            fut.set_result(self.runner(req, need))
+            res = self.runner(req, need)
         except BaseException as exc:  # reported through the future
             fut.set_exception(exc)
         finally:
             with self._lock:
+                if res is not None and res.device_bytes > 0:
+                    k = self._key(req)
+                    self.measured_bytes[k] = max(self.measured_bytes.get(k, 0), int(res.device_bytes))
                 self._slots += 1
                 self._in_use -= need
                 self._lock.notify_all()
+        if res is not None:
+            fut.set_result(res)
 
 
 def latency_percentiles(results: list[SolveResult]) -> dict:

@@ -63,8 +63,14 @@ int32_t bp_abi_version(void);
  * budget (src/opencl/opencl_handler.cpp:19-147, :397-462).
  */
 int32_t bp_ctx_create(int32_t device, uint64_t hbm_budget_bytes, bp_ctx* out);
+/* Destroy problems and meshes first: while any made on the context is alive
+ * (a mesh whose deletion waits for its last posed problem included) this
+ * returns BP_ERR_INVALID and the context stays valid. */
 int32_t bp_ctx_destroy(bp_ctx ctx);
-int32_t bp_ctx_set_stream(bp_ctx ctx, void* cuda_stream); /* cudaStream_t; NULL = the context's own */
+/* cudaStream_t; NULL = the context's own.  Work already issued on the
+ * previous stream is waited for before the switch, so device blocks it
+ * releases are never handed to work on the new stream while still in use. */
+int32_t bp_ctx_set_stream(bp_ctx ctx, void* cuda_stream);
 int32_t bp_ctx_memory(bp_ctx ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
 /* Device blocks of destroyed problems that the context keeps for the next
  * problem of similar size (no cudaMalloc / cudaFree between poses): their
@@ -247,7 +253,14 @@ int32_t bp_rhs_posed(bp_problem p, const double* const* charges_xyzq, const int3
  * [n][4], rhs [2 n_patches]) and the kernels' per-point scratch is a fixed
  * 16 MiB array in the library, held on every GPU that loads it until exit.
  * At most 1048576 qualocation points per call (larger calls return
- * BP_ERR_INVALID).  The first call on a device looks the array up (do it
+ * BP_ERR_INVALID).  The call runs on the calling thread's current device,
+ * whose copy of the array it uses: every buffer must be device memory of
+ * that device (else BP_ERR_INVALID), and cuda_stream a stream of it.
+ * qual_offsets_dev must describe the point list: offsets[0] == 0,
+ * non-decreasing, offsets[n_patches] == n_qual_points (the offsets are read
+ * on the device only; a patch's range is clamped to [0, n_qual_points), so
+ * offsets that break this give wrong sums but no out-of-bounds access).
+ * The first call on a device looks the array up (do it
  * before any stream capture); calls that overlap on the GPU share the array
  * and race, so the caller serialises them.  Ordered on cuda_stream (NULL =
  * the legacy default stream), no host synchronisation. */

@@ -68,3 +68,23 @@ def test_errors_propagate():
     with pytest.raises(RuntimeError):
         f2.result(timeout=10)
     srv.close()
+
+
+def test_measured_footprint_replaces_the_estimate():
+    """A size seen before is admitted by the device bytes its earlier request
+    really held, not by the estimator's guess (which here undercounts)."""
+    needs = []
+
+    def runner(req, need):
+        needs.append(need)
+        start = time.perf_counter()
+        return SolveResult(req.tag, 0.0, 1, True, req.mesh.n_patches, 3 * req.mesh.n_patches, req.arrival, start,
+                           time.perf_counter())
+
+    srv = BemServer(hbm_budget_bytes=10_000, workers=1, runner=runner, estimator=lambda r: r.mesh.n_patches)
+    srv.submit(SolveRequest(FakeMesh(100), 0.1)).result(timeout=10)
+    assert srv.footprint(SolveRequest(FakeMesh(100), 0.1)) == 300
+    srv.submit(SolveRequest(FakeMesh(100), 0.1)).result(timeout=10)
+    srv.submit(SolveRequest(FakeMesh(50), 0.1)).result(timeout=10)  # unseen size: the estimate
+    srv.close()
+    assert needs == [100, 300, 50]
