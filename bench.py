@@ -212,30 +212,119 @@ def stage_profile(bp, x, y, reps: int = 5):
     return ms, launches
 
 
-def cpu_baseline(bp, budget_s: float = 15.0) -> dict:
-    """The oracle (restated reference CPU matvec: cached near-field stream +
-    plane-wave FMM) timed on this host on a bounded sample."""
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def oracle_timings(arr, tree, charges, kappa: float, edge: float, nterms: int, eps_solvent: float,
+                   matvec_budget_s: float, steps: int | None = None, warmup: int = 0) -> dict:
+    """The reference's CPU path restated by the oracle (-march=native build,
+    OpenMP over the loops the reference parallelises), timed on this host:
+    the near-field precalc (once), matvecs (``steps`` of them after
+    ``warmup``, or as many as fit in ``matvec_budget_s``), and one full solve
+    with its right-hand side timed apart.  Returns the timings and the
+    oracle problem (the caller closes it)."""
     import oracle as O
-    threads = os.cpu_count() or 1
-    arr = bp.gathered()
-    centre, edge = bp.calculate_bounding_cube()
+    O.use_native()
     t0 = time.perf_counter()
-    pr = O.Problem(arr, bp.host_tree(), bp.kappa, fp32=True, cube_edge=edge, nterms=bp.nterms)
-    setup_s = time.perf_counter() - t0
+    pr = O.Problem(arr, tree, kappa, fp32=True, cube_edge=edge, nterms=nterms)
+    precalc_s = time.perf_counter() - t0
     x = np.random.default_rng(5).standard_normal(2 * pr.n)
-    reps, spent = 0, 0.0
-    while spent < budget_s and reps < 1000:
+    for _ in range(warmup):
+        pr.matvec(x)
+    times = []
+    while (len(times) < steps) if steps else (sum(times) < matvec_budget_s and len(times) < 1000):
         t = time.perf_counter()
         pr.matvec(x)
-        spent += time.perf_counter() - t
-        reps += 1
-    pr.close()
-    return {"value": reps / spent, "unit": "matvec/s", "cores": threads, "kind": "port",
-            "sample": f"{reps} oracle matvecs of the full workload ({spent:.1f} s; near-field precalc "
-                      f"{setup_s:.1f} s excluded, as in BEEP::benchmark)"}
+        times.append(time.perf_counter() - t)
+    t = time.perf_counter()
+    rhs = O.rhs(pr.patches, charges, eps_solvent)
+    rhs_s = time.perf_counter() - t
+    t = time.perf_counter()
+    xs, its, rr = pr.solve(rhs, 1e-6, 100)
+    gmres_s = time.perf_counter() - t
+    return dict(problem=pr, x=x, rhs=rhs, solution=xs, iterations=its, precalc_s=precalc_s, matvec_s=times,
+                rhs_s=rhs_s, gmres_s=gmres_s)
+
+
+def cpu_record(t: dict, kind: str = "port") -> dict:
+    mv = len(t["matvec_s"]) / sum(t["matvec_s"])
+    return {"value": mv, "unit": "matvec/s", "cores": cpu_threads(), "kind": kind,
+            "sample": f"{len(t['matvec_s'])} matvecs of the full workload ({sum(t['matvec_s']):.1f} s) by the "
+                      f"oracle's restatement of the reference CPU path (cached FP32 near field + FP64 plane-wave "
+                      f"FMM, OpenMP, -O3 -march=native); near-field precalc, right-hand side and GMRES timed once",
+            "matvec_ms": 1e3 / mv, "precalc_s": t["precalc_s"], "rhs_s": t["rhs_s"], "gmres_s": t["gmres_s"],
+            "gmres_iterations": t["iterations"], "solves_per_s": 1.0 / (t["rhs_s"] + t["gmres_s"]),
+            "solves_per_s_gmres_only": 1.0 / t["gmres_s"],
+            "note": "the right-hand side is a direct FP64 sum (the reference's is a 6-figure FMM); "
+                    "solves_per_s counts right-hand side + GMRES on a built problem, as the engine's does"}
+
+
+def cpu_baseline_and_parity(bp, bp64, budget_s: float = 12.0) -> tuple[dict, dict]:
+    """CPU baseline on the benchmark's problem (same tree and inputs), and the
+    engines' parity against the oracle on it: the mixed engine against the
+    reference-faithful oracle (matvec, solved f/h, energy), and both engines'
+    matvec rows against the FP64 direct-sum oracle on 1024 targets."""
+    import oracle as O
+    arr = bp.gathered()
+    tree = bp.host_tree()
+    _, edge = bp.calculate_bounding_cube()
+    inst = bp.instances[0]
+    t = oracle_timings(arr, tree, inst.charges, bp.kappa, edge, bp.nterms, bp.eps_solvent, budget_s)
+    pr, x = t["problem"], t["x"]
+    n = pr.n
+    try:
+        yo = pr.matvec(x)
+        ym, y64 = bp.matvec(x), bp64.matvec(x)
+        ecf, ech = O.energy_coefficients(arr["gal_off"], arr["gal"], arr["area"], inst.charges,
+                                         inst.mesh.patches.total_area)
+        xo = t["solution"]
+        eo = O.energy(xo[:n], xo[n:], ecf, ech, inst.dielectric_ratio)
+        em, _ = bp.calculate_energies()
+        targets = np.random.default_rng(6).choice(n, 1024, replace=False)
+        ex = O.exact_rows(arr, tree, bp.kappa, x, targets)
+        mf, mh = O.row_errors(ym, ex, targets, n)
+        df, dh = O.row_errors(y64, ex, targets, n)
+        of, oh = O.row_errors(yo, ex, targets, n)
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        parity = {
+            "error_vs_oracle": {
+                "what": "mixed engine against the oracle (the reference's CPU path restated: FP32 near-field "
+                        "coefficients, FP64 FMM) on the same tree and inputs",
+                "matvec_rel_l2": rel(ym, yo), "solution_f_rel_l2": rel(bp.x[:n], xo[:n]),
+                "solution_h_rel_l2": rel(bp.x[n:], xo[n:]), "energy_rel": abs(em - eo) / abs(eo),
+                "gmres_iterations_oracle": t["iterations"]},
+            "error_vs_direct": {
+                "what": "matvec rows on 1024 random target patches against the FP64 direct-sum oracle (every "
+                        "near pair in FP64, far field summed exactly): the order-9 FMM's truncation",
+                "mixed_f": mf, "mixed_h": mh, "fp64_f": df, "fp64_h": dh, "oracle_fmm_f": of, "oracle_fmm_h": oh}}
+    finally:
+        pr.close()
+    return cpu_record(t), parity
 
 
 # --------------------------------------------------------------------------- arms
+def prepare_inputs(name: str, path: str) -> None:
+    """Writes the workload's gathered patch arrays, charges and bounding cube
+    to ``path`` (npz).  Run in a child process of the reference arm, so the
+    reference arm's own process never loads the engine library (the surface
+    point generation is the engine's host geometry code)."""
+    desc, meshes, kappa, nbsize = workload(name)
+    import beep3_b200 as b
+    bp = b.BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision="mixed")
+    for mesh, off, q in meshes:
+        bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
+    arr = bp.gathered()
+    centre, edge = bp.calculate_bounding_cube()
+    charges = np.concatenate([i.charges for i in bp.instances])
+    np.savez(path, **{k: v for k, v in arr.items() if k != "first"}, charges=charges, centre=centre,
+             edge=edge, kappa=kappa, nbsize=nbsize, nterms=bp.nterms, eps_solvent=bp.eps_solvent,
+             desc=json.dumps(desc))
+
+
 def run_reference(args):
     world, rank, local, dist = dist_setup(args)
     if rank != 0:
@@ -244,33 +333,32 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the matvec workloads only"}),
               flush=True)
         return
-    desc, meshes, kappa, nbsize = workload(args.workload)
-    import beep3_b200 as b  # geometry preparation (host) only
-    bp = b.BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision="mixed")
-    for mesh, off, q in meshes:
-        bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
-    import oracle as O
-    arr = bp.gathered()
-    centre, edge = bp.calculate_bounding_cube()
-    pr = O.Problem(arr, bp.host_tree(), kappa, fp32=True, cube_edge=edge, nterms=bp.nterms)
-    x = np.random.default_rng(5).standard_normal(2 * pr.n)
-    for _ in range(args.warmup):
-        pr.matvec(x)
-    times = []
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        pr.matvec(x)
-        times.append(time.perf_counter() - t)
-    tot = sum(times)
-    val = args.steps / tot
-    threads = os.cpu_count() or 1
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "inputs.npz")
+        subprocess.run([sys.executable, str(Path(__file__).resolve()), "--prepare-inputs", path, "--workload",
+                        args.workload], check=True)
+        z = np.load(path)
+        arr = {k: z[k] for k in ("centroid", "normal", "area", "eps", "gc", "qual_off", "qual", "quad_off", "quad",
+                                 "gal_off", "gal")}
+        charges, centre, edge = z["charges"], z["centre"], float(z["edge"])
+        kappa, nbsize, nterms = float(z["kappa"]), int(z["nbsize"]), int(z["nterms"])
+        eps_solvent, desc = float(z["eps_solvent"]), json.loads(str(z["desc"]))
+    from oracle import tree as OT
+    tree = OT.build(arr["centroid"], centre, edge, nbsize)
+    t = oracle_timings(arr, tree, charges, kappa, edge, nterms, eps_solvent, 0.0, steps=args.steps,
+                       warmup=args.warmup)
+    t["problem"].close()
+    rec = cpu_record(t)
+    val = rec["value"]
+    tot = sum(t["matvec_s"])
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "matvec/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32/fp64",
-            "data": "synthetic", "config": desc,
-            "cpu_baseline": {"value": val, "unit": "matvec/s", "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} oracle matvecs of the full workload"},
-            "e2e": {"value": val, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 near field/fp64 FMM",
+            "data": "synthetic", "config": desc, "cpu_baseline": rec,
+            "e2e": {"value": val, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "engine_library_loaded": any("libbeep3_b200" in ln for ln in Path("/proc/self/maps").read_text()
+                                         .splitlines())}
     print(json.dumps(line), flush=True)
 
 
@@ -483,7 +571,8 @@ def _run_ours(args, world, rank, local, dist):
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(bp)
+        line["cpu_baseline"], parity = cpu_baseline_and_parity(bp, bp64)
+        line.update(parity)
     if rank == 0:
         print(json.dumps(line), flush=True)
     bp.close()
@@ -507,7 +596,11 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--prepare-inputs", metavar="NPZ", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.prepare_inputs:
+        prepare_inputs(args.workload, args.prepare_inputs)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -123,7 +123,8 @@ typedef struct {
   double cube_centre[3];  /* bounding cube (BEEP::calculate_bounding_cube) */
   double cube_edge;
   int32_t nbsize;         /* target mean neighbourhood size of the adaptive tree */
-  int32_t nterms;         /* FMM order; 9 (reference matvec order) or 18 */
+  int32_t nterms;         /* FMM order: 9, the reference's matvec order (FMM_BEM_Octree<9,9,67>);
+                             other orders return BP_ERR_UNSUPPORTED */
   int32_t precision;      /* enum bp_precision */
   int32_t flags;          /* reserved, 0 */
 } bp_params;

@@ -20,15 +20,45 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
 
 _lib = None
+_native = False
 
 
-def build() -> Path:
-    srcs = list(HERE.glob("*.cpp")) + list(HERE.glob("*.h"))
-    if not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
-        res = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+def _cpu_tag() -> str:
+    """Identifies this host's CPU (model and instruction-set flags)."""
+    import hashlib
+    try:
+        text = Path("/proc/cpuinfo").read_text()
+    except OSError:
+        text = ""
+    keep = [ln for ln in text.splitlines() if ln.startswith(("model name", "flags"))][:2]
+    return hashlib.sha1("\n".join(keep).encode()).hexdigest()[:12]
+
+
+def native_lib_path() -> Path:
+    return HERE / "_build" / f"native-{_cpu_tag()}" / "liboracle.so"
+
+
+def build(native: bool = False) -> Path:
+    """Builds the portable library, or with ``native`` the -march=native one
+    for this host's CPU (the timed CPU baseline)."""
+    out = native_lib_path() if native else LIB
+    srcs = list(HERE.glob("*.cpp")) + list(HERE.glob("*.h")) + [HERE / "Makefile"]
+    if not out.exists() or any(s.stat().st_mtime > out.stat().st_mtime for s in srcs):
+        cmd = ["make", "-C", str(HERE)]
+        if native:
+            cmd += ["native", f"NATIVE_DIR={out.parent.relative_to(HERE)}"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError("oracle build failed:\n" + res.stdout + res.stderr)
-    return LIB
+    return out
+
+
+def use_native() -> None:
+    """Makes lib() load the -march=native build (call before the first use)."""
+    global _native
+    if _lib is not None and not _native:
+        raise RuntimeError("the portable oracle library is already loaded")
+    _native = True
 
 
 class OrPatches(C.Structure):
@@ -47,8 +77,7 @@ MATVEC_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_d
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        build()
-        L = C.CDLL(str(LIB))
+        L = C.CDLL(str(build(native=_native)))
         P = C.c_void_p
         L.or_pair_coefficients.argtypes = [C.POINTER(OrPatches), C.c_int, P, P, C.c_double, C.c_int, P]
         L.or_singular.argtypes = [C.POINTER(OrPatches), C.c_double, C.c_int, P]
@@ -172,6 +201,90 @@ def energy(f, h, ecf, ech, eps_ratio: float) -> float:
         comp = (t - s) - y
         s = t
     return s * 0.5 * CONVERT_KJ_PER_MOL
+
+
+def far_pairs(tree: dict, n: int, targets) -> tuple[np.ndarray, np.ndarray]:
+    """(target, source) pairs outside each target leaf's 27-box neighbourhood
+    (the complement of the cached near field, Octree::get_neighbourhood_contents,
+    src/fmm/octree.h:618-650), grouped by target."""
+    info, contents = tree["info"], tree["contents"]
+    neigh = neighbours_from_info(info)
+    leaf_of = np.full(n, -1)
+    for k, r in enumerate(info):
+        if r[4] & 2:
+            leaf_of[contents[r[6]:r[6] + r[7]]] = k
+    T, S = [], []
+    for t in targets:
+        near = np.zeros(n, bool)
+        for m in neigh[leaf_of[t]]:
+            if m >= 0:
+                near[contents[info[m, 6]:info[m, 6] + info[m, 7]]] = True
+        s = np.nonzero(~near)[0]
+        T.append(np.full(len(s), t))
+        S.append(s)
+    return np.concatenate(T).astype(np.int32), np.concatenate(S).astype(np.int32)
+
+
+def direct_far(arrays: dict, tree: dict, kappa: float, x, targets, beta0: float = 1e-10) -> np.ndarray:
+    """The exact far field at the targets (2N vector, zero elsewhere): the
+    12-channel sum over every far pair that the plane-wave FMM approximates
+    (the method of src/fmm/test_fmm.cpp:181-214).  Targets must be distinct."""
+    pt = Patches(arrays)
+    T, S = far_pairs(tree, pt.n, targets)
+    x = _c(x)
+    y = np.zeros(2 * pt.n)
+    lib().or_fmm_direct(C.byref(pt.s), kappa, beta0, len(T), _p(T), _p(S), _p(x), _p(y))
+    return y
+
+
+def exact_rows(arrays: dict, tree: dict, kappa: float, x, targets, beta0: float = 1e-10) -> np.ndarray:
+    """FP64 direct-sum oracle of the matvec rows of the targets (2N vector,
+    zero elsewhere): the same discretisation with every near-field pair
+    integrated in FP64 (the singular diagonal included) and the far field
+    summed directly instead of by the FMM."""
+    pt = Patches(arrays)
+    n = pt.n
+    tg = np.asarray(targets, np.int64)
+    info, contents = tree["info"], tree["contents"]
+    neigh = neighbours_from_info(info)
+    leaf_of = np.full(n, -1)
+    for k, r in enumerate(info):
+        if r[4] & 2:
+            leaf_of[contents[r[6]:r[6] + r[7]]] = k
+    I, J = [], []
+    for t in tg:
+        cols = [contents[info[m, 6]:info[m, 6] + info[m, 7]] for m in neigh[leaf_of[t]] if m >= 0]
+        cols = np.concatenate(cols)
+        cols = cols[cols != t]
+        I.append(np.full(len(cols), t))
+        J.append(cols)
+    I = np.concatenate(I).astype(np.int32)
+    J = np.concatenate(J).astype(np.int32)
+    coef = pair_coefficients(pt, I, J, kappa, fp32=False)
+    x = _c(x)
+    y = direct_far(arrays, tree, kappa, x, tg, beta0)
+    f, h = x[:n], x[n:]
+    np.add.at(y, I, coef[:, 1] * f[J] - coef[:, 0] * h[J])
+    np.add.at(y, n + I, coef[:, 3] * f[J] - coef[:, 2] * h[J])
+    # singular self-patch terms with the geometric corrections, targets only
+    sub = {k: np.asarray(arrays[k])[tg] for k in ("centroid", "normal", "area", "eps", "gc")}
+    for key, pts in (("qual", "qual_off"), ("quad", "quad_off"), ("gal", "gal_off")):
+        off = np.asarray(arrays[pts])
+        pieces = [np.asarray(arrays[key])[off[t]:off[t + 1]] for t in tg]
+        sub[pts] = np.concatenate([[0], np.cumsum([len(q) for q in pieces])]).astype(np.int32)
+        sub[key] = np.concatenate(pieces)
+    d = singular(Patches(sub), kappa, fp32=False)
+    y[tg] += d[:, 1] * f[tg] - d[:, 0] * h[tg]
+    y[n + tg] += d[:, 3] * f[tg] - d[:, 2] * h[tg]
+    return y
+
+
+def row_errors(y, ref, targets, n) -> tuple[float, float]:
+    """Relative L2 error of the f rows and of the h rows over the targets."""
+    t = np.asarray(targets)
+    ef = np.linalg.norm(y[t] - ref[t]) / np.linalg.norm(ref[t])
+    eh = np.linalg.norm(y[n + t] - ref[n + t]) / np.linalg.norm(ref[n + t])
+    return float(ef), float(eh)
 
 
 class Problem:

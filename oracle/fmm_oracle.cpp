@@ -892,10 +892,12 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
   auto flags = [&](int k) { return F->I(k)[4]; };
   auto count = [&](int k) { return F->I(k)[7]; };
   auto child = [&](int k, int c) { return F->I(k)[10 + c - 1]; };
-  // P2M at non-empty childless nodes (src/fmm/fmm_bem_hybrid.h:282-335)
-  std::vector<double> p;
+  // P2M at non-empty childless nodes (src/fmm/fmm_bem_hybrid.h:282-335);
+  // nodes in parallel as the reference's patches (src/fmm/fmm.h:1550)
+#pragma omp parallel for schedule(dynamic, 1)
   for (int k = 0; k < nn; ++k) {
     if ((flags(k) & 1) || count(k) == 0) continue;
+    std::vector<double> p;
     const int lev = level_of(k);
     const double* c0 = &F->geom[4 * (size_t)k];
     const int cs = F->I(k)[6], cc = count(k);
@@ -931,17 +933,29 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
       }
     }
   }
-  // M2M upward (src/fmm/fmm_bem_hybrid.h:337-410)
+  // M2M upward (src/fmm/fmm_bem_hybrid.h:337-410).  Parents in parallel
+  // (the reference runs ympshift's channels in parallel, src/fmm/fmm.h:1801);
+  // each parent takes its children in node order, as the serial loop does.
   for (int lev = bottom; lev > 0; --lev) {
+    std::vector<int> parents;
+    std::vector<std::vector<int>> kids(nn);
     for (int k = 0; k < nn; ++k) {
       if (level_of(k) != lev || count(k) == 0) continue;
       const int par = F->I(k)[5];
-      const int32_t* ik = F->I(k);
-      int id = 1 + (ik[1] & 1) + 2 * (ik[2] & 1) + 4 * (ik[3] & 1);
-      const Rot& rd = (id > 4) ? F->G.rdmsq3 : F->G.rdsq3;
-      for (int ch = 0; ch < 12; ++ch) {
-        const LevelGlobals& LGl = ch < 8 ? F->LG[lev] : F->LG0[lev];
-        shift(NT, id, true, M[k][ch], M[par][ch], LGl.mpshift, LGl, rd);
+      if (kids[par].empty()) parents.push_back(par);
+      kids[par].push_back(k);
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int pi = 0; pi < (int)parents.size(); ++pi) {
+      const int par = parents[pi];
+      for (int k : kids[par]) {
+        const int32_t* ik = F->I(k);
+        int id = 1 + (ik[1] & 1) + 2 * (ik[2] & 1) + 4 * (ik[3] & 1);
+        const Rot& rd = (id > 4) ? F->G.rdmsq3 : F->G.rdsq3;
+        for (int ch = 0; ch < 12; ++ch) {
+          const LevelGlobals& LGl = ch < 8 ? F->LG[lev] : F->LG0[lev];
+          shift(NT, id, true, M[k][ch], M[par][ch], LGl.mpshift, LGl, rd);
+        }
       }
     }
   }
@@ -952,6 +966,8 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
     const int npA = A.nexptotp, npB = B.nexptotp;
     // waves[node][dir][ch] for non-empty nodes at lev+1
     std::vector<std::vector<cd>> waves(nn);
+    // multipole -> six plane waves per node in parallel (src/fmm/fmm.h:2376)
+#pragma omp parallel for schedule(dynamic, 1)
     for (int k = 0; k < nn; ++k) {
       if (level_of(k) != lev + 1 || count(k) == 0) continue;
       waves[k].assign(6 * 12 * (size_t)std::max(npA, npB), cd(0));
@@ -968,6 +984,10 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
       }
     }
     const size_t W = std::max(npA, npB);
+    // interaction lists and wave -> local conversion per parent in parallel
+    // (src/fmm/fmm_octree.h:169, src/fmm/fmm.h:1616, :1676, :2407); a parent
+    // writes only its own children's locals
+#pragma omp parallel for schedule(dynamic, 1)
     for (int k = 0; k < nn; ++k) {
       if (level_of(k) != lev) continue;
       if ((flags(k) & 2) || (flags(k) & 4)) continue;  // leaf or shadow
@@ -1020,8 +1040,10 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
       }
     }
   }
-  // L2L (src/fmm/fmm_bem_hybrid.h:412-439, :86-124)
+  // L2L (src/fmm/fmm_bem_hybrid.h:412-439, :86-124), parents in parallel
+  // (each child has one parent)
   for (int lev = 0; lev < bottom; ++lev) {
+#pragma omp parallel for schedule(dynamic, 1)
     for (int k = 0; k < nn; ++k) {
       if (level_of(k) != lev) continue;
       if (!(flags(k) & 1) || (flags(k) & 2)) continue;  // has children and not leaf
@@ -1036,14 +1058,15 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
       }
     }
   }
-  // L2P at leaf patch centroids (src/fmm/fmm_bem_hybrid.h:583-642)
+  // L2P at leaf patch centroids (src/fmm/fmm_bem_hybrid.h:583-642; the
+  // reference's patches in parallel, :606), leaves in parallel
+#pragma omp parallel for schedule(dynamic, 1)
   for (int k = 0; k < nn; ++k) {
     if (!(flags(k) & 2)) continue;
     const int lev = level_of(k);
     const double s = get_scale(F->beta, F->edge, lev), s0 = get_scale(F->beta0, F->edge, lev);
     const double* c0 = &F->geom[4 * (size_t)k];
     const int cs = F->I(k)[6], cc = count(k);
-#pragma omp parallel for schedule(dynamic, 4)
     for (int t = 0; t < cc; ++t) {
       const int i = F->contents[cs + t];
       eval_patch(NT, F->beta, F->beta0, s, s0, P->centroid + 3 * (size_t)i, c0, Lc[k], P->normal + 3 * (size_t)i,
@@ -1055,11 +1078,20 @@ void or_fmm_apply(OrFmm* F, const double* x, double* y) {
 // Direct 12-channel far field over explicit (target, source) pairs, the sum
 // the FMM approximates: y[t] += FMM_results_to_BEM of the screened /
 // pseudo-Laplace potentials, fields and Hessians at target centroids.
+// Pairs of one target must be contiguous and no target may appear in two
+// runs; runs are summed in parallel, each in pair order.
 void or_fmm_direct(const OrPatches* P, double kappa, double beta0, int npairs, const int32_t* T, const int32_t* S,
                    const double* x, double* y) {
+  std::vector<int> runs;
+  for (int k = 0; k < npairs; ++k)
+    if (k == 0 || T[k] != T[k - 1]) runs.push_back(k);
+  runs.push_back(npairs);
+  const int n_runs = (int)runs.size() - 1;
   const int n = P->n;
   const double beta = kappa < beta0 ? beta0 : kappa;
-  for (int k = 0; k < npairs; ++k) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int ri = 0; ri < n_runs; ++ri)
+  for (int k = runs[ri]; k < runs[ri + 1]; ++k) {
     const int t = T[k], s = S[k];
     double q[12];
     patch_charges(P, s, x[s], x[n + s], q);

@@ -163,6 +163,9 @@ struct OrNear {
   // are float in ref mode, double in exact mode (both stored as double).
   std::vector<int32_t> src, targ;
   std::vector<double> coef;  // 4 per record
+  // records [row_begin[i], row_end[i]) after the n diagonal records are
+  // row i's: a patch is a row of exactly one leaf, whose block is row-major
+  std::vector<int64_t> row_begin, row_end;
 };
 
 extern "C" {
@@ -247,12 +250,18 @@ OrNear* or_near_create(const OrPatches* P, const OrTree* T, double kappa, int fp
     }
     for (int r = 0; r < ccount; ++r) {
       int i = T->contents[cstart + r];
+      nf->row_begin.resize(P->n, 0);
+      nf->row_end.resize(P->n, 0);
+      nf->row_begin[i] = (int64_t)nf->src.size();
       for (int32_t j : cols) {
         nf->src.push_back(i);
         nf->targ.push_back(j);
       }
+      nf->row_end[i] = (int64_t)nf->src.size();
     }
   }
+  nf->row_begin.resize(P->n, 0);
+  nf->row_end.resize(P->n, 0);
   size_t total = nf->src.size() - P->n;
   nf->coef.resize(4 * nf->src.size());
   or_pair_coefficients(P, (int)total, nf->src.data() + P->n, nf->targ.data() + P->n, kappa, fp32,
@@ -266,15 +275,27 @@ int64_t or_near_count(const OrNear* nf) { return (int64_t)nf->src.size(); }
 
 // y_f[src] += B f[targ] - A h[targ] ; y_h[src] += D f[targ] - C h[targ]
 // (src/bem/local_integrations.h:123-130); y is overwritten.
+//
+// The reference streams its cached records serially (CACHE_GPU_RESULTS is
+// defined in the CPU build, src/beep/beep.h:71, so evaluate_local_neighbours
+// runs only the loop at src/beep/beep.cpp:1049-1062).  Here rows run in
+// parallel, each row summing its diagonal record and then its block in the
+// serial loop's order, so the result is the serial result bit for bit.
 void or_near_apply(const OrNear* nf, const double* x, double* y) {
   const int n = nf->n;
-  std::memset(y, 0, sizeof(double) * 2 * (size_t)n);
-  const size_t m = nf->src.size();
-  for (size_t k = 0; k < m; ++k) {
-    const double* c = &nf->coef[4 * k];
-    const int i = nf->src[k], j = nf->targ[k];
-    y[i] += c[1] * x[j] - c[0] * x[n + j];
-    y[n + i] += c[3] * x[j] - c[2] * x[n + j];
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    const double* d = &nf->coef[4 * (size_t)i];
+    double yf = d[1] * x[i] - d[0] * x[n + i];
+    double yh = d[3] * x[i] - d[2] * x[n + i];
+    for (int64_t k = nf->row_begin[i]; k < nf->row_end[i]; ++k) {
+      const double* c = &nf->coef[4 * k];
+      const int j = nf->targ[k];
+      yf += c[1] * x[j] - c[0] * x[n + j];
+      yh += c[3] * x[j] - c[2] * x[n + j];
+    }
+    y[i] = yf;
+    y[n + i] = yh;
   }
 }
 
