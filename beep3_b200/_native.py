@@ -112,6 +112,7 @@ _SIGS = {
     "bp_matvec": [_P, _P, _P],
     "bp_matvec_device": [_P, _P, _P],
     "bp_matvec_profile": [_P, _P, _P, _I, _P, _P, C.POINTER(_I)],
+    "bp_problem_test_wait_timeout": [_P, _I],
     "bp_solve": [_P, _P, _P, _D, _I, _I, C.POINTER(_I), C.POINTER(_D)],
     "bp_solve_device": [_P, _P, _P, _D, _I, _I, C.POINTER(_I), C.POINTER(_D)],
     "bp_rhs": [_P, _P, _I, _D, _P],

@@ -598,6 +598,17 @@ BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, 
   });
 }
 
+BP_API int32_t bp_problem_test_wait_timeout(bp_problem p, int32_t enable) {
+  return guarded_engine([&]() -> int32_t {
+    Problem* P = as_problem(p);
+    if (!P) return fail(BP_ERR_INVALID, "bp_problem_test_wait_timeout: null problem");
+    DeviceGuard g(P->ctx->device);
+    if (!fmm_set_stall_test(*P, enable != 0))
+      return fail(BP_ERR_UNSUPPORTED, "bp_problem_test_wait_timeout: the problem runs no tensor-core FMM kernel");
+    return BP_OK;
+  });
+}
+
 BP_API int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charges, double eps_solvent, double* rhs) {
   return guarded_engine([&]() -> int32_t {
     Problem* P = as_problem(p);

@@ -432,6 +432,9 @@ bool fmm_active(const Problem& P);
 // a bounded wait since the problem was created (its results are then void).
 // Synchronises the context stream.
 void fmm_check_waits(Problem& P);
+// Timeout test switch of the tensor-core FMM kernels (see
+// bp_problem_test_wait_timeout); false when the problem has none.
+bool fmm_set_stall_test(Problem& P, bool on);
 void fmm_setup(Problem& P);
 void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st, cudaStream_t stream);
 void matvec_setup(Problem& P);

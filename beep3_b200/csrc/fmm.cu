@@ -1430,6 +1430,7 @@ constexpr int kHalf = kKC / 4 * kPanel;             // bytes of the operator's h
 // and column chunks, and the column tables
 constexpr int smem_bytes(int nc) { return 2 * (2 * kHalf + 2 * (kKC / 4 * nc * 16)) + 16 * nc; }
 constexpr long long kWaitCycles = 2000000000LL;     // about one second at the boost clock
+constexpr long long kStallCycles = 200000LL;        // bound of the timeout test's wait (about 0.1 ms)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -1452,11 +1453,12 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
       : "memory");
   return ok != 0;
 }
-// bounded wait for a barrier phase; false after about a second
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+// bounded wait for a barrier phase; false after `limit` cycles (by default
+// about a second)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, long long limit = kWaitCycles) {
   const long long t0 = clock64();
   while (!mbar_try(bar, phase))
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
 }
 __device__ __forceinline__ float hi_part(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
@@ -1489,21 +1491,25 @@ __device__ __forceinline__ void ld16(uint32_t taddr, uint32_t (&r)[16]) {
 // issues the MMAs of chunk c, all threads start the operator copy
 // (cp.async) and the column loads (into registers) of chunk c + 1, so the
 // loads overlap the tensor-core work; the columns are split into hi / lo
-// when they are stored.  Every wait is bounded and a timeout sets *err (the
-// kernel still waits, with a bound, for its MMAs and frees its tensor
-// memory).
+// when they are stored.  Every wait is bounded and a timeout sets status[0]
+// (the kernel stops issuing, still waits, with the full bound, for the MMAs
+// it committed, skips its store and frees its tensor memory).  status[1] != 0
+// is the timeout test: the first pipeline step of every CTA also waits, with
+// a short bound, on a barrier that nothing arrives on, so that wait always
+// runs out and the timeout path runs.
 template <int NC>
 __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
     const GemmTile* __restrict__ tiles, const GemmCol* __restrict__ cols, const float* __restrict__ packed,
     int n_mtiles, int n_chunks, int K, int R, int seg, long long seg_stride, const float* __restrict__ X,
-    float* __restrict__ Y, int* __restrict__ err) {
+    float* __restrict__ Y, int* __restrict__ status) {
   static_assert(NC % 32 == 0 && NC >= 32 && NC <= 256, "tile width");
   constexpr int kXHalf = tc::kKC / 4 * NC * 16;     // bytes of the columns' hi (or lo) part of a chunk
   constexpr int kStageB = 2 * tc::kHalf + 2 * kXHalf;
   constexpr int kGroups = NC / 32;                  // 8-column groups per warp
   extern __shared__ __align__(1024) unsigned char smem_tc[];
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bars[3];  // [0], [1]: MMA completion per stage; [2]: never arrived on
   __shared__ uint32_t tmem_slot;
+  const bool stall_test = status[1] != 0;
   long long* dsts = reinterpret_cast<long long*>(smem_tc + 2 * kStageB);  // [NC]
   long long* srcs = dsts + NC;                                            // [NC]
   const GemmTile tl = tiles[blockIdx.x];
@@ -1526,6 +1532,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
   if (tid == 0) {
     tc::mbar_init(&bars[0]);
     tc::mbar_init(&bars[1]);
+    tc::mbar_init(&bars[2]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1564,14 +1571,18 @@ __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
     unsigned char* st = smem_tc + (c & 1) * kStageB;
     float* xh = reinterpret_cast<float*>(st + 2 * tc::kHalf);
     float* xl = reinterpret_cast<float*>(st + 2 * tc::kHalf + kXHalf);
+    // after a timed-out wait the stage may still be read by MMAs in flight:
+    // nothing is written to it
+    if (ok) {
 #pragma unroll
-    for (int gi = 0; gi < kGroups; ++gi) {
-      const int n = 8 * (warp + 4 * gi) + (lane >> 2);
+      for (int gi = 0; gi < kGroups; ++gi) {
+        const int n = 8 * (warp + 4 * gi) + (lane >> 2);
 #pragma unroll
-      for (int q = 0; q < tc::kKC / 4; ++q) {
-        const float h = tc::hi_part(xr[gi][q]);
-        xh[(q * NC + n) * 4 + u] = h;
-        xl[(q * NC + n) * 4 + u] = xr[gi][q] - h;
+        for (int q = 0; q < tc::kKC / 4; ++q) {
+          const float h = tc::hi_part(xr[gi][q]);
+          xh[(q * NC + n) * 4 + u] = h;
+          xl[(q * NC + n) * 4 + u] = xr[gi][q] - h;
+        }
       }
     }
     cp_async_wait<0>();
@@ -1600,6 +1611,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
     if (c + 1 < tl.nkc) {
       // stage (c + 1) & 1 was read by the MMAs of chunk c - 1
       if (c >= 1 && !tc::mbar_wait(&bars[(c + 1) & 1], (uint32_t)(((c - 1) >> 1) & 1))) ok = false;
+      if (c == 1 && stall_test && !tc::mbar_wait(&bars[2], 0u, tc::kStallCycles)) ok = false;
       if (ok) issue(c + 1);
     }
   }
@@ -1621,7 +1633,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
       }
     }
   } else if (tid == 0) {
-    atomicExch(err, 1);
+    atomicExch(status, 1);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -1715,7 +1727,7 @@ struct FmmState {
   bool tensor = false;
   DevBuf m2x_tc, xl_tc;
   int m2x_mt = 0, m2x_nc = 0, xl_mt = 0, xl_nc = 0;
-  DevBuf tc_err;   // int: set by a tensor-core kernel whose wait timed out
+  DevBuf tc_status;  // int[2]: [0] set by a tensor-core kernel whose wait timed out; [1] timeout test switch
   // split-K wave -> local: per level the columns' L offsets and the partials
   DevBuf xl_ldst, xl_partials;
   std::vector<int> xlr_first, xlr_count;
@@ -1752,11 +1764,25 @@ bool fmm_active(const Problem& P) { return P.tree.n_levels - 1 >= 2; }
 
 void fmm_check_waits(Problem& P) {
   FmmState* S = P.fmm.get();
-  if (!S || !S->tc_err.get()) return;
+  if (!S || !S->tc_status.get()) return;
   int flag = 0;
-  BP_CUDA(cudaMemcpyAsync(&flag, S->tc_err.get(), sizeof(int), cudaMemcpyDeviceToHost, P.ctx->stream));
+  BP_CUDA(cudaMemcpyAsync(&flag, S->tc_status.get(), sizeof(int), cudaMemcpyDeviceToHost, P.ctx->stream));
   BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
-  if (flag) throw TimeoutError("a tensor-core FMM kernel timed out waiting for its matrix multiplies");
+  if (flag) {
+    // reported once: the next matvec starts clean
+    BP_CUDA(cudaMemsetAsync(S->tc_status.get(), 0, sizeof(int), P.ctx->stream));
+    BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
+    throw TimeoutError("a tensor-core FMM kernel timed out waiting for its matrix multiplies");
+  }
+}
+
+bool fmm_set_stall_test(Problem& P, bool on) {
+  FmmState* S = P.fmm.get();
+  if (!S || !S->tensor || !S->tc_status.get()) return false;
+  const int v = on ? 1 : 0;
+  BP_CUDA(cudaMemcpyAsync(S->tc_status.as<int>() + 1, &v, sizeof(int), cudaMemcpyHostToDevice, P.ctx->stream));
+  BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
+  return true;
 }
 
 namespace {
@@ -2469,8 +2495,8 @@ void fmm_setup(Problem& P) {
     ensure_dynamic_smem((const void*)op_gemm_tc_kernel<tc::kColsM2x>, tc::smem_bytes(tc::kColsM2x));
     ensure_dynamic_smem((const void*)op_gemm_tc_kernel<tc::kColsXl>, tc::smem_bytes(tc::kColsXl));
   }
-  S->tc_err.alloc(c, sizeof(int));
-  BP_CUDA(cudaMemsetAsync(S->tc_err.get(), 0, sizeof(int), c->stream));
+  S->tc_status.alloc(c, 2 * sizeof(int));
+  BP_CUDA(cudaMemsetAsync(S->tc_status.get(), 0, 2 * sizeof(int), c->stream));
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
   BP_CUDA(cudaStreamSynchronize(c->stream));
@@ -2522,11 +2548,11 @@ static void launch_op_gemm(FmmState& S, int first, int count, const T* simt_ops,
       if (tc_cols == tc::kColsM2x)
         op_gemm_tc_kernel<tc::kColsM2x><<<count, tc::kThreads, tc::smem_bytes(tc::kColsM2x), q>>>(
             S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride, X,
-            Y, S.tc_err.as<int>());
+            Y, S.tc_status.as<int>());
       else
         op_gemm_tc_kernel<tc::kColsXl><<<count, tc::kThreads, tc::smem_bytes(tc::kColsXl), q>>>(
             S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride, X,
-            Y, S.tc_err.as<int>());
+            Y, S.tc_status.as<int>());
       BP_LAUNCH_CHECK();
       return;
     }

@@ -218,6 +218,18 @@ int32_t bp_matvec_device(bp_problem p, const double* x_dev, double* y_dev);
 int32_t bp_matvec_profile(bp_problem p, const double* x_dev, double* y_dev, int32_t reps, double* stage_ms,
                           int32_t* stage_launches, int32_t* n_stages);
 
+/* Test of the bounded-wait timeout path (no counterpart in the reference).
+ * The tensor-core kernels of the mixed engine's far field wait on their own
+ * MMA-completion barriers with a bound of about a second; a wait that runs
+ * out abandons the kernel's tile (after draining the MMAs it issued and
+ * freeing its tensor memory) and the next bp_matvec / bp_solve on the
+ * problem returns BP_ERR_TIMEOUT once.  While enable != 0 every CTA of those
+ * kernels also waits, with a bound of 200000 cycles, on a barrier that
+ * nothing arrives on, so that path runs on every matvec.  Returns
+ * BP_ERR_UNSUPPORTED for problems without those kernels (FP64 engine, or no
+ * far field).  Blocking. */
+int32_t bp_problem_test_wait_timeout(bp_problem p, int32_t enable);
+
 /* GMRES(restart) solve of A x = rhs (BEEP::gmres, src/beep/beep.cpp:1262-1483):
  * classical Gram-Schmidt Arnoldi and Givens rotations in FP64, stop when the
  * residual estimate falls below tol * ||rhs||.  x holds the initial guess on
