@@ -609,14 +609,16 @@ constexpr int kXlGroups = 7;                     // lane groups of a translate b
 constexpr int kXlDirThreads = kXlGroups * kPairLanes;
 
 // One block per (target, 4 channels); thread (lane group g, lane i = plane
-// wave) sums W[src][d][ch][i] * factor[combo][i] over a range of the
-// target's entries of direction d, in registers.  The up and down lists
-// are about twice as long as north / south and four times east / west, so
-// the seven lane groups share the work evenly: up and down each split in
-// halves (groups 0 + 1, 2 + 3; the second half's sum is added through shared
-// memory), north (4), south (5), and east then west (6).  ACC[acc_row][ch]
-// [d][i] (re, im) is stored for all six directions, 0 for one without
-// entries.
+// wave) sums W[src][d][ch][i] * factor[combo][i] over its share of the
+// target's entries, in registers.  The entries are sorted by direction and
+// the seven lane groups take equal contiguous slices of them, whatever the
+// mix of directions (it depends on the target's surroundings).  A slice
+// leaves one partial sum per direction it meets, in shared slot g + d (the
+// pairs (g, d) met along the list have distinct g + d, at most 12 of them);
+// then each direction's partials are added in group order (deterministic)
+// and ACC[acc_row][ch][d][i] (re, im) is stored for all six directions, 0
+// for one without entries.
+constexpr int kXlSlots = kXlGroups + 5;
 template <typename T>
 __global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __grid_constant__ Tables<T> tb,
                                                                         int parent_level,
@@ -628,7 +630,7 @@ __global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
   constexpr int U = kXlUnroll;  // entries in flight per thread (measured: 2 beats 4, 6 and 8 spill)
-  __shared__ C part[2][CB][kPairLanes];  // second halves of up and down
+  __shared__ C part[kXlSlots][CB][kPairLanes];
   const int NPM = tb.np_max;
   const int t = blockIdx.x / (kCh / CB);
   const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
@@ -667,38 +669,38 @@ __global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __
           for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
     }
   };
-  auto store = [&](int d, const C (&a)[CB]) {
-    if (i >= NPM) return;
+  // slice [gb, ge) of the target's entries
+  const int n = tg.n_entries;
+  const int gb = (int)(((long long)g * n) / kXlGroups), ge = (int)(((long long)(g + 1) * n) / kXlGroups);
+  for (int d = 0; d < 6; ++d) {
+    const int b = max(gb, tg.dir_start[d]), e = min(ge, tg.dir_start[d + 1]);
+    if (b >= e) continue;
+    C a[CB];
+    accum(d, b, e, a);
+#pragma unroll
+    for (int c = 0; c < CB; ++c) part[g + d][c][i] = a[c];
+  }
+  __syncthreads();
+  if (g < 6 && i < NPM) {
+    // direction g: the slices that meet its entries, in order
+    const int d = g, b = tg.dir_start[d], e = tg.dir_start[d + 1];
+    C a[CB];
+#pragma unroll
+    for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
+    if (b < e) {
+      const int g0 = (int)(((long long)b * kXlGroups) / max(n, 1));
+      for (int gg = max(g0 - 1, 0); gg < kXlGroups; ++gg) {
+        const int sb = (int)(((long long)gg * n) / kXlGroups), se = (int)(((long long)(gg + 1) * n) / kXlGroups);
+        if (se <= b) continue;
+        if (sb >= e) break;
+        if (max(sb, b) >= min(se, e)) continue;
+#pragma unroll
+        for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], part[gg + d][c][i]);
+      }
+    }
     C* out = ACC + (((size_t)tg.acc_row * kCh + ch0) * 6 + d) * NPM + i;
 #pragma unroll
     for (int c = 0; c < CB; ++c) out[(size_t)c * 6 * NPM] = a[c];
-  };
-  C a[CB];
-  if (g < 4) {  // halves of up (0, 1) and down (2, 3)
-    const int d = g >> 1, b = tg.dir_start[d], e = tg.dir_start[d + 1], mid = b + (e - b + 1) / 2;
-    if (g & 1) {
-      accum(d, mid, e, a);
-#pragma unroll
-      for (int c = 0; c < CB; ++c) part[d][c][i] = a[c];
-    } else {
-      accum(d, b, mid, a);
-    }
-  } else if (g < 6) {
-    const int d = g - 2;
-    accum(d, tg.dir_start[d], tg.dir_start[d + 1], a);
-    store(d, a);
-  } else {
-    accum(4, tg.dir_start[4], tg.dir_start[5], a);
-    store(4, a);
-    accum(5, tg.dir_start[5], tg.dir_start[6], a);
-    store(5, a);
-  }
-  __syncthreads();
-  if (g < 4 && !(g & 1)) {
-    const int d = g >> 1;
-#pragma unroll
-    for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], part[d][c][i]);
-    store(d, a);
   }
   (void)n_targets;
 }
@@ -1786,38 +1788,6 @@ bool fmm_set_stall_test(Problem& P, bool on) {
 }
 
 namespace {
-
-// Generates the 1512 interaction entries (src/fmm/interaction_list.h):
-// source = child of a non-self neighbour of the parent, target = child of
-// the parent, separated by >= 2 child boxes along some axis; the direction
-// is UP/DOWN by dz, else NORTH/SOUTH by dy, else EAST/WEST by dx.
-struct RawInteraction {
-  int nb, dir, targ, src, dx, dy, dz;
-};
-std::vector<RawInteraction> interaction_table() {
-  std::vector<RawInteraction> out;
-  for (int nb = 0; nb < 27; ++nb) {
-    if (nb == 13) continue;
-    const int pz = nb / 9 - 1, py = (nb % 9) / 3 - 1, px = nb % 3 - 1;
-    for (int t = 0; t < 8; ++t) {
-      const int tx = t & 1, ty = (t >> 1) & 1, tz = t >> 2;
-      for (int s = 0; s < 8; ++s) {
-        const int sx = 2 * px + (s & 1), sy = 2 * py + ((s >> 1) & 1), sz = 2 * pz + (s >> 2);
-        const int dx = tx - sx, dy = ty - sy, dz = tz - sz;
-        if (std::abs(dx) < 2 && std::abs(dy) < 2 && std::abs(dz) < 2) continue;
-        int dir;
-        if (dz >= 2) dir = 0;
-        else if (dz <= -2) dir = 1;
-        else if (dy >= 2) dir = 2;
-        else if (dy <= -2) dir = 3;
-        else if (dx >= 2) dir = 4;
-        else dir = 5;
-        out.push_back({nb, dir, t, s, dx, dy, dz});
-      }
-    }
-  }
-  return out;
-}
 
 template <typename T>
 void fill_tables(FmmState& S, const Problem& P, Tables<T>& tb, DevBuf& buf, const GlobalTables& G,

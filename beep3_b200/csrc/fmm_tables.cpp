@@ -13,7 +13,9 @@
 //     i_0 = sinh(x)/x where the reference calls Cody's RIBESL).
 #include "fmm_tables.h"
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <stdexcept>
 
 namespace bp {
@@ -53,6 +55,37 @@ void bessel_in(double scal, double x, int nb, double* b) {
     c *= inv_scal;
     if (std::fabs(b[i]) <= enmten) c = 0.0;
   }
+}
+
+// Source = child of a non-self neighbour of the parent, target = child of
+// the parent, separated by >= 2 child boxes along some axis.  The wave
+// travels along the axis of the largest separation, ties going to z, then
+// y, then x (UP/DOWN, NORTH/SOUTH, EAST/WEST by its sign): that is the
+// direction of every entry of the reference's table (checked against the
+// table itself by the tests), and it keeps the sideways offsets of a wave
+// small.  Child ids are 0-based here (the reference's are 1..8): bit 0 x,
+// bit 1 y, bit 2 z.
+std::vector<RawInteraction> interaction_table() {
+  std::vector<RawInteraction> out;
+  for (int nb = 0; nb < 27; ++nb) {
+    if (nb == 13) continue;
+    const int pz = nb / 9 - 1, py = (nb % 9) / 3 - 1, px = nb % 3 - 1;
+    for (int t = 0; t < 8; ++t) {
+      const int tx = t & 1, ty = (t >> 1) & 1, tz = t >> 2;
+      for (int s = 0; s < 8; ++s) {
+        const int sx = 2 * px + (s & 1), sy = 2 * py + ((s >> 1) & 1), sz = 2 * pz + (s >> 2);
+        const int dx = tx - sx, dy = ty - sy, dz = tz - sz;
+        const int m = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
+        if (m < 2) continue;
+        int dir;
+        if (std::abs(dz) == m) dir = dz > 0 ? 0 : 1;
+        else if (std::abs(dy) == m) dir = dy > 0 ? 2 : 3;
+        else dir = dx > 0 ? 4 : 5;
+        out.push_back({nb, dir, t, s, dx, dy, dz});
+      }
+    }
+  }
+  return out;
 }
 
 double fmm_scale(double beta, double edge, int level) {

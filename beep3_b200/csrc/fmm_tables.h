@@ -10,6 +10,18 @@ using cplx = std::complex<double>;
 
 // i_n(x) / scal^n for n = 0..nb
 void bessel_in(double scal, double x, int nb, double* b);
+
+// One entry of the plane-wave interaction list of a parent node: the source
+// is child `src` (0..7) of neighbour `nb` (0..26, 13 = the parent itself) of
+// the parent, the target child `targ` (0..7) of the parent, (dx, dy, dz) the
+// target's offset from the source in child boxes, dir the wave direction
+// (0 up, 1 down, 2 north, 3 south, 4 east, 5 west).
+struct RawInteraction {
+  int nb, dir, targ, src, dx, dy, dz;
+};
+// The 1512 entries of the reference's table (src/fmm/interaction_list.h),
+// generated from its rule instead of stored.
+std::vector<RawInteraction> interaction_table();
 // min(beta * edge, 1) / 2^level
 double fmm_scale(double beta, double edge, int level);
 void yarvin_rokhlin(int nt, std::vector<double>& x, std::vector<double>& w, std::vector<int>& numfour,

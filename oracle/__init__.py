@@ -53,6 +53,37 @@ def build(native: bool = False) -> Path:
     return out
 
 
+REFERENCE = Path("/root/reference")
+REF_LIB = HERE / "_ref" / "libref_pieces.so"
+
+
+def build_ref() -> Path | None:
+    """Builds oracle/_ref/libref_pieces.so (the reference's own RIBESL and
+    interaction table) when the reference tree is present; returns the
+    library path when it exists."""
+    src = HERE / "ref_pieces.cpp"
+    if (REFERENCE / "src" / "fmm" / "bessel_gamma.h").exists():
+        if not REF_LIB.exists() or src.stat().st_mtime > REF_LIB.stat().st_mtime:
+            res = subprocess.run(["make", "-C", str(HERE), "ref", f"REFERENCE={REFERENCE}"], capture_output=True,
+                                 text=True)
+            if res.returncode != 0:
+                raise RuntimeError("reference pieces build failed:\n" + res.stdout + res.stderr)
+    return REF_LIB if REF_LIB.exists() else None
+
+
+def ref_lib() -> C.CDLL | None:
+    """The reference's own compiled pieces, or None when they are not built."""
+    path = build_ref()
+    if path is None:
+        return None
+    L = C.CDLL(str(path))
+    L.ref_ribesl.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p]
+    L.ref_ribesl.restype = C.c_int
+    L.ref_interaction_list.argtypes = [C.c_void_p]
+    L.ref_interaction_list.restype = C.c_int
+    return L
+
+
 def use_native() -> None:
     """Makes lib() load the -march=native build (call before the first use)."""
     global _native
@@ -98,6 +129,8 @@ def lib() -> C.CDLL:
             L.or_fmm_destroy.argtypes = [P]
             L.or_fmm_apply.argtypes = [P, P, P]
             L.or_fmm_direct.argtypes = [C.POINTER(OrPatches), C.c_double, C.c_double, C.c_int, P, P, P, P]
+            L.or_interaction_list.argtypes = [P]
+            L.or_interaction_list.restype = C.c_int
         _lib = L
     return _lib
 

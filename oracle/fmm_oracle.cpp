@@ -26,12 +26,14 @@
 //     (the 1512-entry table of src/fmm/interaction_list.h is generated from
 //      its rule: source = child of a non-self neighbour of the parent,
 //      target = child of the parent, |offset| >= 2 on some axis; direction
-//      UP/DOWN by dz, else NORTH/SOUTH by dy, else EAST/WEST by dx)
+//      along the axis of the largest |offset|, ties to z, then y, then x --
+//      equal to the stored table entry for entry)
 //   evaluate_local_expansion_at_xyz (12-way, potential, field, Hessian)
 //                                              src/fmm/fmm.h:40-415, :696-892
 //   FMM_results_to_BEM                         src/bem/bem_kernels.cpp:12-121
 //   charges of a node patch                     src/bem/node_patch.h:339-394
 // Everything in FP64.
+#include <algorithm>
 #include <cassert>
 #include <cmath>
 #include <complex>
@@ -823,14 +825,13 @@ std::vector<Interaction> interaction_list() {
       for (int s = 1; s <= 8; ++s) {
         int sx = 2 * px + ((s - 1) & 1), sy = 2 * py + (((s - 1) >> 1) & 1), sz = 2 * pz + ((s - 1) >> 2);
         int dx = tx - sx, dy = ty - sy, dz = tz - sz;
-        if (std::abs(dx) < 2 && std::abs(dy) < 2 && std::abs(dz) < 2) continue;
+        const int m = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
+        if (m < 2) continue;
+        // the axis of the largest separation, ties to z, then y, then x
         int dir;
-        if (dz >= 2) dir = UP;
-        else if (dz <= -2) dir = DOWN;
-        else if (dy >= 2) dir = NORTH;
-        else if (dy <= -2) dir = SOUTH;
-        else if (dx >= 2) dir = EAST;
-        else dir = WEST;
+        if (std::abs(dz) == m) dir = dz > 0 ? UP : DOWN;
+        else if (std::abs(dy) == m) dir = dy > 0 ? NORTH : SOUTH;
+        else dir = dx > 0 ? EAST : WEST;
         out.push_back({nb, dir, t, s, dx, dy, dz});
       }
     }
@@ -868,6 +869,19 @@ struct OrFmm {
 };
 
 extern "C" {
+
+// The oracle's interaction list, 7 ints per entry (neighbour, direction,
+// target child 1..8, source child 1..8, dx, dy, dz); returns the count and
+// fills out when it is not null.
+int or_interaction_list(int32_t* out) {
+  const std::vector<Interaction> l = interaction_list();
+  if (out)
+    for (size_t k = 0; k < l.size(); ++k) {
+      const int32_t v[7] = {l[k].nb, (int32_t)l[k].dir, l[k].targ, l[k].src, l[k].dx, l[k].dy, l[k].dz};
+      for (int c = 0; c < 7; ++c) out[7 * k + c] = v[c];
+    }
+  return (int)l.size();
+}
 
 OrFmm* or_fmm_create(const OrPatches* P, const OrTree* T, double kappa, double beta0, double edge, int nterms) {
   return new OrFmm(P, T, nterms, kappa, beta0, edge);

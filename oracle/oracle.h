@@ -45,6 +45,7 @@ struct OrFmm;
 OrFmm* or_fmm_create(const OrPatches* P, const OrTree* T, double kappa, double beta0, double edge, int nterms);
 void or_fmm_destroy(OrFmm* F);
 void or_fmm_apply(OrFmm* F, const double* x, double* y);
+int or_interaction_list(int32_t* out);
 void or_fmm_direct(const OrPatches* P, double kappa, double beta0, int npairs, const int32_t* T, const int32_t* S,
                    const double* x, double* y);
 int or_gmres(or_matvec_fn mv, void* user, int n2, const double* b, double* x, double tol, int max_iters, int restart,

@@ -1,8 +1,9 @@
 // Test shim: compiles the engine's host FMM table source and the oracle's
 // FMM restatement into one test library and exposes their special
 // functions (scaled modified spherical Bessel i_n, associated Legendre
-// functions) through extern "C" wrappers, so the tests can compare them
-// with scipy.  Built by tests/native/__init__.py; not part of the product.
+// functions) and the engine's generated interaction list through extern "C"
+// wrappers, so the tests can compare them with scipy and with the
+// reference's own code.  Built by tests/native/__init__.py; not part of the product.
 #include "../../beep3_b200/csrc/fmm_tables.cpp"
 #include "../../oracle/fmm_oracle.cpp"
 
@@ -18,6 +19,18 @@ void shim_engine_legendre_gt1(int nmax, double scal, double x, double* y) {
   std::vector<double> v;
   bp::legendre_gt1(nmax, scal, x, v);
   std::copy(v.begin(), v.end(), y);
+}
+
+// engine: its generated interaction list, 7 ints per entry (child ids
+// 0-based); returns the count
+int shim_engine_interaction_list(int32_t* out) {
+  const std::vector<bp::RawInteraction> l = bp::interaction_table();
+  if (out)
+    for (size_t k = 0; k < l.size(); ++k) {
+      const int32_t v[7] = {l[k].nb, l[k].dir, l[k].targ, l[k].src, l[k].dx, l[k].dy, l[k].dz};
+      for (int c = 0; c < 7; ++c) out[7 * k + c] = v[c];
+    }
+  return (int)l.size();
 }
 
 // oracle: the same i_n
