@@ -346,6 +346,13 @@ struct Problem {
   bool graph_failed = false;
   // Krylov workspace
   DevBuf d_V, d_w, d_scal;
+  // one GMRES cycle's Arnoldi loop as a graph with a device-side WHILE node
+  // (built for basis size gmres_graph_m on the V / scalar blocks it was
+  // captured with)
+  cudaGraphExec_t gmres_graph = nullptr;
+  int gmres_graph_m = 0;
+  const void* gmres_graph_v = nullptr;
+  bool gmres_graph_failed = false;
   // grow-only scratch of the source terms (charges, per-point values, the
   // right-hand side of bp_solve): kept so repeated calls allocate nothing
   DevBuf scratch_charges, scratch_vals, scratch_b;
@@ -367,6 +374,7 @@ struct Problem {
     for (const Placement& pl : placements)
       if (mesh_release(pl.mesh)) delete pl.mesh;
     if (graph) cudaGraphExecDestroy(graph);
+    if (gmres_graph) cudaGraphExecDestroy(gmres_graph);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);
