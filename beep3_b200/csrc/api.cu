@@ -450,6 +450,7 @@ BP_API int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info) {
   info->device_bytes = P->ctx->used;
   info->tree_ms = P->tree_ms;
   info->assemble_ms = P->assemble_ms;
+  info->gmres_graph = P->gmres_graph ? 1 : 0;
   return BP_OK;
 }
 

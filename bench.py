@@ -566,6 +566,7 @@ def _run_ours(args, world, rank, local, dist):
         "solve_latency_ms": {"p50": float(np.percentile(solve_ms, 50)), "p99": float(np.percentile(solve_ms, 99))},
         "solve_parts_ms": {"rhs": float(np.median(rhs_ms)), "gmres": float(np.median(gmres_ms))},
         "gmres_iterations": {"mixed": info.num_iterations, "fp64": info64.num_iterations},
+        "gmres_loop_on_device": bool(bp.info().gmres_graph),
         "energy_kj_per_mol": {"mixed": e_mixed, "fp64": e_fp64,
                               "rel_err_mixed_vs_fp64": abs(e_mixed - e_fp64) / abs(e_fp64)},
         "clocks": clocks,

@@ -140,6 +140,9 @@ typedef struct {
   uint64_t device_bytes;
   double tree_ms;
   double assemble_ms;        /* device time of the singular + near-field assembly kernels */
+  int64_t gmres_graph;       /* 1 once a solve ran its Arnoldi loop as one CUDA graph with a
+                                device-side loop condition, 0 before the first solve or when the
+                                host drove the loop step by step */
 } bp_problem_info;
 
 /* Builds the adaptive octree, the singular self-patch integrals and the

@@ -116,3 +116,13 @@ def test_budget_is_enforced(kirkwood_case):
     with pytest.raises(b.BudgetExceeded):
         bp.build()
     bp.close()
+
+
+def test_gmres_loop_runs_as_one_graph(kirkwood_case):
+    """The Arnoldi loop of a cycle runs as one CUDA graph with a device-side
+    loop condition (no host round trip per step)."""
+    bp = make_beep(kirkwood_case["mesh"], precision="mixed")
+    assert bp.info().gmres_graph == 0
+    info = bp.solve(1e-6, 100)
+    assert info.converged and bp.info().gmres_graph == 1
+    bp.close()
