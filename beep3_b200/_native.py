@@ -26,6 +26,8 @@ BP_ERR_NOT_CONVERGED = 8
 BP_PREC_FP64 = 0
 BP_PREC_MIXED = 1
 
+BP_FLAG_NEARFIELD_ON_DEMAND = 1
+
 _ERR_NAMES = {
     BP_ERR_INVALID: "invalid argument", BP_ERR_CUDA: "CUDA error", BP_ERR_NOMEM: "out of host memory",
     BP_ERR_BUDGET: "HBM budget exceeded", BP_ERR_TIMEOUT: "device wait timed out",

@@ -198,10 +198,13 @@ class BEEP:
 
     def __init__(self, eps_solvent: float = 80.0, kappa: float = 0.1, nbsize: int = DEFAULT_NBSIZE,
                  nterms: int = 9, precision: str = "fp64", device: int = 0, hbm_budget_bytes: int = 0,
-                 context: EngineContext | None = None):
+                 context: EngineContext | None = None, nearfield_on_demand: bool = False):
         """``context``: an EngineContext shared with scenarios run before or
         after this one (its device and budget apply); by default the scenario
-        has its own."""
+        has its own.  ``nearfield_on_demand``: recompute the near field in
+        every matvec instead of caching its coefficients (the reference's
+        uncached GPU path): no coefficient memory, the assembly's cost per
+        matvec."""
         self.eps_solvent = float(eps_solvent)
         self.kappa = float(kappa)
         self.nbsize = int(nbsize)
@@ -209,6 +212,7 @@ class BEEP:
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.precision = precision
+        self.nearfield_on_demand = bool(nearfield_on_demand)
         self.instances: list[MeshInstance] = []
         self.device = int(device)
         self.hbm_budget_bytes = int(hbm_budget_bytes)
@@ -349,7 +353,8 @@ class BEEP:
             insts[k].offset[:] = [float(v) for v in inst.offset]
             insts[k].dielectric_ratio = inst.dielectric_ratio
         prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge, self.nbsize, self.nterms,
-                          N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED, 0)
+                          N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED,
+                          N.BP_FLAG_NEARFIELD_ON_DEMAND if self.nearfield_on_demand else 0)
         h = C.c_void_p()
         N.check(N.lib().bp_problem_create_posed(self.context(), insts, len(self.instances), C.byref(prm), C.byref(h)))
         self._problem = h

@@ -78,6 +78,7 @@ int32_t check_params(const char* who, const bp_params* prm) {
   if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
     return fail(BP_ERR_INVALID, std::string(who) + ": unknown precision");
   if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, std::string(who) + ": bad kappa");
+  if (prm->flags & ~BP_FLAG_NEARFIELD_ON_DEMAND) return fail(BP_ERR_INVALID, std::string(who) + ": unknown flags");
   if (prm->nterms != 9)
     return fail(BP_ERR_UNSUPPORTED, std::string(who) +
                                         ": FMM order must be 9 (the reference's BEM matvec order; the far-field "

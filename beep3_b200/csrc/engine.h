@@ -251,6 +251,8 @@ struct NfItem {
 // of (A, B, C, D) coefficients, rows = the leaf's patches, cols = the
 // patches of its 27-box neighbourhood.
 struct NearField {
+  bool on_demand = false;  // no cached coefficients: instant_kernel every matvec
+  size_t instant_smem = 0;
   int n_leaves = 0;
   int64_t n_pairs = 0;
   int n_items = 0;

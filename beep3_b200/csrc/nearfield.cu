@@ -347,6 +347,142 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
   }
 }
 
+// The near field without cached coefficients (the reference's
+// BEM_kernels_instant + processBEMBlockResults for its uncached OpenCL path,
+// src/bem/opencl_bem_kernels.cl:237-352, src/beep/beep.cpp:999-1008): the
+// work items and point staging of assemble_kernel, but each thread applies
+// the (A, B, C, D) of a pair to x at once and keeps, per staged row, the sums
+// over its columns; the block then adds them in a fixed order (warp
+// shuffles, then warps in order) and writes the rows with the FP64 diagonal
+// and, when given, the far field.  Every row of a leaf belongs to one work
+// item, so no two blocks write the same row.  The cost is the assembly's,
+// every matvec; the memory is that of the points only.
+template <typename T>
+__global__ void __launch_bounds__(kAsmThreads) instant_kernel(
+    const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
+    const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int32_t* __restrict__ qoff,
+    const T* __restrict__ qual, int nq, const int32_t* __restrict__ poff, const T* __restrict__ quad, int np,
+    const double* __restrict__ eps, T kappa, const double* __restrict__ diag, int n, const double* __restrict__ x,
+    const double* __restrict__ yfar, double* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sq = reinterpret_cast<T*>(smem_raw);  // [qual_total][8]
+  __shared__ int s_start[kAsmRows + 1];
+  __shared__ int s_row[kAsmRows];
+  __shared__ double s_red[kAsmThreads / 32][kAsmRows][2];
+  const NfItem it = items[blockIdx.x];
+  const int64_t r0 = row_off[it.leaf] + it.row_begin;
+  const int64_t c0 = col_off[it.leaf];
+  const int ncols = (int)(col_off[it.leaf + 1] - c0);
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int r = 0; r < it.row_count; ++r) {
+      const int i = rows[r0 + r];
+      s_row[r] = i;
+      s_start[r] = acc;
+      acc += qoff[i + 1] - qoff[i];
+    }
+    s_start[it.row_count] = acc;
+  }
+  __syncthreads();
+  for (int r = 0; r < it.row_count; ++r) {
+    const int i = s_row[r];
+    const int base = qoff[i];
+    const int cnt = s_start[r + 1] - s_start[r];
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      T* dst = sq + 8 * (s_start[r] + k);
+      for (int f = 0; f < 7; ++f) dst[f] = qual[(size_t)f * nq + base + k];
+      dst[7] = T(0);
+    }
+  }
+  __syncthreads();
+  const bool with_d = kappa != T(0);
+  const T ek = exp_scale<T>(kappa);
+  T accf[kAsmRows], acch[kAsmRows];
+#pragma unroll
+  for (int r = 0; r < kAsmRows; ++r) accf[r] = acch[r] = T(0);
+  for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) {
+    const int j = cols[c0 + cc];
+    const T ie = T(1.0 / eps[j]);
+    const T fj = T(x[j]), hj = T(x[n + j]);
+    const int ps = poff[j], pe = poff[j + 1];
+    const bool one_point = pe - ps == 1;
+    T p1[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (one_point)
+      for (int f = 0; f < 7; ++f) p1[f] = quad[(size_t)f * np + ps];
+#pragma unroll
+    for (int r = 0; r < kAsmRows; ++r) {
+      if (r >= it.row_count || s_row[r] == j) continue;  // the self pair is the FP64 diagonal
+      T A = 0, B = 0, C = 0, D = 0;
+      const int qs = s_start[r], qe = s_start[r + 1];
+      if (one_point) {
+        for (int q = qs; q < qe; ++q) {
+          T u[7];
+          load_qpoint(sq, q, u);
+          T a = 0, b = 0, c = 0, d = 0;
+          pair_term_unit<T>(u[0], u[1], u[2], u[3], u[4], u[5], p1[0], p1[1], p1[2], p1[3], p1[4], p1[5], kappa, ek,
+                            ie, with_d, a, b, c, d);
+          A += a * u[6];
+          B += b * u[6];
+          C += c * u[6];
+          D += d * u[6];
+        }
+        A *= p1[6];
+        B *= p1[6];
+        C *= p1[6];
+        D *= p1[6];
+      } else {
+        for (int q = qs; q < qe; ++q) {
+          T u[7];
+          load_qpoint(sq, q, u);
+          T a = 0, b = 0, c = 0, d = 0;
+          for (int p = ps; p < pe; ++p) {
+            pair_term<T>(u[0], u[1], u[2], u[3], u[4], u[5], quad[p], quad[(size_t)np + p],
+                         quad[2 * (size_t)np + p], quad[3 * (size_t)np + p], quad[4 * (size_t)np + p],
+                         quad[5 * (size_t)np + p], quad[6 * (size_t)np + p], kappa, ie, with_d, a, b, c, d);
+          }
+          A += a * u[6];
+          B += b * u[6];
+          C += c * u[6];
+          D += d * u[6];
+        }
+      }
+      accf[r] += B * fj - A * hj;
+      acch[r] += (D * ie) * fj - C * hj;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < kAsmRows; ++r) {
+    double df = (double)accf[r], dh = (double)acch[r];
+    for (int o = 16; o > 0; o >>= 1) {
+      df += __shfl_xor_sync(0xffffffffu, df, o);
+      dh += __shfl_xor_sync(0xffffffffu, dh, o);
+    }
+    if (lane == 0) {
+      s_red[warp][r][0] = df;
+      s_red[warp][r][1] = dh;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < it.row_count) {
+    const int r = threadIdx.x, i = s_row[r];
+    double df = 0.0, dh = 0.0;
+    for (int w = 0; w < kAsmThreads / 32; ++w) {
+      df += s_red[w][r][0];
+      dh += s_red[w][r][1];
+    }
+    const double fi = x[i], hi = x[n + i];
+    double yf = df + (diag[4 * i + 1] * fi - diag[4 * i + 0] * hi);
+    double yh = dh + (diag[4 * i + 3] * fi - diag[4 * i + 2] * hi);
+    if (yfar) {
+      yf += yfar[i];
+      yh += yfar[n + i];
+    }
+    y[i] = yf;
+    y[n + i] = yh;
+  }
+}
+
 // y_f[i] = sum_j B_ij f_j - A_ij h_j ; y_h[i] = sum_j D_ij f_j - C_ij h_j
 // over the leaf's columns (the cached-coefficient stream of
 // src/beep/beep.cpp:1049-1062).  Accumulation type AccT.
@@ -520,10 +656,11 @@ void nf_assemble(Problem& P) {
   if (smem > 200 * 1024) throw std::invalid_argument("too many qualocation points per patch");
   // inputs and outputs are placed on the context's stream; the kernels run
   // on the assembly stream once they are
+  nf.on_demand = (P.params.flags & BP_FLAG_NEARFIELD_ON_DEMAND) != 0;
   P.asm_gc = upload(ctx, P.h_gc);  // geometric correction per patch
   P.asm_items = upload(ctx, asm_items);
   P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
-  nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
+  if (!nf.on_demand) nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
   BP_CUDA(cudaEventRecord(P.asm_in, ctx->stream));
   const cudaStream_t st = P.asm_stream;
   BP_CUDA(cudaStreamWaitEvent(st, P.asm_in, 0));
@@ -538,6 +675,20 @@ void nf_assemble(Problem& P) {
     BP_LAUNCH_CHECK();
   }
   const DevBuf& d_asm_items = P.asm_items;
+  if (nf.on_demand) {
+    // only the singular diagonal is assembled; every matvec recomputes the
+    // pairs over the assembly's work items
+    BP_CUDA(cudaEventRecord(P.asm_t1, st));
+    nf.instant_smem = smem;
+    if (P.fp64)
+      ensure_dynamic_smem((const void*)instant_kernel<double>, smem);
+    else
+      ensure_dynamic_smem((const void*)instant_kernel<float>, smem);
+    nf.h_items = asm_items;
+    nf.items = upload(ctx, nf.h_items);
+    nf.n_items = (int)nf.h_items.size();
+    return;
+  }
   if (!asm_items.empty()) {
     if (P.fp64) {
       ensure_dynamic_smem((const void*)assemble_kernel<double>, smem);
@@ -588,6 +739,23 @@ void nf_join(Problem& P) {
 int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_dev, cudaStream_t stream) {
   NearField& nf = P.nf;
   if (nf.n_items == 0) return 0;
+  if (nf.on_demand) {
+    const int nq = P.n_qual_pts, np = P.n_quad_pts;
+    if (P.fp64)
+      instant_kernel<double><<<nf.n_items, kAsmThreads, nf.instant_smem, stream>>>(
+          nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+          nf.col_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual.as<double>(), nq, P.d_quad_off.as<int32_t>(),
+          P.d_quad.as<double>(), np, P.d_eps.as<double>(), P.params.kappa, P.d_diag.as<double>(), P.n, x_dev,
+          yfar_dev, y_dev);
+    else
+      instant_kernel<float><<<nf.n_items, kAsmThreads, nf.instant_smem, stream>>>(
+          nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+          nf.col_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(), nq, P.d_quad_off.as<int32_t>(),
+          P.d_quad_f.as<float>(), np, P.d_eps.as<double>(), (float)P.params.kappa, P.d_diag.as<double>(), P.n, x_dev,
+          yfar_dev, y_dev);
+    BP_LAUNCH_CHECK();
+    return 1;
+  }
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
   const size_t smem = 2 * elem * (size_t)nf.max_cols;
   const int grid = std::min(nf.n_items, kApplyBlocksPerSm * P.ctx->sm_count);

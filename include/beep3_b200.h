@@ -126,8 +126,18 @@ typedef struct {
   int32_t nterms;         /* FMM order: 9, the reference's matvec order (FMM_BEM_Octree<9,9,67>);
                              other orders return BP_ERR_UNSUPPORTED */
   int32_t precision;      /* enum bp_precision */
-  int32_t flags;          /* reserved, 0 */
+  int32_t flags;          /* bitwise or of enum bp_flags */
 } bp_params;
+
+enum bp_flags {
+  /* Near field computed in every matvec from the point lists instead of
+   * cached: no coefficient storage (16 or 32 bytes per near pair), at the
+   * assembly's cost per matvec.  The reference's uncached OpenCL path
+   * (BEM_kernels_instant, src/bem/opencl_bem_kernels.cl:237-352;
+   * src/beep/beep.cpp:999-1008); for problems whose coefficients would not
+   * fit the HBM budget. */
+  BP_FLAG_NEARFIELD_ON_DEMAND = 1
+};
 
 typedef struct {
   int64_t n_patches;
