@@ -636,18 +636,6 @@ struct XgChunk<double> {
   static constexpr int value = 8;
 };
 
-// one complex value copied asynchronously into shared memory
-__device__ __forceinline__ void cp_async_c(float2* smem, const float2* gmem) {
-  cp_async_elem<double>(reinterpret_cast<double*>(smem), reinterpret_cast<const double*>(gmem));
-}
-__device__ __forceinline__ void cp_async_c(double2* smem, const double2* gmem) { cp_async16(smem, gmem); }
-
-// dynamic shared memory of xl_group_kernel: two chunks of waves
-template <typename T>
-constexpr size_t xg_smem_bytes() {
-  return 2 * (size_t)XgChunk<T>::value * kXlChannels * kPairLanes * sizeof(typename C2T<T>::type);
-}
-
 template <typename T>
 __global__ void __launch_bounds__(kXgThreads) xl_group_kernel(const __grid_constant__ Tables<T> tb, int parent_level,
                                                               const XlTask* __restrict__ tasks,
@@ -660,8 +648,7 @@ __global__ void __launch_bounds__(kXgThreads) xl_group_kernel(const __grid_const
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
   constexpr int KU = XgChunk<T>::value;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* sw = reinterpret_cast<C*>(smem_raw);  // [2 buffers][KU][CB][kPairLanes]
+  __shared__ C sw[KU][CB][kPairLanes];
   const XlTask tk = tasks[blockIdx.x / (kCh / CB)];
   const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
   const int t = threadIdx.x / kPairLanes, i = threadIdx.x - t * kPairLanes;
@@ -676,42 +663,28 @@ __global__ void __launch_bounds__(kXgThreads) xl_group_kernel(const __grid_const
     e = toff[tk.toff_first + t];
     e_end = toff[tk.toff_first + t + 1];
   }
-  // the waves of sources [base, base + KU) into buffer buf: a source's four
-  // channels of this direction are 4 NPM consecutive complex values
-  auto issue = [&](int base, int buf) {
-    const int nu = min(KU, tk.n_src - base);
-    for (int o = threadIdx.x; o < nu * CB * NPM; o += blockDim.x) {
-      const int u = o / (CB * NPM), rem = o - u * (CB * NPM);
-      const int c = rem / NPM, ii = rem - c * NPM;
-      cp_async_c(sw + (((size_t)buf * KU + u) * CB + c) * kPairLanes + ii,
-                 W + (((size_t)src_nodes[tk.src_first + base + u] * 6 + tk.dir) * kCh + ch0 + c) * NPM + ii);
-    }
-    cp_async_commit();
-  };
   C acc[CB];
 #pragma unroll
   for (int c = 0; c < CB; ++c) acc[c] = cmk<C>(0, 0);
-  if (tk.n_src > 0) issue(0, 0);
-  for (int base = 0, k = 0; base < tk.n_src; base += KU, ++k) {
-    const int buf = k & 1, nu = min(KU, tk.n_src - base);
-    if (base + KU < tk.n_src) {
-      issue(base + KU, buf ^ 1);  // that buffer's readers finished at the end of the previous pass
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  for (int base = 0; base < tk.n_src; base += KU) {
+    const int nu = min(KU, tk.n_src - base);
+    if (base > 0) __syncthreads();  // the previous chunk's readers are done
+    // the chunk's waves: a source's four channels of this direction are
+    // 4 NPM consecutive complex values
+    for (int o = threadIdx.x; o < nu * CB * NPM; o += blockDim.x) {
+      const int u = o / (CB * NPM), rem = o - u * (CB * NPM);
+      const int c = rem / NPM, ii = rem - c * NPM;
+      sw[u][c][ii] = W[(((size_t)src_nodes[tk.src_first + base + u] * 6 + tk.dir) * kCh + ch0 + c) * NPM + ii];
     }
     __syncthreads();
-    const C* chunk = sw + (size_t)buf * KU * CB * kPairLanes;
     if (live)
       for (; e < e_end; ++e) {
         const XlEnt en = ents[e];
         if (en.u >= base + nu) break;
         const C f = tc[(size_t)en.combo * NPM];
-        const C* wv = chunk + (size_t)(en.u - base) * CB * kPairLanes + i;
 #pragma unroll
-        for (int c = 0; c < CB; ++c) acc[c] = cadd(acc[c], cmul(wv[c * kPairLanes], f));
+        for (int c = 0; c < CB; ++c) acc[c] = cadd(acc[c], cmul(sw[en.u - base][c][i], f));
       }
-    __syncthreads();
   }
   if (mine && i < NPM) {
     C* out = ACC + (((size_t)targets[tk.first_tgt + t].acc_row * kCh + ch0) * 6 + tk.dir) * NPM + i;
@@ -2527,10 +2500,6 @@ void fmm_setup(Problem& P) {
     ensure_dynamic_smem((const void*)p2m_kernel<float>, S->smem_p2m);
   }
   ensure_dynamic_smem((const void*)m2x_kernel<double>, S->smem_m2x);
-  if (S->fp64)
-    ensure_dynamic_smem((const void*)xl_group_kernel<double>, xg_smem_bytes<double>());
-  else
-    ensure_dynamic_smem((const void*)xl_group_kernel<float>, xg_smem_bytes<float>());
   if (S->tensor) {
     ensure_dynamic_smem((const void*)op_gemm_tc_kernel<tc::kColsM2x>, tc::smem_bytes(tc::kColsM2x));
     ensure_dynamic_smem((const void*)op_gemm_tc_kernel<tc::kColsXl>, tc::smem_bytes(tc::kColsXl));
@@ -2634,7 +2603,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
     if (S.xlt_count[lev]) {
       begin(4, q);
       const int nb = S.xg_count[lev] * (kCh / kXlChannels);
-      xl_group_kernel<T><<<nb, kXgThreads, xg_smem_bytes<T>(), q>>>(tb, lev - 1, S.xg_tasks.as<XlTask>() + S.xg_first[lev],
+      xl_group_kernel<T><<<nb, kXgThreads, 0, q>>>(tb, lev - 1, S.xg_tasks.as<XlTask>() + S.xg_first[lev],
                                                    S.xl_targets.as<XlTarget>() + S.xlt_first[lev], S.xg_src.as<int>(),
                                                    S.xg_toff.as<int>(), S.xg_ents.as<XlEnt>(), W, S.acc.as<C>());
       BP_LAUNCH_CHECK();
