@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(kM2xThreads) m2x_kernel(const __grid_constant_
 }
 
 // ---------------------------------------------------------------- X2L
-// X2L is split in two.  xl_group_kernel applies the diagonal plane-wave
+// X2L is split in two.  xl_translate_kernel applies the diagonal plane-wave
 // translations (translate_up/down_wave) of every target's interaction list
 // and leaves, per (target, channel), the six accumulated waves as 6 x 2NPM
 // reals in the ACC scratch.  The conversion of those waves to a local
@@ -603,94 +603,106 @@ struct XlEntry {
 };
 constexpr int kCombos = 686;
 constexpr int kXlChannels = 4;                    // channels per translate block (one screening group)
-// Parent-stationary form of the translations.  The targets of one parent
-// (siblings) draw on largely the same sources, so a task is one (sibling
-// group, direction): the distinct source nodes the group's targets use in
-// that direction, and for each target its entries (source index u,
-// translation factor combo) sorted by u.  A block takes one task and four
-// channels; it streams the sources' waves through shared memory in chunks,
-// each source loaded once for all siblings, and thread (target slot t,
-// lane i = plane wave) sums its target's entries of the chunk in
-// registers.  Every (target, direction) belongs to exactly one task, so
-// ACC[acc_row][ch][d][i] is written once (0 without entries).
-struct XlTask {
-  int dir;
-  int first_tgt, n_tgt;  // the group's targets [first_tgt, first_tgt + n_tgt) of the level's XlTarget list
-  int src_first, n_src;  // the direction's distinct source nodes, xl_src[src_first ..]
-  int toff_first;        // target t's entries: xl_ent[xl_toff[toff_first + t] .. xl_toff[toff_first + t + 1])
-};
-struct XlEnt {
-  short u;      // index into the task's sources
-  short combo;  // translation factor: up * 343 + (a+3) * 49 + (b+3) * 7 + (c+3)
-};
-constexpr int kXgTargets = 8;                      // targets of a sibling group
-constexpr int kXgThreads = kXgTargets * kPairLanes;
-template <typename T>
-struct XgChunk;  // sources staged per pass
-template <>
-struct XgChunk<float> {
-  static constexpr int value = 16;
-};
-template <>
-struct XgChunk<double> {
-  static constexpr int value = 8;
-};
+constexpr int kXlUnroll = 2;
 
+constexpr int kXlGroups = 7;                     // lane groups of a translate block
+constexpr int kXlDirThreads = kXlGroups * kPairLanes;
+
+// One block per (target, 4 channels); thread (lane group g, lane i = plane
+// wave) sums W[src][d][ch][i] * factor[combo][i] over its share of the
+// target's entries, in registers.  The entries are sorted by direction and
+// the seven lane groups take equal contiguous slices of them, whatever the
+// mix of directions (it depends on the target's surroundings).  A slice
+// leaves one partial sum per direction it meets, in shared slot g + d (the
+// pairs (g, d) met along the list have distinct g + d, at most 12 of them);
+// then each direction's partials are added in group order (deterministic)
+// and ACC[acc_row][ch][d][i] (re, im) is stored for all six directions, 0
+// for one without entries.
+constexpr int kXlSlots = kXlGroups + 5;
 template <typename T>
-__global__ void __launch_bounds__(kXgThreads) xl_group_kernel(const __grid_constant__ Tables<T> tb, int parent_level,
-                                                              const XlTask* __restrict__ tasks,
-                                                              const XlTarget* __restrict__ targets,
-                                                              const int* __restrict__ src_nodes,
-                                                              const int* __restrict__ toff,
-                                                              const XlEnt* __restrict__ ents,
-                                                              const typename C2T<T>::type* __restrict__ W,
-                                                              typename C2T<T>::type* __restrict__ ACC) {
+__global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __grid_constant__ Tables<T> tb,
+                                                                        int parent_level,
+                                                                        const XlTarget* __restrict__ targets,
+                                                                        int n_targets,
+                                                                        const XlEntry* __restrict__ entries,
+                                                                        const typename C2T<T>::type* __restrict__ W,
+                                                                        typename C2T<T>::type* __restrict__ ACC) {
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
-  constexpr int KU = XgChunk<T>::value;
-  __shared__ C sw[KU][CB][kPairLanes];
-  const XlTask tk = tasks[blockIdx.x / (kCh / CB)];
-  const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
-  const int t = threadIdx.x / kPairLanes, i = threadIdx.x - t * kPairLanes;
+  constexpr int U = kXlUnroll;  // entries in flight per thread (measured: 2 beats 4, 6 and 8 spill)
+  __shared__ C part[kXlSlots][CB][kPairLanes];
   const int NPM = tb.np_max;
+  const int t = blockIdx.x / (kCh / CB);
+  const int ch0 = (blockIdx.x % (kCh / CB)) * CB;
+  const int g = threadIdx.x / kPairLanes, i = threadIdx.x - g * kPairLanes;
   const int lg = 2 * parent_level + (ch0 >= 8 ? 1 : 0);
+  const XlTarget tg = targets[t];  // t < n_targets: the grid has one block set per target
   const int np = tb.nexptotp[lg];
-  const bool mine = t < tk.n_tgt;
-  const bool live = mine && i < NPM && i < np;  // plane waves beyond this level's count stay 0
+  const bool live = i < NPM && i < np;  // plane waves beyond this level's count stay 0
   const C* tc = tb.tcomb + (size_t)lg * kCombos * NPM + i;
-  int e = 0, e_end = 0;
-  if (mine) {
-    e = toff[tk.toff_first + t];
-    e_end = toff[tk.toff_first + t + 1];
-  }
-  C acc[CB];
+  // sum over entries [b, e) of direction d
+  auto accum = [&](int d, int b, int e, C (&a)[CB]) {
 #pragma unroll
-  for (int c = 0; c < CB; ++c) acc[c] = cmk<C>(0, 0);
-  for (int base = 0; base < tk.n_src; base += KU) {
-    const int nu = min(KU, tk.n_src - base);
-    if (base > 0) __syncthreads();  // the previous chunk's readers are done
-    // the chunk's waves: a source's four channels of this direction are
-    // 4 NPM consecutive complex values
-    for (int o = threadIdx.x; o < nu * CB * NPM; o += blockDim.x) {
-      const int u = o / (CB * NPM), rem = o - u * (CB * NPM);
-      const int c = rem / NPM, ii = rem - c * NPM;
-      sw[u][c][ii] = W[(((size_t)src_nodes[tk.src_first + base + u] * 6 + tk.dir) * kCh + ch0 + c) * NPM + ii];
-    }
-    __syncthreads();
-    if (live)
-      for (; e < e_end; ++e) {
-        const XlEnt en = ents[e];
-        if (en.u >= base + nu) break;
-        const C f = tc[(size_t)en.combo * NPM];
+    for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
+    if (!live) return;
+    const XlEntry* ent = entries + tg.first_entry;
+    const C* Wd = W + ((size_t)d * kCh + ch0) * NPM + i;
+    for (int k0 = b; k0 < e; k0 += U) {
+      int src[U], combo[U];
 #pragma unroll
-        for (int c = 0; c < CB; ++c) acc[c] = cadd(acc[c], cmul(sw[en.u - base][c][i], f));
+      for (int u = 0; u < U; ++u) {
+        const XlEntry en = ent[min(k0 + u, e - 1)];
+        src[u] = en.src;
+        combo[u] = en.combo;
       }
-  }
-  if (mine && i < NPM) {
-    C* out = ACC + (((size_t)targets[tk.first_tgt + t].acc_row * kCh + ch0) * 6 + tk.dir) * NPM + i;
+      C tt[U], w[U][CB];
 #pragma unroll
-    for (int c = 0; c < CB; ++c) out[(size_t)c * 6 * NPM] = acc[c];
+      for (int u = 0; u < U; ++u) {
+        tt[u] = tc[(size_t)combo[u] * NPM];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) w[u][c] = Wd[((size_t)src[u] * 6 * kCh + c) * NPM];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (k0 + u < e)
+#pragma unroll
+          for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], cmul(w[u][c], tt[u]));
+    }
+  };
+  // slice [gb, ge) of the target's entries
+  const int n = tg.n_entries;
+  const int gb = (int)(((long long)g * n) / kXlGroups), ge = (int)(((long long)(g + 1) * n) / kXlGroups);
+  for (int d = 0; d < 6; ++d) {
+    const int b = max(gb, tg.dir_start[d]), e = min(ge, tg.dir_start[d + 1]);
+    if (b >= e) continue;
+    C a[CB];
+    accum(d, b, e, a);
+#pragma unroll
+    for (int c = 0; c < CB; ++c) part[g + d][c][i] = a[c];
   }
+  __syncthreads();
+  if (g < 6 && i < NPM) {
+    // direction g: the slices that meet its entries, in order
+    const int d = g, b = tg.dir_start[d], e = tg.dir_start[d + 1];
+    C a[CB];
+#pragma unroll
+    for (int c = 0; c < CB; ++c) a[c] = cmk<C>(0, 0);
+    if (b < e) {
+      const int g0 = (int)(((long long)b * kXlGroups) / max(n, 1));
+      for (int gg = max(g0 - 1, 0); gg < kXlGroups; ++gg) {
+        const int sb = (int)(((long long)gg * n) / kXlGroups), se = (int)(((long long)(gg + 1) * n) / kXlGroups);
+        if (se <= b) continue;
+        if (sb >= e) break;
+        if (max(sb, b) >= min(se, e)) continue;
+#pragma unroll
+        for (int c = 0; c < CB; ++c) a[c] = cadd(a[c], part[gg + d][c][i]);
+      }
+    }
+    C* out = ACC + (((size_t)tg.acc_row * kCh + ch0) * 6 + d) * NPM + i;
+#pragma unroll
+    for (int c = 0; c < CB; ++c) out[(size_t)c * 6 * NPM] = a[c];
+  }
+  (void)n_targets;
 }
 
 // Conversion of one accumulated-wave vector to a local expansion, applied
@@ -1704,8 +1716,6 @@ struct FmmState {
   Tables<float> tb_f{};
   DevBuf M, L, W;  // expansions and plane waves
   DevBuf p2m_items, xl_targets, xl_entries, leaf_items;
-  DevBuf xg_tasks, xg_src, xg_toff, xg_ents;  // parent-stationary translation tasks
-  std::vector<int> xg_first, xg_count;        // per level
   int n_p2m = 0, n_leaf = 0;
   size_t smem_p2m = 0, smem_shift = 0, smem_m2x = 0, smem_prep = 0, smem_eval = 0, smem_op = 0, smem_xlb = 0;
   // operator form of multipole -> plane waves and accumulated waves -> local
@@ -2380,55 +2390,6 @@ void fmm_setup(Problem& P) {
     S->xlr_count[lev] = (int)xl_ldst.size() - S->xlr_first[lev];
     if (S->tensor) xl_part += (long long)kXlSplit * ncl * R2;
   }
-  // parent-stationary translation tasks: per level, per sibling group (the
-  // targets of one parent are consecutive in xlt), per direction
-  {
-    std::vector<XlTask> tasks;
-    std::vector<int> xsrc, xtoff;
-    std::vector<XlEnt> xents;
-    S->xg_first.assign(nlev, 0);
-    S->xg_count.assign(nlev, 0);
-    for (int lev = 1; lev < nlev; ++lev) {
-      S->xg_first[lev] = (int)tasks.size();
-      const int q0 = S->xlt_first[lev], q1 = q0 + S->xlt_count[lev];
-      for (int g0 = q0; g0 < q1;) {
-        const int parent = T.nodes[xlt[g0].node].parent;
-        int g1 = g0 + 1;
-        while (g1 < q1 && T.nodes[xlt[g1].node].parent == parent) ++g1;
-        if (g1 - g0 > kXgTargets) throw std::runtime_error("more than 8 targets under one parent");
-        for (int d = 0; d < 6; ++d) {
-          std::map<int, int> u_of;  // source node -> index (sorted by node)
-          for (int q = g0; q < g1; ++q)
-            for (int k = xlt[q].dir_start[d]; k < xlt[q].dir_start[d + 1]; ++k) u_of[xle[xlt[q].first_entry + k].src] = 0;
-          if (u_of.size() > 32767) throw std::runtime_error("too many translation sources");
-          XlTask tk{d, g0 - q0, g1 - g0, (int)xsrc.size(), (int)u_of.size(), (int)xtoff.size()};
-          int u = 0;
-          for (auto& kv : u_of) {
-            kv.second = u++;
-            xsrc.push_back(kv.first);
-          }
-          for (int q = g0; q < g1; ++q) {
-            xtoff.push_back((int)xents.size());
-            std::vector<XlEnt> mine;
-            for (int k = xlt[q].dir_start[d]; k < xlt[q].dir_start[d + 1]; ++k) {
-              const XlEntry& en = xle[xlt[q].first_entry + k];
-              mine.push_back({(short)u_of[en.src], en.combo});
-            }
-            std::stable_sort(mine.begin(), mine.end(), [](const XlEnt& a, const XlEnt& b) { return a.u < b.u; });
-            xents.insert(xents.end(), mine.begin(), mine.end());
-          }
-          xtoff.push_back((int)xents.size());
-          tasks.push_back(tk);
-        }
-        g0 = g1;
-      }
-      S->xg_count[lev] = (int)tasks.size() - S->xg_first[lev];
-    }
-    S->xg_tasks = upload(c, tasks);
-    S->xg_src = upload(c, xsrc);
-    S->xg_toff = upload(c, xtoff);
-    S->xg_ents = upload(c, xents);
-  }
   S->op_tiles = upload(c, otiles);
   S->op_cols = upload(c, ocols);
   S->xl_targets = upload(c, xlt);
@@ -2602,10 +2563,10 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
     }
     if (S.xlt_count[lev]) {
       begin(4, q);
-      const int nb = S.xg_count[lev] * (kCh / kXlChannels);
-      xl_group_kernel<T><<<nb, kXgThreads, 0, q>>>(tb, lev - 1, S.xg_tasks.as<XlTask>() + S.xg_first[lev],
-                                                   S.xl_targets.as<XlTarget>() + S.xlt_first[lev], S.xg_src.as<int>(),
-                                                   S.xg_toff.as<int>(), S.xg_ents.as<XlEnt>(), W, S.acc.as<C>());
+      const int nb = S.xlt_count[lev] * (kCh / kXlChannels);
+      xl_translate_kernel<T><<<nb, kXlDirThreads, 0, q>>>(tb, lev - 1, S.xl_targets.as<XlTarget>() + S.xlt_first[lev],
+                                                      S.xlt_count[lev], S.xl_entries.as<XlEntry>(), W,
+                                                      S.acc.as<C>());
       BP_LAUNCH_CHECK();
       if (S.tensor) {  // k-range partials, then their fixed-order sum into L
         launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops.as<T>(), S.xl_tc.as<float>(), S.xl_mt,
