@@ -79,6 +79,7 @@ class bp_problem_info(C.Structure):
         ("n_patches", C.c_int64), ("n_levels", C.c_int64), ("n_nodes", C.c_int64), ("n_leaves", C.c_int64),
         ("n_nearfield_pairs", C.c_int64), ("n_nearfield_cols", C.c_int64), ("fmm_active", C.c_int64), ("device_bytes", C.c_uint64),
         ("tree_ms", C.c_double), ("assemble_ms", C.c_double), ("gmres_graph", C.c_int64),
+        ("fmm_setup_ms", C.c_double), ("setup_ms", C.c_double),
     ]
 
 

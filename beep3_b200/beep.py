@@ -220,6 +220,11 @@ class BEEP:
         self._own_engine = context is None
         # rigid-body scans: keep each mesh's own-charge potential across moves
         self.cache_own_potentials = False
+        # round the bounding cube's edge up to the grid 2^(k/8), so that
+        # scenarios of nearly the same extent (the poses of a scan) share the
+        # far-field tables and operators their context keeps; the tree then
+        # differs from the exact cube's, within the FMM's truncation error
+        self.snap_cube_edge = False
         if context is not None:
             self.device = context.device
         self._problem = None
@@ -259,6 +264,8 @@ class BEEP:
         edge = float(np.max(hi - lo))
         if edge <= 0:
             raise ValueError("degenerate bounding cube")
+        if self.snap_cube_edge:
+            edge = float(2.0 ** (np.ceil(np.log2(edge) * 8.0) / 8.0))
         self.bounding_cube = ((hi + lo) / 2.0, edge)
         return self.bounding_cube
 

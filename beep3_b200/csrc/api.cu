@@ -103,10 +103,13 @@ void finish_problem(Ctx* c, Problem& P) {
   P.d_y.alloc(c, sizeof(double) * 2 * (size_t)P.n);
   nf_build_structure(P);
   nf_assemble(P);
+  auto t1 = std::chrono::steady_clock::now();
   if (fmm_active(P)) fmm_setup(P);  // host work overlaps the assembly kernels
+  P.fmm_setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
   nf_join(P);
   matvec_setup(P);
   BP_CUDA(cudaStreamSynchronize(c->stream));
+  P.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   float ms = 0.f;
   BP_CUDA(cudaEventElapsedTime(&ms, P.asm_t0, P.asm_t1));
   P.assemble_ms = ms;
@@ -174,7 +177,8 @@ BP_API int32_t bp_ctx_destroy(bp_ctx ctx) {
                                       " mesh(es) of this context are still alive; destroy them first");
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
-    c->trim();  // the released blocks kept for reuse
+    c->fmm_plans.clear();  // their device blocks go back to the cache
+    c->trim();             // the released blocks kept for reuse
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return BP_OK;
@@ -451,6 +455,8 @@ BP_API int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info) {
   info->device_bytes = P->ctx->used;
   info->tree_ms = P->tree_ms;
   info->assemble_ms = P->assemble_ms;
+  info->fmm_setup_ms = P->fmm_setup_ms;
+  info->setup_ms = P->setup_ms;
   info->gmres_graph = P->gmres_graph ? 1 : 0;
   return BP_OK;
 }

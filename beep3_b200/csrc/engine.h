@@ -66,6 +66,8 @@ int32_t guarded_engine(F&& f) {
   }
 }
 
+struct FmmPlan;  // fmm.cu: far-field tables and operators shared by problems
+
 struct Ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
@@ -84,6 +86,10 @@ struct Ctx {
   // problems and meshes made on the context and not yet deleted: the
   // context may not be destroyed under them
   std::atomic<int> live_problems{0}, live_meshes{0};
+  // far-field plans of recent problems, most recently used last
+  std::vector<std::shared_ptr<FmmPlan>> fmm_plans;
+  std::mutex plan_mu;
+  static constexpr size_t kFmmPlans = 4;
   // released blocks beyond this are freed at once, the longest unused first
   static constexpr uint64_t kCacheMax = 16ull << 30;
 
@@ -359,7 +365,7 @@ struct Problem {
   // right-hand side of bp_solve): kept so repeated calls allocate nothing
   DevBuf scratch_charges, scratch_vals, scratch_b;
   int krylov_m = 0;
-  double tree_ms = 0, assemble_ms = 0;
+  double tree_ms = 0, assemble_ms = 0, fmm_setup_ms = 0, setup_ms = 0;
   // the near-field assembly runs on a stream of its own while the far field
   // is set up; its inputs stay allocated until it is joined (nf_join)
   cudaStream_t asm_stream = nullptr;

@@ -1710,7 +1710,9 @@ __global__ void __launch_bounds__(256) prep_csr_kernel(int E, int EQ, const Leaf
 struct FmmState {
   int nt = 9, E = 55, nlev = 0, np_max = 0, nl = 0;
   bool fp64 = true;
-  DevBuf tables_buf;    // one allocation holding every table
+  // buffers a far-field plan shares among problems (see FmmPlan)
+  using SharedBuf = std::shared_ptr<DevBuf>;
+  SharedBuf tables_buf = std::make_shared<DevBuf>();  // one allocation holding every table
   DevBuf tables_buf_d;  // FP64 tables used only to tabulate operators of an FP32 problem
   Tables<double> tb_d{};
   Tables<float> tb_f{};
@@ -1719,15 +1721,15 @@ struct FmmState {
   int n_p2m = 0, n_leaf = 0;
   size_t smem_p2m = 0, smem_shift = 0, smem_m2x = 0, smem_prep = 0, smem_eval = 0, smem_op = 0, smem_xlb = 0;
   // operator form of multipole -> plane waves and accumulated waves -> local
-  DevBuf m2x_ops;  // [lg][2E][m2x_rp]
-  DevBuf xl_ops;   // [lg][12 NPM][xl_rp]
+  SharedBuf m2x_ops = std::make_shared<DevBuf>();  // [lg][2E][m2x_rp]
+  SharedBuf xl_ops = std::make_shared<DevBuf>();   // [lg][12 NPM][xl_rp]
   int m2x_rp = 0, xl_rp = 0;
   DevBuf op_tiles, op_cols;
   DevBuf acc;      // [target row][channel][6 dirs][NPM] accumulated waves
   // FP32 engine: the same operators packed for the tensor cores (hi / lo
   // halves in the MMA's shared-memory layout), row tiles and k chunks
   bool tensor = false;
-  DevBuf m2x_tc, xl_tc;
+  SharedBuf m2x_tc = std::make_shared<DevBuf>(), xl_tc = std::make_shared<DevBuf>();
   int m2x_mt = 0, m2x_nc = 0, xl_mt = 0, xl_nc = 0;
   DevBuf tc_status;  // int[2]: [0] set by a tensor-core kernel whose wait timed out; [1] timeout test switch
   // split-K wave -> local: per level the columns' L offsets and the partials
@@ -1740,11 +1742,12 @@ struct FmmState {
   DevBuf eval_basis;  // [eval item][2 groups][EQ][kEvalChunk], geometry only
   int n_eval = 0;
   // operator form of M2M / L2L and of the L2P preparation
-  DevBuf shift_ops;  // [op][k][r], op = ((kind*nlev + level)*2 + group)*8 + octant-1
+  SharedBuf shift_ops = std::make_shared<DevBuf>();  // [op][k][r], op = ((kind*nlev + level)*2 + group)*8 + octant-1
   DevBuf shift_tiles, shift_cols, m2m_reduce, m2m_partials;
   std::vector<int> m2m_tfirst, m2m_tcount, m2m_rfirst, m2m_rcount;  // per child level
   std::vector<int> l2l_tfirst, l2l_tcount;                          // per parent level
-  DevBuf prep_rowptr, prep_cols, prep_vals;
+  SharedBuf prep_rowptr = std::make_shared<DevBuf>(), prep_cols = std::make_shared<DevBuf>(),
+            prep_vals = std::make_shared<DevBuf>();
   size_t smem_gemm = 0, smem_csr = 0;
   // per level: M2X tiles of the level's nodes, X2L targets on the level and
   // their conversion tiles; a stream per level runs them as soon as the
@@ -1759,6 +1762,76 @@ struct FmmState {
     for (cudaStream_t t : lstreams) cudaStreamDestroy(t);
   }
 };
+
+// The part of a far-field set-up that depends only on the FMM order, the
+// screening constants, the cube edge, the number of levels and the
+// precision: the device tables and the dense operators tabulated from them
+// (M2M / L2L shifts, L2P preparation for every level, multipole -> waves
+// and waves -> local, packed for the tensor cores in the FP32 engine).  A
+// context keeps its few most recent plans; a problem built on it with the
+// same key (a pose of a scan whose bounding cube is unchanged) adopts the
+// plan instead of computing it, and holds it while it lives.
+struct FmmPlan {
+  int nt = 0, nlev = 0;
+  double kappa = 0, beta0 = 0, edge = 0;
+  bool fp64 = true;
+  int np_max = 0, nl = 0;
+  Tables<double> tb_d{};
+  Tables<float> tb_f{};
+  FmmState::SharedBuf tables_buf, shift_ops, prep_rowptr, prep_cols, prep_vals, m2x_ops, xl_ops, m2x_tc, xl_tc;
+  int m2x_mt = 0, m2x_nc = 0, xl_mt = 0, xl_nc = 0;
+  size_t smem_csr = 0;
+  bool matches(const Problem& P, int levels) const {
+    return nt == P.params.nterms && nlev == levels && kappa == P.params.kappa && beta0 == P.params.beta0 &&
+           edge == P.params.cube_edge && fp64 == P.fp64;
+  }
+};
+
+static std::shared_ptr<FmmPlan> find_fmm_plan(Problem& P, int levels) {
+  Ctx* c = P.ctx;
+  std::lock_guard<std::mutex> lk(c->plan_mu);
+  for (size_t k = 0; k < c->fmm_plans.size(); ++k)
+    if (c->fmm_plans[k]->matches(P, levels)) {
+      std::shared_ptr<FmmPlan> p = c->fmm_plans[k];
+      c->fmm_plans.erase(c->fmm_plans.begin() + k);
+      c->fmm_plans.push_back(p);  // most recently used last
+      return p;
+    }
+  return nullptr;
+}
+
+static void keep_fmm_plan(Problem& P, const FmmState& S) {
+  auto p = std::make_shared<FmmPlan>();
+  p->nt = S.nt;
+  p->nlev = S.nlev;
+  p->kappa = P.params.kappa;
+  p->beta0 = P.params.beta0;
+  p->edge = P.params.cube_edge;
+  p->fp64 = S.fp64;
+  p->np_max = S.np_max;
+  p->nl = S.nl;
+  if (S.fp64)
+    p->tb_d = S.tb_d;  // an FP32 plan's FP64 tables were only used to tabulate its operators
+  p->tb_f = S.tb_f;
+  p->tables_buf = S.tables_buf;
+  p->shift_ops = S.shift_ops;
+  p->prep_rowptr = S.prep_rowptr;
+  p->prep_cols = S.prep_cols;
+  p->prep_vals = S.prep_vals;
+  p->m2x_ops = S.m2x_ops;
+  p->xl_ops = S.xl_ops;
+  p->m2x_tc = S.m2x_tc;
+  p->xl_tc = S.xl_tc;
+  p->m2x_mt = S.m2x_mt;
+  p->m2x_nc = S.m2x_nc;
+  p->xl_mt = S.xl_mt;
+  p->xl_nc = S.xl_nc;
+  p->smem_csr = S.smem_csr;
+  Ctx* c = P.ctx;
+  std::lock_guard<std::mutex> lk(c->plan_mu);
+  c->fmm_plans.push_back(p);
+  while (c->fmm_plans.size() > Ctx::kFmmPlans) c->fmm_plans.erase(c->fmm_plans.begin());
+}
 
 void fmm_destroy(FmmState* s) { delete s; }
 
@@ -1958,7 +2031,7 @@ __global__ void csr_fill_kernel(const T* __restrict__ D, int nb, int rows, const
 }
 
 template <typename T>
-static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const std::vector<LeafItem>& leaves) {
+static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb) {
   using C = typename C2T<T>::type;
   Ctx* c = P.ctx;
   cudaStream_t st = c->stream;
@@ -1966,15 +2039,17 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
   const int EQ = (NT + 3) * (NT + 4) / 2;
   // shifts: kind 0 = M2M (level = child level), kind 1 = L2L (level = parent level)
   const int n_ops = 2 * nlev * 2 * 8;
-  S.shift_ops.alloc(c, sizeof(T) * (size_t)n_ops * R * ((R + 3) & ~3));
-  shift_basis_kernel<T><<<n_ops * R, 64, S.smem_shift, st>>>(tb, nlev, S.shift_ops.as<T>());
+  S.shift_ops->alloc(c, sizeof(T) * (size_t)n_ops * R * ((R + 3) & ~3));
+  shift_basis_kernel<T><<<n_ops * R, 64, S.smem_shift, st>>>(tb, nlev, S.shift_ops->as<T>());
   BP_LAUNCH_CHECK();
   // L2P preparation operator per level that holds leaves: tabulated on unit
   // inputs (dense columns [b][rows]) and compacted to CSR on the device, the
   // nonzeros of a row in column order
   const int nb = kCh * R, rows = 8 * 2 * EQ;
-  std::vector<int> levels_with_leaves(nlev, 0);
-  for (const LeafItem& lf : leaves) levels_with_leaves[lf.level] = 1;
+  // every level below the root may hold leaves of a problem that shares the
+  // operators
+  std::vector<int> levels_with_leaves(nlev, 1);
+  levels_with_leaves[0] = 0;
   DevBuf Lb(c, sizeof(C) * (size_t)nb * kCh * E);
   prep_basis_inputs<T><<<nb, 128, 0, st>>>(E, nb, Lb.as<C>());
   BP_LAUNCH_CHECK();
@@ -2007,18 +2082,18 @@ static void build_operators(Problem& P, FmmState& S, const Tables<T>& tb, const 
     }
     rp[rows] = nnz;
   }
-  S.prep_rowptr = upload(c, rowptr);
-  S.prep_cols.alloc(c, sizeof(int) * (size_t)std::max(1, nnz));
-  S.prep_vals.alloc(c, sizeof(T) * (size_t)std::max(1, nnz));
+  *S.prep_rowptr = upload(c, rowptr);
+  S.prep_cols->alloc(c, sizeof(int) * (size_t)std::max(1, nnz));
+  S.prep_vals->alloc(c, sizeof(T) * (size_t)std::max(1, nnz));
   if (nnz == 0) {
-    BP_CUDA(cudaMemsetAsync(S.prep_cols.get(), 0, sizeof(int), st));
-    BP_CUDA(cudaMemsetAsync(S.prep_vals.get(), 0, sizeof(T), st));
+    BP_CUDA(cudaMemsetAsync(S.prep_cols->get(), 0, sizeof(int), st));
+    BP_CUDA(cudaMemsetAsync(S.prep_vals->get(), 0, sizeof(T), st));
   }
   for (int lev = 0; lev < nlev; ++lev) {
     if (!levels_with_leaves[lev]) continue;
     csr_fill_kernel<T><<<(rows + 7) / 8, 256, 0, st>>>(Db[lev].as<T>(), nb, rows,
-                                                       S.prep_rowptr.as<int>() + (size_t)lev * (rows + 1),
-                                                       S.prep_cols.as<int>(), S.prep_vals.as<T>());
+                                                       S.prep_rowptr->as<int>() + (size_t)lev * (rows + 1),
+                                                       S.prep_cols->as<int>(), S.prep_vals->as<T>());
     BP_LAUNCH_CHECK();
   }
   S.smem_csr = sizeof(T) * (size_t)kCh * R;
@@ -2112,11 +2187,11 @@ static void build_wave_operators(Problem& P, FmmState& S) {
                                                           out.as<float>());
       BP_LAUNCH_CHECK();
     };
-    pack(m2x, R2, S.m2x_rp, KW, S.m2x_mt, S.m2x_nc, S.m2x_tc);
-    pack(xl, KW, S.xl_rp, R2, S.xl_mt, S.xl_nc, S.xl_tc);
+    pack(m2x, R2, S.m2x_rp, KW, S.m2x_mt, S.m2x_nc, *S.m2x_tc);
+    pack(xl, KW, S.xl_rp, R2, S.xl_mt, S.xl_nc, *S.xl_tc);
   } else {  // the FP64 engine (the FP32 engine always takes the tensor cores)
-    S.m2x_ops = std::move(m2x);
-    S.xl_ops = std::move(xl);
+    *S.m2x_ops = std::move(m2x);
+    *S.xl_ops = std::move(xl);
   }
   BP_CUDA(cudaStreamSynchronize(st));
 }
@@ -2135,8 +2210,15 @@ void fmm_setup(Problem& P) {
   S->E = (S->nt + 1) * (S->nt + 2) / 2;
   S->nlev = T.n_levels;
   S->fp64 = P.fp64;
-  // FP64 tables always: they tabulate the dense operators of both engines
-  {
+  const std::shared_ptr<FmmPlan> plan = find_fmm_plan(P, S->nlev);
+  if (plan) {
+    S->tables_buf = plan->tables_buf;
+    S->tb_d = plan->tb_d;
+    S->tb_f = plan->tb_f;
+    S->np_max = plan->np_max;
+    S->nl = plan->nl;
+  } else {
+    // FP64 tables always: they tabulate the dense operators of both engines
     // host tables (FP64) once; both engines' device copies are made from them
     GlobalTables G;
     G.build(S->nt);
@@ -2146,8 +2228,8 @@ void fmm_setup(Problem& P) {
       LT[2 * l].build(S->nt, beta, l, P.params.cube_edge);
       LT[2 * l + 1].build(S->nt, P.params.beta0, l, P.params.cube_edge);
     }
-    fill_tables<double>(*S, P, S->tb_d, S->fp64 ? S->tables_buf : S->tables_buf_d, G, LT);
-    if (!S->fp64) fill_tables<float>(*S, P, S->tb_f, S->tables_buf, G, LT);
+    fill_tables<double>(*S, P, S->tb_d, S->fp64 ? *S->tables_buf : S->tables_buf_d, G, LT);
+    if (!S->fp64) fill_tables<float>(*S, P, S->tb_f, *S->tables_buf, G, LT);
   }
   if (S->np_max > kPairLanes) throw std::invalid_argument("FMM order too large for the plane-wave thread layout");
   const int nn = (int)T.nodes.size();
@@ -2470,12 +2552,29 @@ void fmm_setup(Problem& P) {
   // device copy of the tree contents (node-major)
   P.fmm_contents = upload(c, T.contents);
   BP_CUDA(cudaStreamSynchronize(c->stream));
-  if (S->fp64)
-    build_operators<double>(P, *S, S->tb_d, leaves);
-  else
-    build_operators<float>(P, *S, S->tb_f, leaves);
-  build_wave_operators(P, *S);
-  S->tables_buf_d.reset();  // the FP64 copy of an FP32 problem's tables is no longer needed
+  if (plan) {
+    S->shift_ops = plan->shift_ops;
+    S->prep_rowptr = plan->prep_rowptr;
+    S->prep_cols = plan->prep_cols;
+    S->prep_vals = plan->prep_vals;
+    S->m2x_ops = plan->m2x_ops;
+    S->xl_ops = plan->xl_ops;
+    S->m2x_tc = plan->m2x_tc;
+    S->xl_tc = plan->xl_tc;
+    S->m2x_mt = plan->m2x_mt;
+    S->m2x_nc = plan->m2x_nc;
+    S->xl_mt = plan->xl_mt;
+    S->xl_nc = plan->xl_nc;
+    S->smem_csr = plan->smem_csr;
+  } else {
+    if (S->fp64)
+      build_operators<double>(P, *S, S->tb_d);
+    else
+      build_operators<float>(P, *S, S->tb_f);
+    build_wave_operators(P, *S);
+    S->tables_buf_d.reset();  // the FP64 copy of an FP32 problem's tables is no longer needed
+    keep_fmm_plan(P, *S);
+  }
   // geometry-only bases of P2M and of the L2P evaluation
   const double* cen = P.d_centroid.as<double>();
   if (S->fp64) {
@@ -2556,7 +2655,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   auto level_x = [&](int lev, cudaStream_t q) {
     if (S.m2x_tcount[lev]) {
       begin(3, q);
-      launch_op_gemm<T>(S, S.m2x_tfirst[lev], S.m2x_tcount[lev], S.m2x_ops.as<T>(), S.m2x_tc.as<float>(), S.m2x_mt,
+      launch_op_gemm<T>(S, S.m2x_tfirst[lev], S.m2x_tcount[lev], S.m2x_ops->as<T>(), S.m2x_tc->as<float>(), S.m2x_mt,
                         S.m2x_nc, R2, S.m2x_rp, KW, 2 * NPM, (long long)kCh * 2 * NPM,
                         reinterpret_cast<const T*>(M), reinterpret_cast<T*>(W), q, tc::kColsM2x);
       end(1);
@@ -2569,7 +2668,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
                                                       S.acc.as<C>());
       BP_LAUNCH_CHECK();
       if (S.tensor) {  // k-range partials, then their fixed-order sum into L
-        launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops.as<T>(), S.xl_tc.as<float>(), S.xl_mt,
+        launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops->as<T>(), S.xl_tc->as<float>(), S.xl_mt,
                           S.xl_nc, KW, S.xl_rp, R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()),
                           reinterpret_cast<T*>(S.xl_partials.as<float>()), q, tc::kColsXl);
         const long long total = (long long)S.xlr_count[lev] * R2;
@@ -2580,7 +2679,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
         BP_LAUNCH_CHECK();
         end(3);
       } else {
-        launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops.as<T>(), S.xl_tc.as<float>(), S.xl_mt,
+        launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops->as<T>(), S.xl_tc->as<float>(), S.xl_mt,
                           S.xl_nc, KW, S.xl_rp, R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()),
                           reinterpret_cast<T*>(Lx), q, tc::kColsXl);
         end(2);
@@ -2620,7 +2719,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
       begin(2, s);
       shift_gemm_kernel<T><<<S.m2m_tcount[lev + 1], kGemmThreads, S.smem_gemm, s>>>(
           S.E, S.shift_tiles.as<ShiftTile>() + S.m2m_tfirst[lev + 1], S.shift_cols.as<ShiftCol>(),
-          S.shift_ops.as<T>(), Mr, Pr);
+          S.shift_ops->as<T>(), Mr, Pr);
       BP_LAUNCH_CHECK();
       shift_reduce_kernel<T><<<S.m2m_rcount[lev + 1], 256, 0, s>>>(
           S.E, S.m2m_reduce.as<ShiftReduce>() + S.m2m_rfirst[lev + 1], Pr, Mr);
@@ -2636,7 +2735,7 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
     join_x(lev + 1);
     begin(6, s);
     shift_gemm_kernel<T><<<S.l2l_tcount[lev], kGemmThreads, S.smem_gemm, s>>>(
-        S.E, S.shift_tiles.as<ShiftTile>() + S.l2l_tfirst[lev], S.shift_cols.as<ShiftCol>(), S.shift_ops.as<T>(),
+        S.E, S.shift_tiles.as<ShiftTile>() + S.l2l_tfirst[lev], S.shift_cols.as<ShiftCol>(), S.shift_ops->as<T>(),
         reinterpret_cast<const T*>(Lx), reinterpret_cast<T*>(Lx));
     BP_LAUNCH_CHECK();
     end(1);
@@ -2645,8 +2744,8 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   begin(5, s);
   {
     const int NT = S.nt, EQ = (NT + 3) * (NT + 4) / 2;
-    prep_csr_kernel<T><<<S.n_leaf, 256, S.smem_csr, s>>>(S.E, EQ, S.leaf_items.as<LeafItem>(), S.prep_rowptr.as<int>(),
-                                                          S.prep_cols.as<int>(), S.prep_vals.as<T>(),
+    prep_csr_kernel<T><<<S.n_leaf, 256, S.smem_csr, s>>>(S.E, EQ, S.leaf_items.as<LeafItem>(), S.prep_rowptr->as<int>(),
+                                                          S.prep_cols->as<int>(), S.prep_vals->as<T>(),
                                                           reinterpret_cast<const T*>(Lx),
                                                           reinterpret_cast<T*>(S.leaf_exp.as<C>()));
     BP_LAUNCH_CHECK();

@@ -58,8 +58,9 @@ def random_poses(n: int, seed: int, rmin: float = 45.0, rmax: float = 80.0) -> l
     return out
 
 
-def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it, context=None):
+def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it, context=None, snap=False):
     bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
+    bp.snap_cube_edge = snap
     try:
         for mesh, off, q in instances:
             bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
@@ -71,7 +72,7 @@ def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it, cont
 
 
 def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, tol, max_it, context=None,
-                 isolated=()):
+                 isolated=(), snap=False):
     """Poses idx on one engine context: the two meshes stay on the device and
     each pose only moves instance B (a new tree, near field and far-field
     set-up, then the solve).  The single-molecule problems in ``isolated``
@@ -79,9 +80,10 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
     energies)."""
     bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
     bp.cache_own_potentials = True  # instance B only moves: its own potential, and A's, stay
+    bp.snap_cube_edge = snap
     out = []
     try:
-        iso = [_solve_energy(inst, kappa, precision, nbsize, device, tol, max_it, context=bp.engine)[0]
+        iso = [_solve_energy(inst, kappa, precision, nbsize, device, tol, max_it, context=bp.engine, snap=snap)[0]
                for inst in isolated]
         if not idx:
             return out, iso
@@ -102,10 +104,16 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
 
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
                     nbsize: int = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
-                    max_iterations: int = 100, contexts: list | None = None) -> ScanResult:
+                    max_iterations: int = 100, contexts: list | None = None,
+                    snap_cube_edges: bool = False) -> ScanResult:
     """``contexts``: EngineContexts for the workers (at least ``workers``), kept
     by the caller across scans so that the meshes and device blocks stay on
-    the device; by default each worker has its own for this scan."""
+    the device; by default each worker has its own for this scan.
+    ``snap_cube_edges``: round each pose's bounding-cube edge up to a grid
+    (BEEP.snap_cube_edge), so that poses of similar extent share the
+    far-field tables and operators a context keeps instead of computing them
+    per pose; energies then differ from the exact cube's by the FMM's
+    truncation error."""
     t0 = time.perf_counter()
     ident = np.array([1.0, 0.0, 0.0, 0.0])
     ca = mesh_a.centre
@@ -119,7 +127,8 @@ def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float 
     isolated[1 % workers].append([(mesh_b, mesh_b.centre, ident)])
     with ThreadPoolExecutor(max_workers=workers) as ex:
         fw = [ex.submit(_scan_worker, mesh_a, mesh_b, poses, list(range(w, len(poses), workers)), kappa, precision,
-                        nbsize, device, tol, max_iterations, contexts[w] if contexts else None, isolated[w])
+                        nbsize, device, tol, max_iterations, contexts[w] if contexts else None, isolated[w],
+                        snap_cube_edges)
               for w in range(workers)]
         outs = [f.result() for f in fw]
     e_a = outs[0][1][0]

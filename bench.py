@@ -405,9 +405,11 @@ def _scan_mode(args, local):
     try:
         # warm-up: a scan of as many other poses, so that every context has
         # seen problems of the sizes the timed scan builds
+        snap = not args.exact_cubes
         rigid_body_scan(ma, mb, random_poses(args.poses, seed=99), kappa=0.1, workers=args.workers, device=local,
-                        contexts=ctxs)
-        res = rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs)
+                        contexts=ctxs, snap_cube_edges=snap)
+        res = rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs,
+                              snap_cube_edges=snap)
     finally:
         for c in ctxs:
             c.close()
@@ -419,7 +421,9 @@ def _scan_mode(args, local):
         "config": {"workload": "batched rigid-body scan: star k=6 (40962 patches, 2000 charges) + star k=5 "
                                "(10242 patches, 500 charges), kappa 0.1, separation 45-80 A",
                    "poses": len(poses), "concurrent_poses": args.workers,
-                   "engine_contexts": "one per worker, kept across scans"},
+                   "engine_contexts": "one per worker, kept across scans",
+                   "cube_edges": "exact per pose" if args.exact_cubes else
+                                 "rounded up to 2^(k/8): poses share far-field plans"},
         "seconds": res.seconds, "mean_iterations": float(np.mean(res.iterations)),
         "interaction_energy_kj_per_mol": {"min": float(e.min()), "max": float(e.max()), "mean": float(e.mean())},
     }), flush=True)
@@ -597,6 +601,8 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--exact-cubes", action="store_true",
+                    help="scan: each pose's exact bounding cube (no far-field plan sharing)")
     ap.add_argument("--prepare-inputs", metavar="NPZ", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.prepare_inputs:

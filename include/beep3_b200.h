@@ -153,6 +153,8 @@ typedef struct {
   int64_t gmres_graph;       /* 1 once a solve ran its Arnoldi loop as one CUDA graph with a
                                 device-side loop condition, 0 before the first solve or when the
                                 host drove the loop step by step */
+  double fmm_setup_ms;       /* host wall time of the far-field set-up (tables, operators, schedule) */
+  double setup_ms;           /* host wall time from the tree build to a problem ready to run */
 } bp_problem_info;
 
 /* Builds the adaptive octree, the singular self-patch integrals and the

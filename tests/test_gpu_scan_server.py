@@ -45,3 +45,42 @@ def test_server_mix_equals_alone():
         assert a_.energy_kj_per_mol == m_.energy_kj_per_mol
     p = latency_percentiles(mix)
     assert p["p99"] >= p["p50"] > 0
+
+
+def test_far_field_plan_shared_between_problems():
+    """A problem whose far-field key (order, kappa, cube edge, levels,
+    precision) matches a plan its context keeps adopts it: its results are
+    bitwise those of the same problem built on a fresh context, and its
+    set-up skips the tables and operators."""
+    a = small_star(4, 7, radius=20.0, n_charges=30)
+    res = {}
+    for precision in ("mixed", "fp64"):
+        shared = b.EngineContext(0)
+        times = []
+        ys = []
+        for _ in range(2):
+            bp = b.BEEP(kappa=0.1, nbsize=100, precision=precision, context=shared)
+            bp.insert_mesh_instance(a)
+            inf = bp.info()
+            assert inf.fmm_active == 1
+            times.append(inf.fmm_setup_ms)
+            x = np.random.default_rng(1).standard_normal(2 * bp.num_patches)
+            ys.append(bp.matvec(x))
+            bp.close()
+        fresh = b.BEEP(kappa=0.1, nbsize=100, precision=precision)
+        fresh.insert_mesh_instance(a)
+        y_fresh = fresh.matvec(x)
+        fresh.close()
+        shared.close()
+        assert np.array_equal(ys[1], ys[0]) and np.array_equal(ys[1], y_fresh)
+        res[precision] = times
+    assert res["mixed"][1] < res["mixed"][0]
+
+
+def test_scan_with_snapped_cubes_matches_exact_cubes():
+    a, c = small_star(4, 11, radius=20.0, n_charges=30), small_star(3, 12, radius=10.0)
+    poses = random_poses(6, seed=5, rmin=35.0, rmax=45.0)
+    exact = rigid_body_scan(a, c, poses, kappa=0.1, workers=2, nbsize=150)
+    snapped = rigid_body_scan(a, c, poses, kappa=0.1, workers=2, nbsize=150, snap_cube_edges=True)
+    ce, cs = np.array(exact.complex_energies), np.array(snapped.complex_energies)
+    assert np.max(np.abs(cs - ce) / np.abs(ce)) < 1e-4
