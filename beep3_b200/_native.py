@@ -104,6 +104,7 @@ _SIGS = {
     "bp_geom_destroy": [_P],
     "bp_problem_create": [_P, C.POINTER(bp_patches), C.POINTER(bp_params), _PP],
     "bp_mesh_create": [_P, C.POINTER(bp_patches), _P, _PP],
+    "bp_mesh_create_from_surface": [_P, _I, _P, _P, _I, _P, _I, _I, _I, _P, _PP, _P],
     "bp_mesh_destroy": [_P],
     "bp_problem_create_posed": [_P, C.POINTER(bp_instance), _I, C.POINTER(bp_params), _PP],
     "bp_problem_destroy": [_P],

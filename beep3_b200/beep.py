@@ -52,6 +52,8 @@ class Mesh:
                  centre=None, vertex_normals=None):
         self.vertices = np.ascontiguousarray(vertices, float)
         self.triangles = np.ascontiguousarray(triangles, np.int32)
+        self.planar, self.qual_rule, self.quad_rule = bool(planar), int(qual_rule), int(quad_rule)
+        self.vertex_normals = None if vertex_normals is None else np.ascontiguousarray(vertex_normals, float)
         self.charges = np.ascontiguousarray(np.asarray(charges, float).reshape(-1, 4))
         self.patches: PatchSet = prepare_patches(self.vertices, self.triangles, planar, qual_rule, quad_rule,
                                                  vertex_normals)
@@ -118,11 +120,16 @@ class EngineContext:
     upload no mesh and reuse the device blocks of the earlier ones.  One
     thread at a time."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_meshes: int = 8):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_meshes: int = 8,
+                 device_geometry: bool = False):
         """``max_meshes``: device-resident meshes kept; beyond it the least
-        recently used one not needed by the scenario being built goes."""
+        recently used one not needed by the scenario being built goes.
+        ``device_geometry``: a mesh's node patches and point lists are
+        generated on the device from its surface (bp_mesh_create_from_surface,
+        bit for bit the host preparation) instead of being uploaded."""
         self.device = int(device)
         self.max_meshes = int(max_meshes)
+        self.device_geometry = bool(device_geometry)
         self._ctx = C.c_void_p()
         N.check(N.lib().bp_ctx_create(self.device, int(hbm_budget_bytes), C.byref(self._ctx)))
         # id(mesh) -> [mesh, handle, build in which it was last used]; holding
@@ -146,13 +153,20 @@ class EngineContext:
             stale = sorted((e[2], k) for k, e in self._meshes.items() if e[2] < self._build)
             while len(self._meshes) >= self.max_meshes and stale:
                 N.lib().bp_mesh_destroy(self._meshes.pop(stale.pop(0)[1])[1])
-            p = mesh.patches
-            pp = N.bp_patches(p.n, N.ptr(p.centroid), N.ptr(p.normal), N.ptr(p.area), None, None,
-                              N.ptr(p.qual_off), N.ptr(p.qual), N.ptr(p.quad_off), N.ptr(p.quad),
-                              N.ptr(p.gal_off), N.ptr(p.gal))
             h = C.c_void_p()
-            N.check(N.lib().bp_mesh_create(self._ctx, C.byref(pp), N.ptr(np.ascontiguousarray(mesh.centre)),
-                                           C.byref(h)))
+            if self.device_geometry:
+                vn = mesh.vertex_normals
+                N.check(N.lib().bp_mesh_create_from_surface(
+                    self._ctx, len(mesh.vertices), N.ptr(mesh.vertices), N.ptr(vn), len(mesh.triangles),
+                    N.ptr(mesh.triangles), int(mesh.planar), mesh.qual_rule, mesh.quad_rule,
+                    N.ptr(np.ascontiguousarray(mesh.centre)), C.byref(h), None))
+            else:
+                p = mesh.patches
+                pp = N.bp_patches(p.n, N.ptr(p.centroid), N.ptr(p.normal), N.ptr(p.area), None, None,
+                                  N.ptr(p.qual_off), N.ptr(p.qual), N.ptr(p.quad_off), N.ptr(p.quad),
+                                  N.ptr(p.gal_off), N.ptr(p.gal))
+                N.check(N.lib().bp_mesh_create(self._ctx, C.byref(pp), N.ptr(np.ascontiguousarray(mesh.centre)),
+                                               C.byref(h)))
             entry = [mesh, h, self._build]
             self._meshes[id(mesh)] = entry
         entry[2] = self._build

@@ -22,6 +22,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                      "--expt-relaxed-constexpr", "-I", str(INCLUDE)]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I", str(INCLUDE)]
+# per-source nvcc flags: the device mesh generator shares the host
+# preparation's surface code and must round as the host does (no FMA)
+NVCC_FILE_FLAGS = {"mesh_gen.cu": ["--fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -57,7 +60,8 @@ def build(verbose: bool = False, extra_nvcc: list[str] | None = None) -> Path:
         if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest_header):
             continue
         if src.suffix == ".cu":
-            cmd = [nvcc, *NVCC_FLAGS, *(extra_nvcc or []), "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc, *NVCC_FLAGS, *NVCC_FILE_FLAGS.get(src.name, []), *(extra_nvcc or []), "-c", str(src), "-o",
+                   str(obj)]
         else:
             cmd = ["g++", *CXX_FLAGS, "-I", str(_cuda_home() / "include"), "-c", str(src), "-o", str(obj)]
         if verbose:

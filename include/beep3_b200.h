@@ -179,6 +179,17 @@ int32_t bp_problem_create(bp_ctx ctx, const bp_patches* patches, const bp_params
  */
 typedef struct bp_mesh_s* bp_mesh;
 int32_t bp_mesh_create(bp_ctx ctx, const bp_patches* patches, const double centre[3], bp_mesh* out);
+/* The same device-resident mesh generated on the device from a closed
+ * triangulated surface (vertices [n_vertices][3], optional unit vertex
+ * normals (NULL or zero rows: area-weighted), anticlockwise triangles
+ * [n_triangles][3]): the node patches and point lists bp_geom_create makes on
+ * the host (Mesh::create_bezier_triangles / create_node_patches,
+ * src/bem/mesh.cpp:1632-1652), bit for bit, with no host point generation or
+ * upload.  totals (may be NULL) = {curved area, planar area}. */
+int32_t bp_mesh_create_from_surface(bp_ctx ctx, int32_t n_vertices, const double* vertices,
+                                    const double* vertex_normals, int32_t n_triangles, const int32_t* triangles,
+                                    int32_t planar, int32_t qual_rule, int32_t quad_rule, const double centre[3],
+                                    bp_mesh* out, double* totals);
 int32_t bp_mesh_destroy(bp_mesh mesh);
 
 typedef struct {
