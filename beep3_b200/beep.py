@@ -212,13 +212,17 @@ class BEEP:
 
     def __init__(self, eps_solvent: float = 80.0, kappa: float = 0.1, nbsize: int = DEFAULT_NBSIZE,
                  nterms: int = 9, precision: str = "fp64", device: int = 0, hbm_budget_bytes: int = 0,
-                 context: EngineContext | None = None, nearfield_on_demand: bool = False):
+                 context: EngineContext | None = None, nearfield_on_demand: bool = False,
+                 tree: str = "reference", leaf_size: int = 64):
         """``context``: an EngineContext shared with scenarios run before or
         after this one (its device and budget apply); by default the scenario
         has its own.  ``nearfield_on_demand``: recompute the near field in
         every matvec instead of caching its coefficients (the reference's
         uncached GPU path): no coefficient memory, the assembly's cost per
-        matvec."""
+        matvec.  ``tree``: "reference" (the reference's octree rules, driven
+        by ``nbsize``) or "device" (built on the GPU from Morton codes, at
+        most ``leaf_size`` patches per leaf; same neighbourhood rule, a
+        different near/far split, so results agree to the FMM's accuracy)."""
         self.eps_solvent = float(eps_solvent)
         self.kappa = float(kappa)
         self.nbsize = int(nbsize)
@@ -227,6 +231,12 @@ class BEEP:
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.precision = precision
         self.nearfield_on_demand = bool(nearfield_on_demand)
+        if tree not in ("reference", "device"):
+            raise ValueError("tree must be 'reference' or 'device'")
+        self.tree_kind = tree
+        self.leaf_size = int(leaf_size)
+        if self.leaf_size <= 0:
+            raise ValueError("leaf_size must be positive")
         self.instances: list[MeshInstance] = []
         self.device = int(device)
         self.hbm_budget_bytes = int(hbm_budget_bytes)
@@ -373,9 +383,11 @@ class BEEP:
             insts[k].rotation[:] = [float(v) for v in inst.matrix.ravel()]
             insts[k].offset[:] = [float(v) for v in inst.offset]
             insts[k].dielectric_ratio = inst.dielectric_ratio
-        prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge, self.nbsize, self.nterms,
-                          N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED,
-                          N.BP_FLAG_NEARFIELD_ON_DEMAND if self.nearfield_on_demand else 0)
+        flags = ((N.BP_FLAG_NEARFIELD_ON_DEMAND if self.nearfield_on_demand else 0) |
+                 (N.BP_FLAG_DEVICE_TREE if self.tree_kind == "device" else 0))
+        prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge,
+                          self.leaf_size if self.tree_kind == "device" else self.nbsize, self.nterms,
+                          N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED, flags)
         h = C.c_void_p()
         N.check(N.lib().bp_problem_create_posed(self.context(), insts, len(self.instances), C.byref(prm), C.byref(h)))
         self._problem = h

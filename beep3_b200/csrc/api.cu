@@ -78,7 +78,9 @@ int32_t check_params(const char* who, const bp_params* prm) {
   if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
     return fail(BP_ERR_INVALID, std::string(who) + ": unknown precision");
   if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, std::string(who) + ": bad kappa");
-  if (prm->flags & ~BP_FLAG_NEARFIELD_ON_DEMAND) return fail(BP_ERR_INVALID, std::string(who) + ": unknown flags");
+  if (prm->flags & ~(BP_FLAG_NEARFIELD_ON_DEMAND | BP_FLAG_DEVICE_TREE))
+    return fail(BP_ERR_INVALID, std::string(who) + ": unknown flags");
+  if (prm->nbsize <= 0) return fail(BP_ERR_INVALID, std::string(who) + ": nbsize must be positive");
   if (prm->nterms != 9)
     return fail(BP_ERR_UNSUPPORTED, std::string(who) +
                                         ": FMM order must be 9 (the reference's BEM matvec order; the far-field "
@@ -90,9 +92,13 @@ int32_t check_params(const char* who, const bp_params* prm) {
 // point lists): tree, per-patch device arrays, near field, FMM, matvec graph.
 void finish_problem(Ctx* c, Problem& P) {
   auto t0 = std::chrono::steady_clock::now();
-  build_reference_tree(P.h_centroid.data(), P.n, P.params.cube_centre, P.params.cube_edge, P.params.nbsize, P.tree);
-  P.tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   P.d_centroid = upload(c, P.h_centroid);
+  if (P.params.flags & BP_FLAG_DEVICE_TREE)
+    build_device_tree(c, P.d_centroid.as<double>(), P.n, P.params.cube_centre, P.params.cube_edge, P.params.nbsize,
+                      P.tree);
+  else
+    build_reference_tree(P.h_centroid.data(), P.n, P.params.cube_centre, P.params.cube_edge, P.params.nbsize, P.tree);
+  P.tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   P.d_normal = upload(c, P.h_normal);
   P.d_area = upload(c, P.h_area);
   P.d_eps = upload(c, P.h_eps);

@@ -434,6 +434,10 @@ struct StageTimes {
   }
 };
 
+// device_tree.cu: leaf-capped octree of the n centroids (device, xyz
+// interleaved) in the cube (centre, edge); at most `cap` patches per leaf
+void build_device_tree(Ctx* c, const double* d_centroids, int n, const double centre[3], double edge, int cap,
+                       TreeInfo& out);
 // nearfield.cu
 void nf_build_structure(Problem& P);
 void nf_assemble(Problem& P);  // launches the assembly on P.asm_stream

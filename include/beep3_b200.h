@@ -122,7 +122,8 @@ typedef struct {
   double beta0;           /* screening standing in for the Laplace channels (1e-10) */
   double cube_centre[3];  /* bounding cube (BEEP::calculate_bounding_cube) */
   double cube_edge;
-  int32_t nbsize;         /* target mean neighbourhood size of the adaptive tree */
+  int32_t nbsize;         /* target mean neighbourhood size of the adaptive tree; with
+                             BP_FLAG_DEVICE_TREE the most patches a leaf may hold */
   int32_t nterms;         /* FMM order: 9, the reference's matvec order (FMM_BEM_Octree<9,9,67>);
                              other orders return BP_ERR_UNSUPPORTED */
   int32_t precision;      /* enum bp_precision */
@@ -136,7 +137,18 @@ enum bp_flags {
    * (BEM_kernels_instant, src/bem/opencl_bem_kernels.cl:237-352;
    * src/beep/beep.cpp:999-1008); for problems whose coefficients would not
    * fit the HBM budget. */
-  BP_FLAG_NEARFIELD_ON_DEMAND = 1
+  BP_FLAG_NEARFIELD_ON_DEMAND = 1,
+  /* Octree built on the device with a cap of nbsize patches per leaf
+   * instead of the reference's refinement (insertion threshold 4*nbsize,
+   * then splitting the leaves with the largest neighbourhoods until the mean
+   * neighbourhood size is at most nbsize: src/fmm/octree.h:867-986,
+   * :1118-1148).  Patches are sorted by the Morton code of their centroid's
+   * cell at depth 20; a node with more than nbsize patches splits; the
+   * neighbourhood rule (the 26 neighbours of a split node split too, their
+   * children being shadows) and the FMM bookkeeping are the reference's.
+   * Results equal the reference-tree problem's to the FMM's accuracy, not
+   * bitwise: the near/far split of pairs differs. */
+  BP_FLAG_DEVICE_TREE = 2
 };
 
 typedef struct {

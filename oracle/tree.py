@@ -199,3 +199,123 @@ def build(points: np.ndarray, centre, edge: float, nbsize: int) -> dict:
             info[k, 8] = mp[L] if nd.contents else -1
             mp[L] += 1 if nd.contents else 0
     return dict(n_levels=len(levels), info=info, geom=geom, contents=np.array(contents, np.int32))
+
+
+DEPTH = 20  # cell bits per axis (OctreeIndexer's 20 levels for 64-bit keys)
+
+
+def cells(points: np.ndarray, centre, edge: float) -> np.ndarray:
+    """Finest-level cell (x, y, z) of every point: floor((p - (c - e/2)) / e
+    * 2^20), clamped to [0, 2^20)."""
+    lo = np.asarray(centre, float) - float(edge) / 2.0
+    t = np.floor((np.asarray(points, float) - lo) / float(edge) * float(1 << DEPTH))
+    return np.clip(t, 0, (1 << DEPTH) - 1).astype(np.int64)
+
+
+def build_leaf_capped(points: np.ndarray, centre, edge: float, cap: int) -> dict:
+    """The leaf-capped octree of the engine's device-tree mode, restated
+    top-down node by node (the engine sorts Morton codes instead):
+
+      * a node of level L < 20 that is not a shadow splits when it holds
+        more than `cap` points; only non-empty children exist;
+      * level by level, every node split by size makes its existing
+        neighbours (of the 26 same-level cells) split too; the children of a
+        node split only this way are shadow non-leaves (the reference's
+        build_neighbourhoods, octree.h:780-806, :1187-1235);
+      * a node is a leaf unless it is a shadow or split by size;
+      * a node's points are ordered by the Morton code of their cell (x the
+        lowest bit of each triple), ties by index; levels in map order
+        x + y 2^L + z 4^L; FMM slots as in `build`.
+    """
+    pts = np.asarray(points, float)
+    n = len(pts)
+    cell = cells(pts, centre, edge)
+
+    def morton(c):
+        k = 0
+        for b in range(DEPTH):
+            k |= ((int(c[0]) >> b) & 1) << (3 * b) | ((int(c[1]) >> b) & 1) << (3 * b + 1) | \
+                 ((int(c[2]) >> b) & 1) << (3 * b + 2)
+        return k
+
+    codes = [morton(cell[i]) for i in range(n)]
+    ids = sorted(range(n), key=lambda i: (codes[i], i))
+    lo = np.asarray(centre, float) - float(edge) / 2.0
+
+    class N:
+        __slots__ = ("level", "ix", "iy", "iz", "items", "parent", "shadow", "split_size", "split_forced",
+                     "children")
+
+    def node(level, ix, iy, iz, items, parent, shadow):
+        nd = N()
+        nd.level, nd.ix, nd.iy, nd.iz, nd.items, nd.parent, nd.shadow = level, ix, iy, iz, items, parent, shadow
+        nd.split_size = nd.split_forced = False
+        nd.children = [None] * 8
+        return nd
+
+    levels = [{(0, 0, 0): node(0, 0, 0, 0, ids, None, False)}]
+    for L in range(DEPTH + 1):
+        lv = levels[L]
+        for nd in lv.values():
+            nd.split_size = (not nd.shadow) and len(nd.items) > cap and L < DEPTH
+        for nd in lv.values():
+            if not nd.split_size:
+                continue
+            for dz in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dx in (-1, 0, 1):
+                        m = lv.get((nd.ix + dx, nd.iy + dy, nd.iz + dz))
+                        if m is not None and m is not nd and not m.split_size:
+                            m.split_forced = True
+        nxt = {}
+        for nd in lv.values():
+            if not (nd.split_size or nd.split_forced):
+                continue
+            sh = DEPTH - L - 1
+            groups: dict = {}
+            for i in nd.items:
+                o = int((cell[i, 0] >> sh) & 1) + 2 * int((cell[i, 1] >> sh) & 1) + 4 * int((cell[i, 2] >> sh) & 1)
+                groups.setdefault(o, []).append(i)
+            for o, items in groups.items():
+                ch = node(L + 1, 2 * nd.ix + (o & 1), 2 * nd.iy + ((o >> 1) & 1), 2 * nd.iz + (o >> 2), items, nd,
+                          nd.split_forced)
+                nd.children[o] = ch
+                nxt[(ch.ix, ch.iy, ch.iz)] = ch
+        if not nxt:
+            break
+        levels.append(nxt)
+
+    def order(L):
+        E = 1 << L
+        return [levels[L][k] for k in sorted(levels[L], key=lambda c: c[0] + c[1] * E + c[2] * E * E)]
+
+    nodes = [nd for L in range(len(levels)) for nd in order(L)]
+    index = {id(nd): k for k, nd in enumerate(nodes)}
+    info = np.zeros((len(nodes), 18), np.int32)
+    geom = np.zeros((len(nodes), 4))
+    contents = []
+    for k, nd in enumerate(nodes):
+        split = nd.split_size or nd.split_forced
+        leaf = not nd.shadow and not nd.split_size
+        info[k, :4] = (nd.level, nd.ix, nd.iy, nd.iz)
+        info[k, 4] = (1 if split else 0) | (2 if leaf else 0) | (4 if nd.shadow else 0)
+        info[k, 5] = index[id(nd.parent)] if nd.parent is not None else -1
+        info[k, 6] = len(contents)
+        info[k, 7] = len(nd.items)
+        contents += nd.items
+        for c in range(8):
+            info[k, 10 + c] = index[id(nd.children[c])] if nd.children[c] is not None else -1
+        e = float(edge) / float(1 << nd.level)
+        geom[k, :3] = lo + (np.array([nd.ix, nd.iy, nd.iz]) + 0.5) * e
+        geom[k, 3] = e
+    mp = [0] * len(levels)
+    lc = [0] * len(levels)
+    for L in range(len(levels) - 1, -1, -1):
+        for k, nd in enumerate(nodes):
+            if nd.level != L:
+                continue
+            info[k, 9] = -1 if nd.shadow else lc[L]
+            lc[L] += 0 if nd.shadow else 1
+            info[k, 8] = mp[L] if nd.items else -1
+            mp[L] += 1 if nd.items else 0
+    return dict(n_levels=len(levels), info=info, geom=geom, contents=np.array(contents, np.int32))

@@ -85,3 +85,42 @@ def test_tree_ties_on_split_planes(nbsize):
     cols = [0, 1, 2, 3, 5, 6, 7, 8] + list(range(10, 18))
     np.testing.assert_array_equal(t["info"][:, cols], r["info"][:, cols])
     np.testing.assert_array_equal(t["contents"], r["contents"])
+
+
+@pytest.mark.parametrize("k,cap,star", [(4, 16, False), (4, 64, True), (5, 64, True), (3, 1, False)])
+def test_leaf_capped_restatement_invariants(k, cap, star):
+    """The device-tree mode's rule, restated: leaves hold at most `cap`
+    points (or sit at depth 20), every existing neighbour of a node split by
+    size has children, shadows are never leaves, and the leaves partition
+    the points, each inside its leaf's cell."""
+    pts, centre, edge = scenario(k, 100, star)
+    t = OT.build_leaf_capped(pts, centre, edge, cap)
+    info, geom, contents = t["info"], t["geom"], t["contents"]
+    n = len(pts)
+    has_ch, leaf, shadow = (info[:, 4] & 1) > 0, (info[:, 4] & 2) > 0, (info[:, 4] & 4) > 0
+    assert not np.any(leaf & shadow)
+    assert np.all((info[leaf, 7] <= cap) | (info[leaf, 0] == OT.DEPTH) | has_ch[leaf])
+    seen = np.zeros(n, int)
+    for r, g in zip(info[leaf], geom[leaf]):
+        items = contents[r[6]:r[6] + r[7]]
+        seen[items] += 1
+        assert np.all(np.abs(pts[items] - g[:3]) <= g[3] / 2 * (1 + 1e-12))
+    assert np.all(seen == 1)
+    at = {(r[0], r[1], r[2], r[3]): j for j, r in enumerate(info)}
+    for j, r in enumerate(info):
+        split_by_size = has_ch[j] and not leaf[j] and not shadow[j]
+        if not split_by_size:
+            continue
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    m = at.get((r[0], r[1] + dx, r[2] + dy, r[3] + dz))
+                    if m is not None:
+                        assert has_ch[m]
+    # children of a split leaf (a neighbour split) are shadows; of a node
+    # split by size, not
+    for j, r in enumerate(info):
+        for c in r[10:18]:
+            if c >= 0:
+                assert info[c, 5] == j
+                assert shadow[c] == (shadow[j] or leaf[j])
