@@ -80,7 +80,7 @@ class bp_problem_info(C.Structure):
         ("n_patches", C.c_int64), ("n_levels", C.c_int64), ("n_nodes", C.c_int64), ("n_leaves", C.c_int64),
         ("n_nearfield_pairs", C.c_int64), ("n_nearfield_cols", C.c_int64), ("fmm_active", C.c_int64), ("device_bytes", C.c_uint64),
         ("tree_ms", C.c_double), ("assemble_ms", C.c_double), ("gmres_graph", C.c_int64),
-        ("fmm_setup_ms", C.c_double), ("setup_ms", C.c_double),
+        ("fmm_setup_ms", C.c_double), ("setup_ms", C.c_double), ("n_scenarios", C.c_int64),
     ]
 
 
@@ -108,6 +108,7 @@ _SIGS = {
     "bp_mesh_create_from_surface": [_P, _I, _P, _P, _I, _P, _I, _I, _I, _P, _PP, _P],
     "bp_mesh_destroy": [_P],
     "bp_problem_create_posed": [_P, C.POINTER(bp_instance), _I, C.POINTER(bp_params), _PP],
+    "bp_problem_create_batch": [_P, C.POINTER(bp_instance), _I, _P, _I, _P, C.POINTER(bp_params), _PP],
     "bp_problem_destroy": [_P],
     "bp_problem_info_get": [_P, C.POINTER(bp_problem_info)],
     "bp_problem_tree": [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_int64), _P, _P, _P],
@@ -120,6 +121,7 @@ _SIGS = {
     "bp_problem_test_wait_timeout": [_P, _I],
     "bp_solve": [_P, _P, _P, _D, _I, _I, C.POINTER(_I), C.POINTER(_D)],
     "bp_solve_device": [_P, _P, _P, _D, _I, _I, C.POINTER(_I), C.POINTER(_D)],
+    "bp_solve_batch": [_P, _P, _P, _D, _I, _I, _P, _P],
     "bp_rhs": [_P, _P, _I, _D, _P],
     "bp_rhs_posed": [_P, _P, _P, _D, _P],
     "bp_rhs_noalloc": [_I, _P, _P, _I, _P, _I, _D, _P, _P],

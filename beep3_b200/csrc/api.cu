@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <future>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -88,16 +89,93 @@ int32_t check_params(const char* who, const bp_params* prm) {
   return BP_OK;
 }
 
+// One tree of the scenarios' trees: level by level, scenario after
+// scenario, node links and contents renumbered (scenario s's patch i is the
+// problem's patch first[s] + i).  Neighbours never cross scenarios, so the
+// near field and the FMM's interaction lists stay inside each scenario; the
+// per-level operators are shared because every scenario's cube has the same
+// edge.
+void merge_forest(const std::vector<TreeInfo>& F, const std::vector<int>& first, TreeInfo& out) {
+  const int S = (int)F.size();
+  out = TreeInfo();
+  for (const TreeInfo& t : F) out.n_levels = std::max(out.n_levels, t.n_levels);
+  std::vector<std::vector<int>> remap(S);
+  for (int s = 0; s < S; ++s) remap[s].assign(F[s].nodes.size(), -1);
+  out.level_start.assign(out.n_levels + 1, 0);
+  for (int l = 0; l < out.n_levels; ++l) {
+    out.level_start[l] = (int)out.nodes.size();
+    for (int s = 0; s < S; ++s) {
+      if (l >= F[s].n_levels) continue;
+      for (int j = F[s].level_start[l]; j < F[s].level_start[l + 1]; ++j) {
+        remap[s][j] = (int)out.nodes.size();
+        out.nodes.push_back(F[s].nodes[j]);
+      }
+    }
+  }
+  out.level_start[out.n_levels] = (int)out.nodes.size();
+  out.n_mp_per_level.assign(out.n_levels, 0);
+  out.n_lc_per_level.assign(out.n_levels, 0);
+  for (int s = 0; s < S; ++s) {
+    const TreeInfo& t = F[s];
+    for (size_t j = 0; j < t.nodes.size(); ++j) {
+      TreeNode& nd = out.nodes[remap[s][j]];
+      auto re = [&](int32_t k) { return k < 0 ? -1 : remap[s][k]; };
+      nd.parent = re(nd.parent);
+      for (int c = 0; c < 8; ++c) nd.children[c] = re(nd.children[c]);
+      for (int nb = 0; nb < 27; ++nb) nd.neighbours[nb] = re(nd.neighbours[nb]);
+    }
+  }
+  // contents, node by node in the merged order; FMM slots per merged level
+  for (int l = out.n_levels - 1; l >= 0; --l)
+    for (int j = out.level_start[l]; j < out.level_start[l + 1]; ++j) {
+      TreeNode& nd = out.nodes[j];
+      nd.lc_idx = (nd.flags & TREE_SHADOW) ? -1 : out.n_lc_per_level[l]++;
+      nd.mp_idx = nd.content_count > 0 ? out.n_mp_per_level[l]++ : -1;
+    }
+  std::vector<int> owner(out.nodes.size(), 0);
+  for (int s = 0; s < S; ++s)
+    for (int k : remap[s]) owner[k] = s;
+  for (size_t j = 0; j < out.nodes.size(); ++j) {
+    TreeNode& nd = out.nodes[j];
+    const int s = owner[j];
+    const int64_t src = nd.content_start;
+    nd.content_start = (int64_t)out.contents.size();
+    for (int32_t q = 0; q < nd.content_count; ++q) out.contents.push_back(first[s] + F[s].contents[src + q]);
+  }
+}
+
 // The steps after the patch geometry is in place (host arrays and device
 // point lists): tree, per-patch device arrays, near field, FMM, matvec graph.
 void finish_problem(Ctx* c, Problem& P) {
   auto t0 = std::chrono::steady_clock::now();
   P.d_centroid = upload(c, P.h_centroid);
-  if (P.params.flags & BP_FLAG_DEVICE_TREE)
-    build_device_tree(c, P.d_centroid.as<double>(), P.n, P.params.cube_centre, P.params.cube_edge, P.params.nbsize,
-                      P.tree);
-  else
-    build_reference_tree(P.h_centroid.data(), P.n, P.params.cube_centre, P.params.cube_edge, P.params.nbsize, P.tree);
+  if (P.scen_first.empty()) {
+    P.scen_first = {0, P.n};
+    P.scen_centre.assign(P.params.cube_centre, P.params.cube_centre + 3);
+  }
+  const int S = P.n_scen();
+  std::vector<TreeInfo> forest(S);
+  auto one_tree = [&](int s) {
+    const int a = P.scen_first[s], n = P.scen_first[s + 1] - a;
+    if (P.params.flags & BP_FLAG_DEVICE_TREE)
+      build_device_tree(c, P.d_centroid.as<double>() + 3 * (size_t)a, n, &P.scen_centre[3 * s], P.params.cube_edge,
+                        P.params.nbsize, S == 1 ? P.tree : forest[s]);
+    else
+      build_reference_tree(P.h_centroid.data() + 3 * (size_t)a, n, &P.scen_centre[3 * s], P.params.cube_edge,
+                           P.params.nbsize, S == 1 ? P.tree : forest[s]);
+  };
+  if (S == 1) {
+    one_tree(0);
+  } else {
+    if (P.params.flags & BP_FLAG_DEVICE_TREE) {
+      for (int s = 0; s < S; ++s) one_tree(s);
+    } else {  // host trees of the scenarios side by side
+      std::vector<std::future<void>> jobs;
+      for (int s = 0; s < S; ++s) jobs.push_back(std::async(std::launch::async, one_tree, s));
+      for (auto& j : jobs) j.get();
+    }
+    merge_forest(forest, P.scen_first, P.tree);
+  }
   P.tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   P.d_normal = upload(c, P.h_normal);
   P.d_area = upload(c, P.h_area);
@@ -336,10 +414,12 @@ BP_API int32_t bp_mesh_destroy(bp_mesh mesh) {
   });
 }
 
-BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int32_t n_inst, const bp_params* prm,
-                                       bp_problem* out) {
-  return guarded_engine([&]() -> int32_t {
-    Ctx* c = as_ctx(ctx);
+// A problem from placed mesh instances; scen_inst (n_scen + 1 instance
+// offsets, null for one scenario) and centres (3 n_scen) split it into
+// independent scenarios.
+static int32_t create_posed(Ctx* c, const bp_instance* inst, int32_t n_inst, const bp_params* prm,
+                            const int32_t* scen_inst, int32_t n_scen, const double* centres, bp_problem* out) {
+  {
     if (!c || !inst || !prm || !out || n_inst <= 0) return fail(BP_ERR_INVALID, "bp_problem_create_posed: bad argument");
     if (const int32_t e = check_params("bp_problem_create_posed", prm)) return e;
     long long n_total = 0, nq = 0, nd = 0, ng = 0;
@@ -431,9 +511,44 @@ BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int3
       bd += m.n_quad_pts;
       bg += m.n_gal_pts;
     }
+    if (scen_inst) {
+      P->scen_first.assign(1, 0);
+      int q = 0;
+      for (int s = 0; s < n_scen; ++s) {
+        int n_s = 0;
+        for (; q < scen_inst[s + 1]; ++q) {
+          P->placements[q].scenario = s;
+          n_s += reinterpret_cast<const DevMesh*>(inst[q].mesh)->n;
+        }
+        P->scen_first.push_back(P->scen_first.back() + n_s);
+      }
+      P->scen_centre.assign(centres, centres + 3 * (size_t)n_scen);
+    }
     finish_problem(c, *P);
     *out = reinterpret_cast<bp_problem>(P.release());
     return BP_OK;
+  }
+}
+
+BP_API int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* inst, int32_t n_inst, const bp_params* prm,
+                                       bp_problem* out) {
+  return guarded_engine([&]() -> int32_t { return create_posed(as_ctx(ctx), inst, n_inst, prm, nullptr, 1, nullptr, out); });
+}
+
+BP_API int32_t bp_problem_create_batch(bp_ctx ctx, const bp_instance* inst, int32_t n_inst,
+                                       const int32_t* scenario_first, int32_t n_scenarios, const double* cube_centres,
+                                       const bp_params* prm, bp_problem* out) {
+  return guarded_engine([&]() -> int32_t {
+    if (!scenario_first || !cube_centres || n_scenarios <= 0 || !prm)
+      return fail(BP_ERR_INVALID, "bp_problem_create_batch: bad argument");
+    if (scenario_first[0] != 0 || scenario_first[n_scenarios] != n_inst)
+      return fail(BP_ERR_INVALID, "bp_problem_create_batch: scenario_first must run from 0 to n_inst");
+    for (int s = 0; s < n_scenarios; ++s)
+      if (scenario_first[s + 1] <= scenario_first[s])
+        return fail(BP_ERR_INVALID, "bp_problem_create_batch: every scenario needs an instance");
+    for (int k = 0; k < 3 * n_scenarios; ++k)
+      if (!std::isfinite(cube_centres[k])) return fail(BP_ERR_INVALID, "bp_problem_create_batch: non-finite centre");
+    return create_posed(as_ctx(ctx), inst, n_inst, prm, scenario_first, n_scenarios, cube_centres, out);
   });
 }
 
@@ -464,6 +579,7 @@ BP_API int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info) {
   info->fmm_setup_ms = P->fmm_setup_ms;
   info->setup_ms = P->setup_ms;
   info->gmres_graph = P->gmres_graph ? 1 : 0;
+  info->n_scenarios = P->n_scen();
   return BP_OK;
 }
 
@@ -578,17 +694,20 @@ BP_API int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_de
     if (!P || !rhs_dev || !x_dev) return fail(BP_ERR_INVALID, "bp_solve_device: null argument");
     if (!(tol > 0)) return fail(BP_ERR_INVALID, "bp_solve_device: tol must be positive");
     DeviceGuard g(P->ctx->device);
-    double rr = 0;
-    int its = gmres_device(*P, rhs_dev, x_dev, tol, max_iters, restart, &rr);
+    std::vector<double> rr(P->n_scen(), 0.0);
+    int its = gmres_device(*P, rhs_dev, x_dev, tol, max_iters, restart, rr.data());
+    const double worst = *std::max_element(rr.begin(), rr.end());
     if (iterations) *iterations = its;
-    if (rel_residual) *rel_residual = rr;
-    if (rr > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");
+    if (rel_residual) *rel_residual = worst;
+    if (worst > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");
     return BP_OK;
   });
 }
 
-BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
-                        int32_t* iterations, double* rel_residual) {
+// bp_solve (worst scenario's iterations and residual) and bp_solve_batch
+// (one entry per scenario in iterations and rel_residual)
+static int32_t solve_host(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
+                          int32_t* iterations, double* rel_residual, bool scenario_out) {
   return guarded_engine([&]() -> int32_t {
     Problem* P = as_problem(p);
     if (!P || !rhs || !x) return fail(BP_ERR_INVALID, "bp_solve: null argument");
@@ -600,16 +719,34 @@ BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, 
     if (b.bytes() < bytes) b.alloc(P->ctx, bytes);
     BP_CUDA(cudaMemcpyAsync(b.get(), rhs, bytes, cudaMemcpyHostToDevice, st));
     BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
-    double rr = 0;
-    int its = gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, &rr);
+    std::vector<double> rr(P->n_scen(), 0.0);
+    std::vector<int> its(P->n_scen(), 0);
+    gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, rr.data(), its.data());
     BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
     fmm_check_waits(*P);
-    if (iterations) *iterations = its;
-    if (rel_residual) *rel_residual = rr;
-    if (rr > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");
+    const double worst = *std::max_element(rr.begin(), rr.end());
+    if (scenario_out) {  // bp_solve_batch: per scenario
+      std::copy(its.begin(), its.end(), iterations);
+      std::copy(rr.begin(), rr.end(), rel_residual);
+    } else {
+      if (iterations) *iterations = *std::max_element(its.begin(), its.end());
+      if (rel_residual) *rel_residual = worst;
+    }
+    if (worst > tol) return fail(BP_ERR_NOT_CONVERGED, "GMRES reached its iteration limit");
     return BP_OK;
   });
+}
+
+BP_API int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
+                        int32_t* iterations, double* rel_residual) {
+  return solve_host(p, rhs, x, tol, max_iters, restart, iterations, rel_residual, false);
+}
+
+BP_API int32_t bp_solve_batch(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters,
+                              int32_t restart, int32_t* iterations, double* rel_residual) {
+  if (!iterations || !rel_residual) return fail(BP_ERR_INVALID, "bp_solve_batch: null output array");
+  return solve_host(p, rhs, x, tol, max_iters, restart, iterations, rel_residual, true);
 }
 
 BP_API int32_t bp_problem_test_wait_timeout(bp_problem p, int32_t enable) {
@@ -629,6 +766,8 @@ BP_API int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charge
     if (!P || !rhs || (n_charges > 0 && !charges_xyzq) || n_charges < 0)
       return fail(BP_ERR_INVALID, "bp_rhs: bad argument");
     if (!(eps_solvent > 0)) return fail(BP_ERR_INVALID, "bp_rhs: eps_solvent must be positive");
+    if (P->n_scen() > 1)
+      return fail(BP_ERR_INVALID, "bp_rhs: a batch problem takes its charges per instance (bp_rhs_posed)");
     DeviceGuard g(P->ctx->device);
     Ctx* c = P->ctx;
     DevBuf& dch = P->scratch_charges;

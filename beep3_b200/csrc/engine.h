@@ -316,6 +316,7 @@ struct Placement {
   DevMesh* mesh = nullptr;
   double R[9], c[3], o[3];
   int q_begin = 0, q_count = 0;
+  int scenario = 0;  // the independent scenario of a batch the instance belongs to
 };
 
 struct Problem;
@@ -329,7 +330,14 @@ struct Problem {
   bp_params params{};
   bool fp64 = true;
   TreeInfo tree;
-  std::vector<Placement> placements;  // set by bp_problem_create_posed
+  std::vector<Placement> placements;  // set by bp_problem_create_posed / _batch
+  // Independent scenarios (bp_problem_create_batch): scenario s owns patches
+  // [scen_first[s], scen_first[s+1]), has its own tree in the cube of centre
+  // scen_centre[3s..3s+2] (all of edge params.cube_edge) and its own GMRES;
+  // no interaction crosses scenarios.  An ordinary problem is one scenario.
+  std::vector<int> scen_first;
+  std::vector<double> scen_centre;
+  int n_scen() const { return (int)scen_first.size() - 1; }
   // patches (original order)
   std::vector<double> h_centroid, h_normal, h_area, h_eps, h_gc;
   std::vector<int32_t> h_qual_off, h_quad_off, h_gal_off;
@@ -353,7 +361,7 @@ struct Problem {
   cudaGraphExec_t graph = nullptr;
   bool graph_failed = false;
   // Krylov workspace
-  DevBuf d_V, d_w, d_scal;
+  DevBuf d_V, d_w, d_scal, d_seg;
   // one GMRES cycle's Arnoldi loop as a graph with a device-side WHILE node
   // (built for basis size gmres_graph_m on the V / scalar blocks it was
   // captured with)
@@ -460,8 +468,11 @@ void fmm_apply(Problem& P, const double* x_dev, double* y_dev, StageTimes* st, c
 void matvec_setup(Problem& P);
 // krylov.cu
 void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st = nullptr);
+// GMRES of every scenario of P (one for an ordinary problem): rel_resid and
+// iters (may be null) receive one entry per scenario; returns the most
+// iterations any scenario took
 int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,
-                 double* rel_resid);
+                 double* rel_resid, int* iters = nullptr);
 // sources.cu
 void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev);
 // right-hand side of a posed problem from each instance's charges in its

@@ -20,6 +20,7 @@
 // same kernels step by step and reads the stop flag after each.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -38,176 +39,237 @@ constexpr int kDotBlocks = 296;  // 2 per SM on a 148-SM part
 // DBL_MIN guard used by the reference to avoid 0/0 (src/beep/beep.cpp:1360)
 __device__ __forceinline__ double near0(double v) { return v == 0.0 ? 2.2250738585072014e-308 : v; }
 
-// partial[k * gridDim.x + b] = sum over block b's slice of V[:,k] . w
-__global__ void dot_partials(const double* __restrict__ V, int64_t ld, const double* __restrict__ w, int64_t len,
-                             double* __restrict__ partial) {
-  const int k = blockIdx.y;
-  const double* v = V + ld * k;
-  double s = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
-    s += v[i] * w[i];
-  __shared__ double red[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) partial[(int64_t)k * gridDim.x + blockIdx.x] = s;
-  }
-}
-
-// out[k] = sum_b partial[k * nb + b] (fixed order), optionally sqrt
-__global__ void reduce_partials(const double* __restrict__ partial, int nb, double* __restrict__ out, int take_sqrt) {
-  const int k = blockIdx.x;
-  double s = 0.0;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(int64_t)k * nb + b];
-  __shared__ double red[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) out[k] = take_sqrt ? sqrt(s) : s;
-  }
-}
-
-// r = r - b ; then v0 = r / near0(||r||) is done by scale_by_norm
+// r = r - b ; then v0 = r / near0(||r||) is done by seg_scale_by_norm
 __global__ void sub_inplace(double* __restrict__ r, const double* __restrict__ b, int64_t len) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
     r[i] -= b[i];
 }
 
-__global__ void scale_by_norm(double* __restrict__ v, const double* __restrict__ norm, int64_t len) {
-  const double inv = 1.0 / near0(*norm);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
-    v[i] *= inv;
+// Scenarios of a batch problem each run their own GMRES on their part of
+// the vector: scenario s owns entries [a, a+n) (the f half) and
+// [N+a, N+a+n) (the h half); its local index i in [0, 2n) maps to a + i or
+// N + a + i - n.  An ordinary problem is one scenario (a = 0, n = N).
+struct Seg {
+  int a, n;
+};
+__device__ __forceinline__ int64_t seg_at(Seg sg, int64_t N, int64_t i) {
+  return i < sg.n ? sg.a + i : N + sg.a + (i - sg.n);
 }
 
-// Control block of the device-resident solver (after the scalars in d_scal).
+// fixed-order block sum; the total is valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;
+}
+
+// Control block of one scenario's solver (after the scalars in d_scal).
 struct KrylovCtl {
   double nrm_b;  // ||b||
   double h;      // norm of the newest Arnoldi vector before it is normalised
   double stop;   // tol * ||b||
   double last;   // |y_j| after the newest step
   int j;         // Arnoldi steps done in this cycle
-  int cycle;     // step limit of this cycle
+  int cycle;     // step limit of this cycle (0: the scenario sits it out)
   int cont;      // 1 while the cycle goes on
+  int done;      // converged in an earlier step
+  int iters;     // Arnoldi steps over all cycles
+  int pad;
+};
+struct KrylovAll {
+  int any;  // some scenario goes on
   int pad;
 };
 
-__global__ void set_stop(KrylovCtl* ctl, double tol) { ctl->stop = tol * ctl->nrm_b; }
-
-// y[0] = beta = ||r||; a new cycle starts at step 0
-__global__ void cycle_start(KrylovCtl* ctl, double* y, int cycle) {
-  y[0] = ctl->h;
-  ctl->j = 0;
-  ctl->cycle = cycle;
-  ctl->cont = 1;
+// partial[s * nbs + b] = block b's share of |v|^2 over scenario s
+__global__ void seg_sq_partials(const double* __restrict__ v, const Seg* __restrict__ seg, int64_t N,
+                                double* __restrict__ partial) {
+  const int sc = blockIdx.y;
+  const Seg sg = seg[sc];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 2 * (int64_t)sg.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double t = v[seg_at(sg, N, i)];
+    s += t * t;
+  }
+  __shared__ double red[kThreads / 32];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) partial[(int64_t)sc * gridDim.x + blockIdx.x] = s;
 }
 
-// gx = v_j; for j > 0 the newest column is normalised here first (by 1/h)
-__global__ void arnoldi_load(double* __restrict__ V, int64_t len, const KrylovCtl* __restrict__ ctl,
-                             double* __restrict__ gx) {
-  const int j = ctl->j;
-  double* vj = V + len * j;
-  const double inv = j > 0 ? 1.0 / near0(ctl->h) : 1.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
-    double v = vj[i];
-    if (j > 0) {
-      v *= inv;
-      vj[i] = v;
-    }
-    gx[i] = v;
+// ctl[s].nrm_b = sqrt(sum of the partials); the stop level; a fresh solve
+__global__ void norm_b_finish(const double* __restrict__ partial, int nbs, KrylovCtl* __restrict__ ctl, double tol) {
+  const int sc = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nbs; b += blockDim.x) s += partial[(int64_t)sc * nbs + b];
+  __shared__ double red[kThreads / 32];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) {
+    KrylovCtl& c = ctl[sc];
+    c.nrm_b = sqrt(s);
+    c.stop = tol * c.nrm_b;
+    c.done = 0;
+    c.iters = 0;
+    c.last = 0.0;
   }
 }
 
-// partial[k * gridDim.x + b] = block b's share of V[:, k] . w for k <= j
+// ctl[s].h = ||r|| of the scenario
+__global__ void norm_r_finish(const double* __restrict__ partial, int nbs, KrylovCtl* __restrict__ ctl) {
+  const int sc = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nbs; b += blockDim.x) s += partial[(int64_t)sc * nbs + b];
+  __shared__ double red[kThreads / 32];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) ctl[sc].h = sqrt(s);
+}
+
+// v0 = r / near0(||r||) for the scenarios still solving
+__global__ void seg_scale_by_norm(double* __restrict__ v, const Seg* __restrict__ seg, int64_t N,
+                                  const KrylovCtl* __restrict__ ctl) {
+  const int sc = blockIdx.y;
+  if (ctl[sc].done) return;
+  const Seg sg = seg[sc];
+  const double inv = 1.0 / near0(ctl[sc].h);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 2 * (int64_t)sg.n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[seg_at(sg, N, i)] *= inv;
+}
+
+// y[0] = beta = ||r||; a new cycle starts at step 0 for every scenario not
+// yet converged
+__global__ void cycle_start(KrylovCtl* __restrict__ ctl, int n_scen, double* __restrict__ y0, int64_t ks,
+                            int64_t y_off, int cycle, KrylovAll* __restrict__ all) {
+  const int sc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sc == 0) all->any = 1;
+  if (sc >= n_scen) return;
+  KrylovCtl& c = ctl[sc];
+  y0[sc * ks + y_off] = c.h;
+  c.j = 0;
+  c.cycle = c.done ? 0 : cycle;
+  c.cont = c.done ? 0 : 1;
+}
+
+// gx = v_j; for j > 0 the newest column is normalised here first (by 1/h)
+__global__ void arnoldi_load(double* __restrict__ V, int64_t len, const Seg* __restrict__ seg,
+                             const KrylovCtl* __restrict__ ctl, double* __restrict__ gx) {
+  const int sc = blockIdx.y;
+  if (!ctl[sc].cont) return;
+  const Seg sg = seg[sc];
+  const int64_t N = len / 2;
+  const int j = ctl[sc].j;
+  double* vj = V + len * j;
+  const double inv = j > 0 ? 1.0 / near0(ctl[sc].h) : 1.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 2 * (int64_t)sg.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = seg_at(sg, N, i);
+    double v = vj[g];
+    if (j > 0) {
+      v *= inv;
+      vj[g] = v;
+    }
+    gx[g] = v;
+  }
+}
+
+// partial_s[k * nbs + b] = block b's share of V[:, k] . w over scenario s,
+// k <= j (partial_s = partial + s * (m+1) * nbs)
 __global__ void arnoldi_dots(const double* __restrict__ V, int64_t len, const double* __restrict__ w,
-                             const KrylovCtl* __restrict__ ctl, double* __restrict__ partial) {
-  const int j = ctl->j;
+                             const Seg* __restrict__ seg, const KrylovCtl* __restrict__ ctl, int m,
+                             double* __restrict__ partial) {
+  const int sc = blockIdx.y;
+  if (!ctl[sc].cont) return;
+  const Seg sg = seg[sc];
+  const int64_t N = len / 2;
+  const int j = ctl[sc].j, nbs = gridDim.x;
+  double* part = partial + (int64_t)sc * (m + 1) * nbs;
   __shared__ double red[kThreads / 32];
   for (int k = 0; k <= j; ++k) {
     const double* v = V + len * k;
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
-      s += v[i] * w[i];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (threadIdx.x == 0) partial[(int64_t)k * gridDim.x + blockIdx.x] = s;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 2 * (int64_t)sg.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t g = seg_at(sg, N, i);
+      s += v[g] * w[g];
     }
-    __syncthreads();
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) part[(int64_t)k * nbs + blockIdx.x] = s;
   }
 }
 
-// U[j(j+1)/2 + k] = sum_b partial[k * nb + b] (fixed order), block k <= j
-__global__ void arnoldi_reduce(const double* __restrict__ partial, int nb, const KrylovCtl* __restrict__ ctl,
-                               double* __restrict__ U) {
-  const int k = blockIdx.x, j = ctl->j;
+// U_s[j(j+1)/2 + k] = sum_b partial_s[k * nbs + b] (fixed order), block k <= j
+__global__ void arnoldi_reduce(const double* __restrict__ partial, int nbs, const KrylovCtl* __restrict__ ctl, int m,
+                               double* __restrict__ U0, int64_t ks) {
+  const int k = blockIdx.x, sc = blockIdx.y;
+  if (!ctl[sc].cont) return;
+  const int j = ctl[sc].j;
   if (k > j) return;
+  const double* part = partial + (int64_t)sc * (m + 1) * nbs;
   double s = 0.0;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(int64_t)k * nb + b];
+  for (int b = threadIdx.x; b < nbs; b += blockDim.x) s += part[(int64_t)k * nbs + b];
   __shared__ double red[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) U[j * (j + 1) / 2 + k] = s;
-  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) U0[sc * ks + j * (j + 1) / 2 + k] = s;
 }
 
-// V[:, j+1] = w - V[:, 0..j] u (u = U's column j), and block b's share of
-// |V[:, j+1]|^2 into partial[b] (the same slices as arnoldi_dots)
+// V[:, j+1] = w - V[:, 0..j] u (u = U_s's column j) over scenario s, and
+// block b's share of |V[:, j+1]|^2 into partial_s[b] (the slices of
+// arnoldi_dots)
 __global__ void arnoldi_orth(double* __restrict__ V, int64_t len, const double* __restrict__ w,
-                             const double* __restrict__ U, const KrylovCtl* __restrict__ ctl,
-                             double* __restrict__ partial) {
-  const int j = ctl->j;
-  const double* u = U + j * (j + 1) / 2;
+                             const double* __restrict__ U0, int64_t ks, const Seg* __restrict__ seg,
+                             const KrylovCtl* __restrict__ ctl, int m, double* __restrict__ partial) {
+  const int sc = blockIdx.y;
+  if (!ctl[sc].cont) return;
+  const Seg sg = seg[sc];
+  const int64_t N = len / 2;
+  const int j = ctl[sc].j;
+  const double* u = U0 + sc * ks + j * (j + 1) / 2;
   double* out = V + len * (j + 1);
   double s2 = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 2 * (int64_t)sg.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = seg_at(sg, N, i);
     double s = 0.0;
-    for (int k = 0; k <= j; ++k) s += V[len * k + i] * u[k];
-    const double v = w[i] - s;
-    out[i] = v;
+    for (int k = 0; k <= j; ++k) s += V[len * k + g] * u[k];
+    const double v = w[g] - s;
+    out[g] = v;
     s2 += v * v;
   }
   __shared__ double red[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s2 = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    if (threadIdx.x == 0) partial[blockIdx.x] = s2;
-  }
+  s2 = block_sum(s2, red);
+  if (threadIdx.x == 0) partial[(int64_t)sc * (m + 1) * gridDim.x + blockIdx.x] = s2;
 }
 
-// h = ||V[:, j+1]|| from the partials (fixed order); the Givens step of
-// column j (src/beep/beep.cpp:1399-1416); j += 1; the stop test
-// (src/beep/beep.cpp:1421).  With a conditional handle the decision drives
-// the graph's WHILE node.
-__global__ void arnoldi_finish(const double* __restrict__ partial, int nb, double* __restrict__ U,
-                               double* __restrict__ c, double* __restrict__ s, double* __restrict__ y,
-                               KrylovCtl* __restrict__ ctl, cudaGraphConditionalHandle handle, int use_handle) {
+// One block per scenario: h = ||V[:, j+1]|| from the partials (fixed order);
+// the Givens step of column j (src/beep/beep.cpp:1399-1416); j += 1; the
+// stop test (src/beep/beep.cpp:1421).  With a conditional handle and one
+// scenario the decision drives the graph's WHILE node (with several,
+// any_continue does).
+__global__ void arnoldi_finish(const double* __restrict__ partial, int nbs, int m, double* __restrict__ U0,
+                               int64_t ks, KrylovCtl* __restrict__ ctl, cudaGraphConditionalHandle handle,
+                               int use_handle) {
+  const int sc = blockIdx.x;
+  if (!ctl[sc].cont) return;
+  const double* part = partial + (int64_t)sc * (m + 1) * nbs;
   double acc = 0.0;
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += partial[b];
+  for (int b = threadIdx.x; b < nbs; b += blockDim.x) acc += part[b];
   __shared__ double red[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-  __syncthreads();
+  acc = block_sum(acc, red);
   if (threadIdx.x != 0) return;
-  acc = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += red[w];
+  double* U = U0 + sc * ks;
+  double* c = U + m * (m + 1) / 2;
+  double* s = c + m;
+  double* y = s + m;
+  KrylovCtl& C = ctl[sc];
   const double h = sqrt(acc);
-  const int j = ctl->j;
+  const int j = C.j;
   int uij = j * (j + 1) / 2;
   for (int i = 0; i < j; ++i) {
     const double tmp = c[i] * U[uij] - s[i] * U[uij + 1];
@@ -223,19 +285,38 @@ __global__ void arnoldi_finish(const double* __restrict__ partial, int nb, doubl
   y[j + 1] = s[j] * y[j];
   y[j] = c[j] * y[j];
   const double last = fabs(y[j + 1]);
-  const int cont = (j + 1 < ctl->cycle && last > ctl->stop) ? 1 : 0;
-  ctl->h = h;
-  ctl->j = j + 1;
-  ctl->last = last;
-  ctl->cont = cont;
-  if (use_handle) cudaGraphSetConditional(handle, cont);
+  const int cont = (j + 1 < C.cycle && last > C.stop) ? 1 : 0;
+  C.h = h;
+  C.j = j + 1;
+  C.last = last;
+  C.cont = cont;
+  if (last <= C.stop) C.done = 1;
+  if (use_handle && gridDim.x == 1) cudaGraphSetConditional(handle, cont);
 }
 
-// Solve the packed upper-triangular U y = y (column-major, first j columns)
-// unless U and y are both zero (src/beep/beep.cpp:1422-1426).
-__global__ void packed_back_substitution(const double* __restrict__ U, const KrylovCtl* __restrict__ ctl,
-                                         double* __restrict__ y) {
-  const int j = ctl->j;
+// all->any = some scenario goes on; drives the WHILE node of a batch
+__global__ void any_continue(const KrylovCtl* __restrict__ ctl, int n_scen, KrylovAll* __restrict__ all,
+                             cudaGraphConditionalHandle handle, int use_handle) {
+  int any = 0;
+  for (int sc = threadIdx.x; sc < n_scen; sc += blockDim.x) any |= ctl[sc].cont;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    all->any = any;
+    if (use_handle) cudaGraphSetConditional(handle, any);
+  }
+}
+
+// Per scenario: solve the packed upper-triangular U y = y (column-major,
+// first j columns) unless U and y are both zero (src/beep/beep.cpp:1422-1426);
+// count the cycle's steps.
+__global__ void packed_back_substitution(double* __restrict__ U0, int64_t ks, int m, KrylovCtl* __restrict__ ctl,
+                                         int n_scen) {
+  const int sc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sc >= n_scen) return;
+  const double* U = U0 + sc * ks;
+  double* y = U0 + sc * ks + m * (m + 1) / 2 + 2 * m;
+  const int j = ctl[sc].j;
+  ctl[sc].iters += j;
   double su = 0.0, sy = 0.0;
   const int uij = j * (j + 1) / 2;
   for (int k = 0; k < uij; ++k) su += fabs(U[k]);
@@ -248,14 +329,22 @@ __global__ void packed_back_substitution(const double* __restrict__ U, const Kry
   }
 }
 
-// x -= V[:, 0..j) y
-__global__ void update_x(const double* __restrict__ V, int64_t ld, const KrylovCtl* __restrict__ ctl,
-                         const double* __restrict__ y, double* __restrict__ x, int64_t len) {
-  const int j = ctl->j;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+// x -= V[:, 0..j) y over each scenario
+__global__ void update_x(const double* __restrict__ V, int64_t len, const Seg* __restrict__ seg,
+                         const KrylovCtl* __restrict__ ctl, const double* __restrict__ U0, int64_t ks, int m,
+                         double* __restrict__ x) {
+  const int sc = blockIdx.y;
+  const int j = ctl[sc].j;
+  if (j == 0) return;
+  const Seg sg = seg[sc];
+  const int64_t N = len / 2;
+  const double* y = U0 + sc * ks + m * (m + 1) / 2 + 2 * m;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 2 * (int64_t)sg.n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = seg_at(sg, N, i);
     double s = 0.0;
-    for (int k = 0; k < j; ++k) s += V[ld * k + i] * y[k];
-    x[i] -= s;
+    for (int k = 0; k < j; ++k) s += V[len * k + g] * y[k];
+    x[g] -= s;
   }
 }
 
@@ -391,44 +480,59 @@ void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* s
 
 namespace {
 
-// Scalar block of the solver: U (m(m+1)/2), c (m), s (m), y (m+1), partial
-// sums (kDotBlocks * (m+1)), then the control block.
+// Scalar block of the solver, per scenario s: U (m(m+1)/2), c (m), s (m),
+// y (m+1) at s * ks; then the dot partials ((m+1) * nbs per scenario), the
+// control blocks and the batch flag.
 struct KrylovView {
-  double *U, *c, *s, *y, *partial;
+  double* U0;  // scenario s's U at U0 + s * ks, then its c, s, y
+  int64_t ks;
+  double* partial;
   KrylovCtl* ctl;
+  KrylovAll* all;
+  int nbs;  // dot-product blocks per scenario
+  int gx;   // elementwise blocks per scenario
 };
-size_t krylov_scalar_bytes(int m) {
-  const size_t nd = (size_t)m * (m + 1) / 2 + 2 * (size_t)m + (m + 1) + (size_t)kDotBlocks * (m + 1);
-  return sizeof(double) * nd + sizeof(KrylovCtl);
+int dot_blocks(int n_scen) { return n_scen == 1 ? kDotBlocks : std::max(16, kDotBlocks / n_scen); }
+int64_t scal_stride(int m) { return (int64_t)m * (m + 1) / 2 + 2 * (int64_t)m + (m + 1); }
+size_t krylov_scalar_bytes(int m, int n_scen) {
+  const size_t nd = (size_t)n_scen * (scal_stride(m) + (size_t)(m + 1) * dot_blocks(n_scen));
+  return sizeof(double) * nd + sizeof(KrylovCtl) * n_scen + sizeof(KrylovAll);
 }
 KrylovView krylov_view(Problem& P, int m) {
+  const int S = P.n_scen();
   KrylovView v;
-  v.U = P.d_scal.as<double>();
-  v.c = v.U + (size_t)m * (m + 1) / 2;
-  v.s = v.c + m;
-  v.y = v.s + m;
-  v.partial = v.y + (m + 1);
-  v.ctl = reinterpret_cast<KrylovCtl*>(v.partial + (size_t)kDotBlocks * (m + 1));
+  v.ks = scal_stride(m);
+  v.nbs = dot_blocks(S);
+  v.U0 = P.d_scal.as<double>();
+  v.partial = v.U0 + S * v.ks;
+  v.ctl = reinterpret_cast<KrylovCtl*>(v.partial + (size_t)S * (m + 1) * v.nbs);
+  v.all = reinterpret_cast<KrylovAll*>(v.ctl + S);
+  int nmax = 1;
+  for (int s = 0; s < S; ++s) nmax = std::max(nmax, P.scen_first[s + 1] - P.scen_first[s]);
+  v.gx = std::max(1, std::min(grid_for(2 * (int64_t)nmax), S == 1 ? 4 * 148 : std::max(4, 4 * 148 / S)));
   return v;
 }
 
-// One Arnoldi step on stream st: v_j -> gx, the matvec into gy, the CGS
-// orthogonalisation of gy into V[:, j+1] and the Givens step.  With a handle
-// the last kernel sets the enclosing WHILE node's condition.
+// One Arnoldi step of every scenario still solving, on stream st: v_j -> gx,
+// the matvec into gy, the CGS orthogonalisation of gy into V[:, j+1] and the
+// Givens step.  With a handle the last kernel sets the enclosing WHILE
+// node's condition.
 void arnoldi_step_launches(Problem& P, int m, cudaStream_t st, cudaGraphConditionalHandle handle, int use_handle) {
   const int64_t len = 2 * (int64_t)P.n;
+  const int S = P.n_scen();
   const KrylovView kv = krylov_view(P, m);
+  const Seg* seg = P.d_seg.as<Seg>();
   double* V = P.d_V.as<double>();
   double* gx = P.d_gx.as<double>();
   double* gy = P.d_gy.as<double>();
-  arnoldi_load<<<grid_for(len), kThreads, 0, st>>>(V, len, kv.ctl, gx);
+  arnoldi_load<<<dim3(kv.gx, S), kThreads, 0, st>>>(V, len, seg, kv.ctl, gx);
   BP_LAUNCH_CHECK();
   matvec_launches(P, gx, gy, st, P.side, nullptr);
-  arnoldi_dots<<<kDotBlocks, kThreads, 0, st>>>(V, len, gy, kv.ctl, kv.partial);
-  arnoldi_reduce<<<m, kThreads, 0, st>>>(kv.partial, kDotBlocks, kv.ctl, kv.U);
-  arnoldi_orth<<<kDotBlocks, kThreads, 0, st>>>(V, len, gy, kv.U, kv.ctl, kv.partial);
-  arnoldi_finish<<<1, kThreads, 0, st>>>(kv.partial, kDotBlocks, kv.U, kv.c, kv.s, kv.y, kv.ctl, handle,
-                                         use_handle);
+  arnoldi_dots<<<dim3(kv.nbs, S), kThreads, 0, st>>>(V, len, gy, seg, kv.ctl, m, kv.partial);
+  arnoldi_reduce<<<dim3(m, S), kThreads, 0, st>>>(kv.partial, kv.nbs, kv.ctl, m, kv.U0, kv.ks);
+  arnoldi_orth<<<dim3(kv.nbs, S), kThreads, 0, st>>>(V, len, gy, kv.U0, kv.ks, seg, kv.ctl, m, kv.partial);
+  arnoldi_finish<<<S, kThreads, 0, st>>>(kv.partial, kv.nbs, m, kv.U0, kv.ks, kv.ctl, handle, use_handle);
+  if (S > 1) any_continue<<<1, kThreads, 0, st>>>(kv.ctl, S, kv.all, handle, use_handle);
   BP_LAUNCH_CHECK();
 }
 
@@ -485,38 +589,43 @@ bool ensure_gmres_graph(Problem& P, int m) {
 }  // namespace
 
 int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,
-                 double* rel_resid) {
+                 double* rel_resid, int* iters) {
   Ctx* ctx = P.ctx;
   cudaStream_t st = ctx->stream;
   const int64_t len = 2 * (int64_t)P.n;
+  const int S = P.n_scen();
   if (max_iters <= 0) throw std::invalid_argument("max_iters must be positive");
   const int m = (restart > 0 && restart < max_iters) ? restart : max_iters;
   if (P.krylov_m != m || !P.d_V.get()) {
     P.d_V.alloc(ctx, sizeof(double) * (size_t)len * (m + 1));
-    P.d_scal.alloc(ctx, krylov_scalar_bytes(m));
+    P.d_scal.alloc(ctx, krylov_scalar_bytes(m, S));
     P.krylov_m = m;
   }
+  if (!P.d_seg.get()) {
+    std::vector<Seg> seg(S);
+    for (int s = 0; s < S; ++s) seg[s] = {P.scen_first[s], P.scen_first[s + 1] - P.scen_first[s]};
+    P.d_seg = upload(ctx, seg);
+  }
+  const Seg* seg = P.d_seg.as<Seg>();
   double* V = P.d_V.as<double>();
   const KrylovView kv = krylov_view(P, m);
-  auto norm_into = [&](const double* v, double* out) {
-    dot_partials<<<dim3(kDotBlocks, 1), kThreads, 0, st>>>(v, len, v, len, kv.partial);
-    reduce_partials<<<1, kThreads, 0, st>>>(kv.partial, kDotBlocks, out, 1);
-  };
-  const int g = grid_for(len);
-  norm_into(b_dev, &kv.ctl->nrm_b);
-  set_stop<<<1, 1, 0, st>>>(kv.ctl, tol);
+  const int sb = (S + kThreads - 1) / kThreads;
+  seg_sq_partials<<<dim3(kv.nbs, S), kThreads, 0, st>>>(b_dev, seg, P.n, kv.partial);
+  norm_b_finish<<<S, kThreads, 0, st>>>(kv.partial, kv.nbs, kv.ctl, tol);
   BP_LAUNCH_CHECK();
   const bool graph = ensure_gmres_graph(P, m);
   int total = 0;
-  KrylovCtl h_ctl{};
+  std::vector<KrylovCtl> h_ctl(S);
   while (true) {
-    BP_CUDA(cudaMemsetAsync(kv.U, 0, sizeof(double) * ((size_t)m * (m + 1) / 2 + 2 * m + (m + 1)), st));
-    // r = A x - b into V[:,0], normalised; y[0] = beta
+    BP_CUDA(cudaMemsetAsync(kv.U0, 0, sizeof(double) * (size_t)S * kv.ks, st));
+    // r = A x - b into V[:,0], normalised per scenario; y[0] = beta
     matvec_device(P, x_dev, V);
-    sub_inplace<<<g, kThreads, 0, st>>>(V, b_dev, len);
-    norm_into(V, &kv.ctl->h);
-    scale_by_norm<<<g, kThreads, 0, st>>>(V, &kv.ctl->h, len);
-    cycle_start<<<1, 1, 0, st>>>(kv.ctl, kv.y, std::min(m, max_iters - total));
+    sub_inplace<<<grid_for(len), kThreads, 0, st>>>(V, b_dev, len);
+    seg_sq_partials<<<dim3(kv.nbs, S), kThreads, 0, st>>>(V, seg, P.n, kv.partial);
+    norm_r_finish<<<S, kThreads, 0, st>>>(kv.partial, kv.nbs, kv.ctl);
+    seg_scale_by_norm<<<dim3(kv.gx, S), kThreads, 0, st>>>(V, seg, P.n, kv.ctl);
+    cycle_start<<<sb, kThreads, 0, st>>>(kv.ctl, S, kv.U0, kv.ks, (int64_t)m * (m + 1) / 2 + 2 * m,
+                                         std::min(m, max_iters - total), kv.all);
     BP_LAUNCH_CHECK();
     if (graph) {
       BP_CUDA(cudaGraphLaunch(P.gmres_graph, st));
@@ -524,21 +633,36 @@ int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int
       while (true) {
         arnoldi_step_launches(P, m, st, cudaGraphConditionalHandle{}, 0);
         int cont = 0;
-        BP_CUDA(cudaMemcpyAsync(&cont, &kv.ctl->cont, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (S == 1)
+          BP_CUDA(cudaMemcpyAsync(&cont, &kv.ctl->cont, sizeof(int), cudaMemcpyDeviceToHost, st));
+        else
+          BP_CUDA(cudaMemcpyAsync(&cont, &kv.all->any, sizeof(int), cudaMemcpyDeviceToHost, st));
         BP_CUDA(cudaStreamSynchronize(st));
         if (!cont) break;
       }
     }
-    packed_back_substitution<<<1, 1, 0, st>>>(kv.U, kv.ctl, kv.y);
-    update_x<<<g, kThreads, 0, st>>>(V, len, kv.ctl, kv.y, x_dev, len);
+    packed_back_substitution<<<sb, kThreads, 0, st>>>(kv.U0, kv.ks, m, kv.ctl, S);
+    update_x<<<dim3(kv.gx, S), kThreads, 0, st>>>(V, len, seg, kv.ctl, kv.U0, kv.ks, m, x_dev);
     BP_LAUNCH_CHECK();
-    BP_CUDA(cudaMemcpyAsync(&h_ctl, kv.ctl, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, st));
+    BP_CUDA(cudaMemcpyAsync(h_ctl.data(), kv.ctl, sizeof(KrylovCtl) * S, cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
-    total += h_ctl.j;
-    if (h_ctl.last <= h_ctl.stop || total >= max_iters || restart <= 0) break;
+    int steps = 0;
+    bool all_done = true;
+    for (const KrylovCtl& c : h_ctl) {
+      steps = std::max(steps, c.j);
+      all_done = all_done && c.last <= c.stop;
+    }
+    total += steps;
+    if (all_done || total >= max_iters || restart <= 0) break;
   }
-  if (rel_resid) *rel_resid = h_ctl.nrm_b > 0 ? h_ctl.last / h_ctl.nrm_b : 0.0;
-  return total;
+  int worst = 0;
+  for (int s = 0; s < S; ++s) {
+    const KrylovCtl& c = h_ctl[s];
+    if (rel_resid) rel_resid[s] = c.nrm_b > 0 ? c.last / c.nrm_b : 0.0;
+    if (iters) iters[s] = c.iters;
+    worst = std::max(worst, c.iters);
+  }
+  return worst;
 }
 
 }  // namespace bp

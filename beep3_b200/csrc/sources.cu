@@ -295,12 +295,13 @@ void rhs_posed_device(Problem& P, const double* const* charges_host, const int32
       w[3] = ch[3];
     }
   }
-  // per instance the other instances' charges, one list after another
+  // per instance the other instances' charges of its scenario, one list
+  // after another
   std::vector<size_t> ostart(ni + 1, 0);
   std::vector<double> others;
   for (int k = 0; k < ni; ++k) {
     for (int j = 0; j < ni; ++j)
-      if (j != k) others.insert(others.end(), world.begin() + 4 * wstart[j], world.begin() + 4 * wstart[j + 1]);
+      if (j != k && P.placements[j].scenario == P.placements[k].scenario) others.insert(others.end(), world.begin() + 4 * wstart[j], world.begin() + 4 * wstart[j + 1]);
     ostart[k + 1] = others.size() / 4;
   }
   DevBuf& dch = P.scratch_charges;

@@ -21,7 +21,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .beep import BEEP, DEFAULT_NBSIZE, Mesh
+from .batch import ScenarioBatch
+from .beep import BEEP, DEFAULT_NBSIZE, EngineContext, Mesh
 from .geometry import random_quaternion
 
 
@@ -102,10 +103,46 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
     return out, iso
 
 
+def _batch_worker(mesh_a, mesh_b, poses, chunks, kappa, precision, nbsize, device, tol, max_it, context=None,
+                  isolated=(), snap=False):
+    """Batches of poses on one engine context: each chunk of poses is one
+    batch problem (every pose a scenario of A and B), solved with shared
+    launches.  The single-molecule problems in ``isolated`` are solved
+    first.  Returns (pose results, their energies)."""
+    eng = context if context is not None else EngineContext(device)
+    out = []
+    try:
+        iso = [_solve_energy(inst, kappa, precision, nbsize, device, tol, max_it, context=eng, snap=snap)[0]
+               for inst in isolated]
+        ident = np.array([1.0, 0.0, 0.0, 0.0])
+        ca = mesh_a.centre
+        for chunk in chunks:
+            scen = []
+            for k in chunk:
+                bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device,
+                          context=eng)
+                bp.snap_cube_edge = snap
+                bp.insert_mesh_instance(mesh_a, offset=ca, rotation=ident, eps_protein=2.0)
+                bp.insert_mesh_instance(mesh_b, offset=ca + poses[k].offset, rotation=poses[k].rotation,
+                                        eps_protein=2.0)
+                scen.append(bp)
+            batch = ScenarioBatch(scen, context=eng)
+            try:
+                info = batch.solve(tol, max_it)
+                es = batch.calculate_energies()
+            finally:
+                batch.close()
+            out.extend((k, e, its) for k, (e, _), its in zip(chunk, es, info.iterations))
+    finally:
+        if context is None:
+            eng.close()
+    return out, iso
+
+
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
                     nbsize: int = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
                     max_iterations: int = 100, contexts: list | None = None,
-                    snap_cube_edges: bool = False) -> ScanResult:
+                    snap_cube_edges: bool = False, batch: int = 1) -> ScanResult:
     """``contexts``: EngineContexts for the workers (at least ``workers``), kept
     by the caller across scans so that the meshes and device blocks stay on
     the device; by default each worker has its own for this scan.
@@ -113,7 +150,11 @@ def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float 
     (BEEP.snap_cube_edge), so that poses of similar extent share the
     far-field tables and operators a context keeps instead of computing them
     per pose; energies then differ from the exact cube's by the FMM's
-    truncation error."""
+    truncation error.  ``batch`` > 1: poses are solved ``batch`` at a time
+    as the scenarios of one batch problem (ScenarioBatch), sorted by
+    separation so that a batch's common cube edge is close to each pose's
+    own; a pose's energy then differs from its own problem's by the FMM's
+    truncation error (its tree is built in the batch's cube)."""
     t0 = time.perf_counter()
     ident = np.array([1.0, 0.0, 0.0, 0.0])
     ca = mesh_a.centre
@@ -125,12 +166,26 @@ def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float 
     isolated = [[] for _ in range(workers)]
     isolated[0].append([(mesh_a, ca, ident)])
     isolated[1 % workers].append([(mesh_b, mesh_b.centre, ident)])
-    with ThreadPoolExecutor(max_workers=workers) as ex:
-        fw = [ex.submit(_scan_worker, mesh_a, mesh_b, poses, list(range(w, len(poses), workers)), kappa, precision,
-                        nbsize, device, tol, max_iterations, contexts[w] if contexts else None, isolated[w],
-                        snap_cube_edges)
-              for w in range(workers)]
-        outs = [f.result() for f in fw]
+    if batch > 1:
+        order = sorted(range(len(poses)), key=lambda k: float(np.linalg.norm(poses[k].offset)))
+        chunks = [order[c:c + batch] for c in range(0, len(order), batch)]
+        workers = max(1, min(workers, len(chunks)))
+        isolated = [[] for _ in range(workers)]
+        isolated[0].append([(mesh_a, ca, ident)])
+        isolated[1 % workers].append([(mesh_b, mesh_b.centre, ident)])
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            fw = [ex.submit(_batch_worker, mesh_a, mesh_b, poses, chunks[w::workers], kappa, precision, nbsize,
+                            device, tol, max_iterations, contexts[w] if contexts else None, isolated[w],
+                            snap_cube_edges)
+                  for w in range(workers)]
+            outs = [f.result() for f in fw]
+    else:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            fw = [ex.submit(_scan_worker, mesh_a, mesh_b, poses, list(range(w, len(poses), workers)), kappa,
+                            precision, nbsize, device, tol, max_iterations, contexts[w] if contexts else None,
+                            isolated[w], snap_cube_edges)
+                  for w in range(workers)]
+            outs = [f.result() for f in fw]
     e_a = outs[0][1][0]
     e_b = outs[1 % workers][1][-1]
     res = sorted(r for o in outs for r in o[0])

@@ -407,9 +407,9 @@ def _scan_mode(args, local):
         # seen problems of the sizes the timed scan builds
         snap = not args.exact_cubes
         rigid_body_scan(ma, mb, random_poses(args.poses, seed=99), kappa=0.1, workers=args.workers, device=local,
-                        contexts=ctxs, snap_cube_edges=snap)
+                        contexts=ctxs, snap_cube_edges=snap, batch=args.batch)
         res = rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs,
-                              snap_cube_edges=snap)
+                              snap_cube_edges=snap, batch=args.batch)
     finally:
         for c in ctxs:
             c.close()
@@ -420,7 +420,8 @@ def _scan_mode(args, local):
         "data": "synthetic", "dtype": "fp32 near field/FMM + fp64 singular/GMRES",
         "config": {"workload": "batched rigid-body scan: star k=6 (40962 patches, 2000 charges) + star k=5 "
                                "(10242 patches, 500 charges), kappa 0.1, separation 45-80 A",
-                   "poses": len(poses), "concurrent_poses": args.workers,
+                   "poses": len(poses), "workers": args.workers,
+                   "poses_per_batch": args.batch,
                    "engine_contexts": "one per worker, kept across scans",
                    "cube_edges": "exact per pose" if args.exact_cubes else
                                  "rounded up to 2^(k/8): poses share far-field plans"},
@@ -596,6 +597,8 @@ def main():
     ap.add_argument("--workload", default="star", choices=["kirkwood", "star", "star-small", "scan", "serve"],
                     help="scan / serve: the batched rigid-body scan and the served request stream")
     ap.add_argument("--poses", type=int, default=64, help="scan: number of poses")
+    ap.add_argument("--batch", type=int, default=1,
+                    help="scan: poses solved together as the scenarios of one batch problem")
     ap.add_argument("--requests", type=int, default=24, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=8.0, help="serve: Poisson arrival rate, requests/s")
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")

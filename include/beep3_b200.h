@@ -167,6 +167,7 @@ typedef struct {
                                 host drove the loop step by step */
   double fmm_setup_ms;       /* host wall time of the far-field set-up (tables, operators, schedule) */
   double setup_ms;           /* host wall time from the tree build to a problem ready to run */
+  int64_t n_scenarios;       /* independent scenarios (bp_problem_create_batch), else 1 */
 } bp_problem_info;
 
 /* Builds the adaptive octree, the singular self-patch integrals and the
@@ -214,6 +215,22 @@ typedef struct {
 /* bp_problem_create for the instances' patches, concatenated in instance
  * order. */
 int32_t bp_problem_create_posed(bp_ctx ctx, const bp_instance* instances, int32_t n_instances,
+                                const bp_params* params, bp_problem* out);
+/* Several independent scenarios in one problem: a batch of poses whose
+ * matvecs and solves share every kernel launch (BEEP::insert_mesh_instance /
+ * move_mesh_instance, src/beep/beep.cpp:223-290, run once per scenario).
+ * Scenario s holds instances [scenario_first[s], scenario_first[s+1])
+ * (scenario_first[0] = 0, scenario_first[n_scenarios] = n_instances, every
+ * scenario non-empty); its tree is built in the cube of centre
+ * cube_centres[3s..3s+2] and edge params->cube_edge (one edge for all, at
+ * least every scenario's own extent; params->cube_centre is ignored).  The
+ * matvec is block diagonal: no interaction crosses scenarios, and each
+ * block equals the matvec of bp_problem_create_posed on the scenario's
+ * instances with that cube, up to rounding.  Patches are concatenated in
+ * instance order; bp_rhs_posed sums each instance's charges over its own
+ * scenario only; bp_solve_batch solves every scenario with its own GMRES. */
+int32_t bp_problem_create_batch(bp_ctx ctx, const bp_instance* instances, int32_t n_instances,
+                                const int32_t* scenario_first, int32_t n_scenarios, const double* cube_centres,
                                 const bp_params* params, bp_problem* out);
 int32_t bp_problem_destroy(bp_problem p);
 int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info);
@@ -275,6 +292,13 @@ int32_t bp_problem_test_wait_timeout(bp_problem p, int32_t enable);
  * max_iters, as in the reference.  Host arrays of 2N doubles. */
 int32_t bp_solve(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
                  int32_t* iterations, double* rel_residual);
+/* bp_solve of a batch problem: every scenario runs its own GMRES (its own
+ * Krylov basis, ||rhs|| and stop test) in shared launches, a converged
+ * scenario sitting out the remaining steps; iterations and rel_residual
+ * receive one entry per scenario.  bp_solve on a batch reports the worst
+ * scenario.  BP_ERR_NOT_CONVERGED when some scenario did not converge. */
+int32_t bp_solve_batch(bp_problem p, const double* rhs, double* x, double tol, int32_t max_iters, int32_t restart,
+                       int32_t* iterations, double* rel_residual);
 /* Same on device arrays (still blocks: the Krylov loop reads its residual). */
 int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_dev, double tol, int32_t max_iters,
                         int32_t restart, int32_t* iterations, double* rel_residual);
@@ -283,7 +307,8 @@ int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_dev, doub
  * Coulomb potential and field of all charges at every qualocation point,
  * weighted and scaled by 1/(4 pi eps_solvent).  charges_xyzq: [n][4]. */
 int32_t bp_rhs(bp_problem p, const double* charges_xyzq, int32_t n_charges, double eps_solvent, double* rhs);
-/* The same for a problem made by bp_problem_create_posed, from each
+/* The same for a problem made by bp_problem_create_posed (or _batch: each
+ * instance then sees the charges of its own scenario only), from each
  * instance's charges in its mesh's own frame (the frame of the points given
  * to bp_mesh_create): charges_xyzq[k] holds n_charges[k] charges of
  * instance k.  The potential of an instance's own charges at its own
