@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
     const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
     const T* __restrict__ coef, const double* __restrict__ diag, int n, const double* __restrict__ x,
-    const double* __restrict__ yfar, double* __restrict__ y, int n_items) {
+    const double* __restrict__ yfar, double* __restrict__ y, int n_items, int stage_cols) {
   extern __shared__ unsigned char smem_raw[];
   T* sf = reinterpret_cast<T*>(smem_raw);
   // persistent: a few blocks per SM stride over the items, leaving room on
@@ -501,6 +501,43 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
   const NfItem it = items[item];
   const int64_t c0 = col_off[it.leaf];
   const int ncols = (int)(col_off[it.leaf + 1] - c0);
+  if (ncols > stage_cols) {
+    // a neighbourhood beyond the shared-memory staging: x gathered through
+    // the column ids (x is L2-resident), one coefficient per lane and step
+    using V4 = typename Vec4<T>::type;
+    const V4* blk = reinterpret_cast<const V4*>(coef) + coef_off[it.leaf];
+    const int lane = threadIdx.x & 31;
+    const int64_t r0 = row_off[it.leaf] + it.row_begin;
+    for (int r = threadIdx.x >> 5; r < it.row_count; r += blockDim.x >> 5) {
+      const V4* rowp = blk + (int64_t)(it.row_begin + r) * ncols;
+      T accf = 0, acch = 0;
+      for (int cc = lane; cc < ncols; cc += 32) {
+        const V4 v = ld_stream(rowp + cc);
+        const int j = cols[c0 + cc];
+        const T xf = T(x[j]), xh = T(x[n + j]);
+        accf += v.y * xf - v.x * xh;
+        acch += v.w * xf - v.z * xh;
+      }
+      double df = (double)accf, dh = (double)acch;
+      for (int o = 16; o > 0; o >>= 1) {
+        df += __shfl_xor_sync(0xffffffffu, df, o);
+        dh += __shfl_xor_sync(0xffffffffu, dh, o);
+      }
+      if (lane == 0) {
+        const int i = rows[r0 + r];
+        const double fi = x[i], hi = x[n + i];
+        double yf = df + (diag[4 * i + 1] * fi - diag[4 * i + 0] * hi);
+        double yh = dh + (diag[4 * i + 3] * fi - diag[4 * i + 2] * hi);
+        if (yfar) {
+          yf += yfar[i];
+          yh += yfar[n + i];
+        }
+        y[i] = yf;
+        y[n + i] = yh;
+      }
+    }
+    continue;
+  }
   T* sh = sf + ncols;
   for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) {
     const int j = cols[c0 + cc];
@@ -564,6 +601,10 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
   }
   }
 }
+
+// Columns of a leaf whose x values the apply kernel stages in shared memory
+// (2 values each): up to the per-block limit of 227 KB
+int apply_stage_cols(size_t elem) { return (int)(227 * 1024 / (2 * elem)); }
 
 }  // namespace
 
@@ -709,9 +750,8 @@ void nf_assemble(Problem& P) {
   }
   BP_CUDA(cudaEventRecord(P.asm_t1, st));
   // apply work items; the apply kernel's shared memory holds the x values of
-  // a leaf's columns
-  const size_t apply_smem = 2 * elem * (size_t)nf.max_cols;
-  if (apply_smem > 227 * 1024) throw std::invalid_argument("neighbourhood too large for the near-field apply");
+  // a leaf's columns (leaves with more columns than fit gather x instead)
+  const size_t apply_smem = 2 * elem * (size_t)std::min(nf.max_cols, apply_stage_cols(elem));
   if (P.fp64)
     ensure_dynamic_smem((const void*)apply_kernel<double>, apply_smem);
   else
@@ -757,18 +797,19 @@ int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_
     return 1;
   }
   const size_t elem = P.fp64 ? sizeof(double) : sizeof(float);
-  const size_t smem = 2 * elem * (size_t)nf.max_cols;
+  const int stage = apply_stage_cols(elem);
+  const size_t smem = 2 * elem * (size_t)std::min(nf.max_cols, stage);
   const int grid = std::min(nf.n_items, kApplyBlocksPerSm * P.ctx->sm_count);
   if (P.fp64) {
     apply_kernel<double><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
         nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev,
-        yfar_dev, y_dev, nf.n_items);
+        yfar_dev, y_dev, nf.n_items, stage);
   } else {
     apply_kernel<float><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
         nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev,
-        yfar_dev, y_dev, nf.n_items);
+        yfar_dev, y_dev, nf.n_items, stage);
   }
   BP_LAUNCH_CHECK();
   return 1;

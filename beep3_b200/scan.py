@@ -59,8 +59,13 @@ def random_poses(n: int, seed: int, rmin: float = 45.0, rmax: float = 80.0) -> l
     return out
 
 
+def _tree_kw(nbsize):
+    """BEEP tree keywords: an nbsize, or a dict of tree settings (autotune)."""
+    return dict(nbsize) if isinstance(nbsize, dict) else dict(nbsize=nbsize)
+
+
 def _solve_energy(instances, kappa, precision, nbsize, device, tol, max_it, context=None, snap=False):
-    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
+    bp = BEEP(eps_solvent=80.0, kappa=kappa, precision=precision, device=device, context=context, **_tree_kw(nbsize))
     bp.snap_cube_edge = snap
     try:
         for mesh, off, q in instances:
@@ -79,7 +84,7 @@ def _scan_worker(mesh_a, mesh_b, poses, idx, kappa, precision, nbsize, device, t
     set-up, then the solve).  The single-molecule problems in ``isolated``
     are solved first, on the same context.  Returns (pose results, their
     energies)."""
-    bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device, context=context)
+    bp = BEEP(eps_solvent=80.0, kappa=kappa, precision=precision, device=device, context=context, **_tree_kw(nbsize))
     bp.cache_own_potentials = True  # instance B only moves: its own potential, and A's, stay
     bp.snap_cube_edge = snap
     out = []
@@ -119,8 +124,8 @@ def _batch_worker(mesh_a, mesh_b, poses, chunks, kappa, precision, nbsize, devic
         for chunk in chunks:
             scen = []
             for k in chunk:
-                bp = BEEP(eps_solvent=80.0, kappa=kappa, nbsize=nbsize, precision=precision, device=device,
-                          context=eng)
+                bp = BEEP(eps_solvent=80.0, kappa=kappa, precision=precision, device=device, context=eng,
+                          **_tree_kw(nbsize))
                 bp.snap_cube_edge = snap
                 bp.insert_mesh_instance(mesh_a, offset=ca, rotation=ident, eps_protein=2.0)
                 bp.insert_mesh_instance(mesh_b, offset=ca + poses[k].offset, rotation=poses[k].rotation,
@@ -140,10 +145,12 @@ def _batch_worker(mesh_a, mesh_b, poses, chunks, kappa, precision, nbsize, devic
 
 
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
-                    nbsize: int = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
+                    nbsize: int | dict = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
                     max_iterations: int = 100, contexts: list | None = None,
                     snap_cube_edges: bool = False, batch: int = 1) -> ScanResult:
-    """``contexts``: EngineContexts for the workers (at least ``workers``), kept
+    """``nbsize``: the reference tree's nbsize, or a dict of BEEP tree keywords
+    (``TuneResult.settings()`` of autotune).  ``contexts``: EngineContexts
+    for the workers (at least ``workers``), kept
     by the caller across scans so that the meshes and device blocks stay on
     the device; by default each worker has its own for this scan.
     ``snap_cube_edges``: round each pose's bounding-cube edge up to a grid
@@ -192,3 +199,34 @@ def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float 
     dt = time.perf_counter() - t0
     ec = [r[1] for r in res]
     return ScanResult([e - e_a - e_b for e in ec], ec, e_a, e_b, dt, [r[2] for r in res])
+
+
+def scan_trial(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
+               workers: int = 4, batch: int = 1, device: int = 0, contexts: list | None = None,
+               snap_cube_edges: bool = False, tol: float = 1e-6, max_iterations: int = 100, repeats: int = 1):
+    """An autotune trial (beep3_b200.autotune) that runs a short scan of
+    ``poses`` in the given worker / batch configuration with each candidate
+    tree: cost = the best of ``repeats`` scans' time per pose, energies = the
+    poses' complex energies."""
+    from ._native import BP_ERR_UNSUPPORTED, BeepError
+    from .autotune import Trial
+
+    def run(tree: str, size: int, nterms: int) -> Trial:
+        t = Trial(tree, size, nterms)
+        best = float("inf")
+        for _ in range(repeats):
+            try:
+                res = rigid_body_scan(mesh_a, mesh_b, poses, kappa=kappa, precision=precision,
+                                      nbsize=t.settings(), workers=workers, device=device, tol=tol,
+                                      max_iterations=max_iterations, contexts=contexts,
+                                      snap_cube_edges=snap_cube_edges, batch=batch)
+            except BeepError as e:
+                if e.code == BP_ERR_UNSUPPORTED:
+                    t.status = "unsupported"
+                    return t
+                raise
+            best = min(best, res.seconds / len(poses) * 1e3)
+            t.energies = list(res.complex_energies)
+        t.cost_ms = best
+        return t
+    return run

@@ -402,14 +402,32 @@ def _scan_mode(args, local):
     # one engine context per worker, kept across scans: the meshes and the
     # device blocks of a pose stay on the device for the next
     ctxs = [b.EngineContext(local) for _ in range(args.workers)]
+    tree = 1500  # the reference's nbsize
+    tuned = None
     try:
+        snap = not args.exact_cubes
+        if args.autotune:
+            # the tree chosen by short scans of 16 other poses in the same
+            # worker / batch configuration, outside the timed scans (energies
+            # within 1e-4 of the reference tree's)
+            from beep3_b200.autotune import autotune
+            from beep3_b200.scan import scan_trial
+            tune_poses = random_poses(16, seed=98)
+            rigid_body_scan(ma, mb, tune_poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs,
+                            snap_cube_edges=snap, batch=args.batch)
+            t0 = time.perf_counter()
+            res_t = autotune(scan_trial(ma, mb, tune_poses, kappa=0.1, workers=args.workers, batch=args.batch,
+                                        device=local, contexts=ctxs, snap_cube_edges=snap))
+            tuned = {"settings": res_t.settings(), "seconds": time.perf_counter() - t0,
+                     "trials": [{"tree": t.tree, "size": t.size, "ms_per_pose": t.cost_ms, "status": t.status}
+                                for t in res_t.trials]}
+            tree = res_t.settings()
         # warm-up: a scan of as many other poses, so that every context has
         # seen problems of the sizes the timed scan builds
-        snap = not args.exact_cubes
         rigid_body_scan(ma, mb, random_poses(args.poses, seed=99), kappa=0.1, workers=args.workers, device=local,
-                        contexts=ctxs, snap_cube_edges=snap, batch=args.batch)
+                        contexts=ctxs, snap_cube_edges=snap, batch=args.batch, nbsize=tree)
         res = rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs,
-                              snap_cube_edges=snap, batch=args.batch)
+                              snap_cube_edges=snap, batch=args.batch, nbsize=tree)
     finally:
         for c in ctxs:
             c.close()
@@ -426,6 +444,7 @@ def _scan_mode(args, local):
                    "cube_edges": "exact per pose" if args.exact_cubes else
                                  "rounded up to 2^(k/8): poses share far-field plans"},
         "seconds": res.seconds, "mean_iterations": float(np.mean(res.iterations)),
+        "tree": tree, "autotune": tuned,
         "interaction_energy_kj_per_mol": {"min": float(e.min()), "max": float(e.max()), "mean": float(e.mean())},
     }), flush=True)
 
@@ -597,6 +616,8 @@ def main():
     ap.add_argument("--workload", default="star", choices=["kirkwood", "star", "star-small", "scan", "serve"],
                     help="scan / serve: the batched rigid-body scan and the served request stream")
     ap.add_argument("--poses", type=int, default=64, help="scan: number of poses")
+    ap.add_argument("--autotune", action="store_true",
+                    help="scan: choose the tree by short measured scans before the timed scans")
     ap.add_argument("--batch", type=int, default=1,
                     help="scan: poses solved together as the scenarios of one batch problem")
     ap.add_argument("--requests", type=int, default=24, help="serve: number of requests")

@@ -47,3 +47,21 @@ def test_on_demand_equals_cached(mesh_case, precision):
     assert abs(e2 - e1) / abs(e1) < 1e-6
     cached.close()
     ondem.close()
+
+
+def test_oversized_neighbourhood_gathers_x():
+    """One leaf of 40962 patches: its 40962 columns exceed the apply
+    kernel's shared-memory staging (29056 in FP32), so the cached apply
+    gathers x through the column ids; it must equal the on-demand path."""
+    V, T = b.icosphere(6, 20.0)
+    mesh = b.Mesh(V, T, b.charges_in_sphere(40, 15.0, seed=77))
+    cached = make_beep(mesh, kappa=0.1, nbsize=40962, precision="mixed")
+    inf = cached.info()
+    assert inf.n_leaves == 1 and inf.n_nearfield_cols == 40962 and inf.fmm_active == 0
+    x = np.random.default_rng(11).standard_normal(2 * cached.num_patches)
+    yc = cached.matvec(x)
+    cached.close()
+    ondem = make_beep(mesh, kappa=0.1, nbsize=40962, precision="mixed", nearfield_on_demand=True)
+    yo = ondem.matvec(x)
+    ondem.close()
+    assert rel_l2(yc, yo) < 1e-6
