@@ -695,7 +695,8 @@ BP_API int32_t bp_solve_device(bp_problem p, const double* rhs_dev, double* x_de
     if (!(tol > 0)) return fail(BP_ERR_INVALID, "bp_solve_device: tol must be positive");
     DeviceGuard g(P->ctx->device);
     std::vector<double> rr(P->n_scen(), 0.0);
-    int its = gmres_device(*P, rhs_dev, x_dev, tol, max_iters, restart, rr.data());
+    const bool x0 = device_all_zero(*P, x_dev, 2 * (int64_t)P->n);
+    int its = gmres_device(*P, rhs_dev, x_dev, tol, max_iters, restart, rr.data(), nullptr, x0);
     const double worst = *std::max_element(rr.begin(), rr.end());
     if (iterations) *iterations = its;
     if (rel_residual) *rel_residual = worst;
@@ -721,7 +722,8 @@ static int32_t solve_host(bp_problem p, const double* rhs, double* x, double tol
     BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
     std::vector<double> rr(P->n_scen(), 0.0);
     std::vector<int> its(P->n_scen(), 0);
-    gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, rr.data(), its.data());
+    const bool x0 = std::all_of(x, x + 2 * (size_t)P->n, [](double v) { return v == 0.0; });
+    gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, rr.data(), its.data(), x0);
     BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
     fmm_check_waits(*P);

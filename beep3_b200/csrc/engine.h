@@ -372,6 +372,10 @@ struct Problem {
   // grow-only scratch of the source terms (charges, per-point values, the
   // right-hand side of bp_solve): kept so repeated calls allocate nothing
   DevBuf scratch_charges, scratch_vals, scratch_b;
+  // qualocation point indices in spatial order within each instance's range
+  // (patches in the tree's leaf order), for the mixed right-hand side; made
+  // on its first use
+  DevBuf d_qual_order;
   int krylov_m = 0;
   double tree_ms = 0, assemble_ms = 0, fmm_setup_ms = 0, setup_ms = 0;
   // the near-field assembly runs on a stream of its own while the far field
@@ -470,9 +474,12 @@ void matvec_setup(Problem& P);
 void matvec_device(Problem& P, const double* x_dev, double* y_dev, StageTimes* st = nullptr);
 // GMRES of every scenario of P (one for an ordinary problem): rel_resid and
 // iters (may be null) receive one entry per scenario; returns the most
-// iterations any scenario took
+// iterations any scenario took.  x_is_zero: the caller knows x = 0 on entry,
+// so the first residual is -b without a matvec.
 int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,
-                 double* rel_resid, int* iters = nullptr);
+                 double* rel_resid, int* iters = nullptr, bool x_is_zero = false);
+// true when every entry of the device vector is zero (one reduction, synchronises)
+bool device_all_zero(Problem& P, const double* x_dev, int64_t len);
 // sources.cu
 void rhs_device(Problem& P, const double* charges_dev, int n_charges, double eps_solvent, double* rhs_dev);
 // right-hand side of a posed problem from each instance's charges in its

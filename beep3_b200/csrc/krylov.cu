@@ -39,6 +39,21 @@ constexpr int kDotBlocks = 296;  // 2 per SM on a 148-SM part
 // DBL_MIN guard used by the reference to avoid 0/0 (src/beep/beep.cpp:1360)
 __device__ __forceinline__ double near0(double v) { return v == 0.0 ? 2.2250738585072014e-308 : v; }
 
+// r = -b: the residual of x = 0, where A x is exactly zero (every term of
+// the near field and of the far field is a product with an entry of x)
+__global__ void negate_into(double* __restrict__ r, const double* __restrict__ b, int64_t len) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    r[i] = -b[i];
+}
+
+// flag = 1 if some entry of x is not zero
+__global__ void any_nonzero(const double* __restrict__ x, int64_t len, int* __restrict__ flag) {
+  int nz = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+    nz |= x[i] != 0.0;
+  if (__syncthreads_or(nz) && threadIdx.x == 0) *flag = 1;
+}
+
 // r = r - b ; then v0 = r / near0(||r||) is done by seg_scale_by_norm
 __global__ void sub_inplace(double* __restrict__ r, const double* __restrict__ b, int64_t len) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
@@ -588,8 +603,20 @@ bool ensure_gmres_graph(Problem& P, int m) {
 
 }  // namespace
 
+bool device_all_zero(Problem& P, const double* x_dev, int64_t len) {
+  cudaStream_t st = P.ctx->stream;
+  DevBuf flag(P.ctx, sizeof(int));
+  BP_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), st));
+  any_nonzero<<<grid_for(len), kThreads, 0, st>>>(x_dev, len, flag.as<int>());
+  BP_LAUNCH_CHECK();
+  int h = 0;
+  BP_CUDA(cudaMemcpyAsync(&h, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  BP_CUDA(cudaStreamSynchronize(st));
+  return h == 0;
+}
+
 int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int max_iters, int restart,
-                 double* rel_resid, int* iters) {
+                 double* rel_resid, int* iters, bool x_is_zero) {
   Ctx* ctx = P.ctx;
   cudaStream_t st = ctx->stream;
   const int64_t len = 2 * (int64_t)P.n;
@@ -616,11 +643,18 @@ int gmres_device(Problem& P, const double* b_dev, double* x_dev, double tol, int
   const bool graph = ensure_gmres_graph(P, m);
   int total = 0;
   std::vector<KrylovCtl> h_ctl(S);
+  bool x_zero = x_is_zero;
   while (true) {
     BP_CUDA(cudaMemsetAsync(kv.U0, 0, sizeof(double) * (size_t)S * kv.ks, st));
-    // r = A x - b into V[:,0], normalised per scenario; y[0] = beta
-    matvec_device(P, x_dev, V);
-    sub_inplace<<<grid_for(len), kThreads, 0, st>>>(V, b_dev, len);
+    // r = A x - b into V[:,0], normalised per scenario; y[0] = beta (for
+    // x = 0, -b: the same bits without the matvec)
+    if (x_zero) {
+      negate_into<<<grid_for(len), kThreads, 0, st>>>(V, b_dev, len);
+      x_zero = false;
+    } else {
+      matvec_device(P, x_dev, V);
+      sub_inplace<<<grid_for(len), kThreads, 0, st>>>(V, b_dev, len);
+    }
     seg_sq_partials<<<dim3(kv.nbs, S), kThreads, 0, st>>>(V, seg, P.n, kv.partial);
     norm_r_finish<<<S, kThreads, 0, st>>>(kv.partial, kv.nbs, kv.ctl);
     seg_scale_by_norm<<<dim3(kv.gx, S), kThreads, 0, st>>>(V, seg, P.n, kv.ctl);

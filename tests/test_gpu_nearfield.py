@@ -87,6 +87,25 @@ def test_restarted_gmres_converges(setup):
     assert np.linalg.norm(r) / np.linalg.norm(bp.rhs) < 1e-6
 
 
+def test_warm_start_runs_the_residual_matvec(setup):
+    """x0 = 0 starts from r = -b without a matvec; a nonzero x0 (the
+    converged solution, host and device entry points) starts from A x0 - b
+    and stops at once."""
+    prec, bp, pr = setup
+    bp.set_rhs()
+    x, its, rr, ok = bp.gmres(1e-8, 200)
+    assert ok and its > 2
+    x2, its2, rr2, ok2 = bp.gmres(1e-8, 200, x0=x)
+    assert ok2 and its2 <= 1
+    assert rel_l2(x2, x) < 1e-6  # one correction step within the 1e-8 stop test
+    import torch
+    xd = torch.tensor(x, device="cuda")
+    bd = torch.tensor(bp.rhs, device="cuda")
+    it, r = C.c_int32(), C.c_double()
+    N.check(N.lib().bp_solve_device(bp.build(), bd.data_ptr(), xd.data_ptr(), 1e-8, 200, 0, C.byref(it), C.byref(r)))
+    assert it.value <= 1 and rel_l2(xd.cpu().numpy(), x) < 1e-6
+
+
 def test_kappa_zero_and_planar(kirkwood_case):
     mesh = b.Mesh(kirkwood_case["V"], kirkwood_case["T"], kirkwood_case["charges"], planar=True)
     bp = make_beep(mesh, kappa=0.0)
