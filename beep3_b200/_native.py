@@ -81,6 +81,8 @@ class bp_problem_info(C.Structure):
         ("n_nearfield_pairs", C.c_int64), ("n_nearfield_cols", C.c_int64), ("fmm_active", C.c_int64), ("device_bytes", C.c_uint64),
         ("tree_ms", C.c_double), ("assemble_ms", C.c_double), ("gmres_graph", C.c_int64),
         ("fmm_setup_ms", C.c_double), ("setup_ms", C.c_double), ("n_scenarios", C.c_int64),
+        ("fmm_m2x_cols", C.c_int64), ("fmm_x2l_cols", C.c_int64), ("fmm_translations", C.c_int64),
+        ("fmm_shift_cols", C.c_int64), ("fmm_plane_waves", C.c_int64), ("fmm_coefficients", C.c_int64),
     ]
 
 

@@ -580,6 +580,13 @@ BP_API int32_t bp_problem_info_get(bp_problem p, bp_problem_info* info) {
   info->setup_ms = P->setup_ms;
   info->gmres_graph = P->gmres_graph ? 1 : 0;
   info->n_scenarios = P->n_scen();
+  const FmmWork w = fmm_work(*P);
+  info->fmm_m2x_cols = w.m2x_cols;
+  info->fmm_x2l_cols = w.x2l_cols;
+  info->fmm_translations = w.xl_entries;
+  info->fmm_shift_cols = w.shift_cols;
+  info->fmm_plane_waves = w.plane_waves;
+  info->fmm_coefficients = w.coefficients;
   return BP_OK;
 }
 

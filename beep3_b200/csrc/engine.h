@@ -460,6 +460,11 @@ void nf_join(Problem& P);      // orders the context's stream after it
 int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_dev, cudaStream_t stream);
 // fmm.cu
 bool fmm_active(const Problem& P);
+struct FmmWork {
+  long long m2x_cols = 0, x2l_cols = 0, xl_entries = 0, shift_cols = 0;
+  int plane_waves = 0, coefficients = 0;  // per direction / per channel
+};
+FmmWork fmm_work(const Problem& P);
 // Throws TimeoutError if a tensor-core FMM kernel of this problem gave up on
 // a bounded wait since the problem was created (its results are then void).
 // Synchronises the context stream.

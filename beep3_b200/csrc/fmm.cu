@@ -1710,6 +1710,9 @@ __global__ void __launch_bounds__(256) prep_csr_kernel(int E, int EQ, const Leaf
 struct FmmState {
   int nt = 9, E = 55, nlev = 0, np_max = 0, nl = 0;
   bool fp64 = true;
+  // work of one far-field pass: columns (node, channel) of the M->X and
+  // wave->local operators, translation entries, M2M / L2L columns
+  FmmWork work;
   // buffers a far-field plan shares among problems (see FmmPlan)
   using SharedBuf = std::shared_ptr<DevBuf>;
   SharedBuf tables_buf = std::make_shared<DevBuf>();  // one allocation holding every table
@@ -1836,6 +1839,8 @@ static void keep_fmm_plan(Problem& P, const FmmState& S) {
 void fmm_destroy(FmmState* s) { delete s; }
 
 bool fmm_active(const Problem& P) { return P.tree.n_levels - 1 >= 2; }
+
+FmmWork fmm_work(const Problem& P) { return P.fmm ? P.fmm->work : FmmWork{}; }
 
 void fmm_check_waits(Problem& P) {
   FmmState* S = P.fmm.get();
@@ -2471,6 +2476,19 @@ void fmm_setup(Problem& P) {
     S->xlc_tcount[lev] = (int)otiles.size() - S->xlc_tfirst[lev];
     S->xlr_count[lev] = (int)xl_ldst.size() - S->xlr_first[lev];
     if (S->tensor) xl_part += (long long)kXlSplit * ncl * R2;
+  }
+  {
+    long long m2x = 0, x2l = 0;
+    for (int lev = 1; lev < nlev; ++lev) {
+      m2x += (long long)src_lev[lev].size() * kCh;
+      x2l += (long long)S->xlt_count[lev] * kCh;
+    }
+    S->work.m2x_cols = m2x;
+    S->work.x2l_cols = x2l;
+    S->work.xl_entries = (long long)xle.size();
+    S->work.shift_cols = (long long)tcols.size();
+    S->work.plane_waves = S->np_max;
+    S->work.coefficients = S->E;
   }
   S->op_tiles = upload(c, otiles);
   S->op_cols = upload(c, ocols);

@@ -212,6 +212,57 @@ def stage_profile(bp, x, y, reps: int = 5):
     return ms, launches
 
 
+def scan_child(local: int) -> dict:
+    """Config B's batched rigid-body scan (64 poses of the two star
+    molecules, 2 workers x 8 poses per batch problem) in a child process on
+    the same GPU: its poses/s line, or the reason it has none."""
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--workload", "scan", "--workers", "2", "--batch", "8"]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+    for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+        d = json.loads(out.stdout.strip().splitlines()[-1])
+        return {k: d[k] for k in ("value", "unit", "seconds", "mean_iterations", "config") if k in d}
+    except Exception as e:  # the headline line stands without it
+        return {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+
+
+def matvec_roofline(inf, n, mv_ms, near_ms, stage_ms, hbm, peaks):
+    """The whole matvec against HBM with the survey's algorithmic bytes,
+    B_mv = P_nf (16 B coefficients + 4 B column id) + 4N x 8 B (x, y) + B_fmm,
+    B_fmm = nodes x 12 channels x (2 x E x 8 B (M, L read + write) + 6 x np x
+    2 x 8 B (plane waves written and read)), FP32 complex; and the far field
+    alone: its time in the graph (the matvec minus the near field, which
+    runs after it), its bytes, and the flops of its operator GEMMs (M->X and
+    wave->local, 12 np x 2E real MACs per column, three TF32 passes each)
+    against the stage times that hold them."""
+    E, NP = int(inf.fmm_coefficients), int(inf.fmm_plane_waves)
+    b_fmm = int(inf.n_nodes) * 12 * (2 * E * 8 + 6 * NP * 2 * 8) if inf.fmm_active else 0
+    b_mv = int(inf.n_nearfield_pairs) * 20 + 4 * n * 8 + b_fmm
+    far_ms = max(mv_ms - near_ms, 1e-9)
+    gemm_flops = 2.0 * (int(inf.fmm_m2x_cols) + int(inf.fmm_x2l_cols)) * (12 * NP) * (2 * E)
+    xl_flops = 8.0 * int(inf.fmm_translations) * 12 * NP
+    shift_flops = 2.0 * int(inf.fmm_shift_cols) * (2 * E) ** 2
+    gemm_stage_ms = float(stage_ms[3] + stage_ms[4])  # M->X and X->L (translations + wave->local) stages
+    tf32 = float(peaks.get("bf16_tflops", 1590.0)) / 2.0
+    achieved_tf = 3 * gemm_flops / (gemm_stage_ms * 1e-3) / 1e12 if gemm_stage_ms > 0 else 0.0
+    return {
+        "bound": "hbm", "unit": "GB/s", "algorithmic_bytes": b_mv, "achieved": b_mv / (mv_ms * 1e-3) / 1e9,
+        "peak": hbm, "frac": b_mv / (mv_ms * 1e-3) / 1e9 / hbm,
+        "far_field": {
+            "ms_in_graph": far_ms, "algorithmic_bytes": b_fmm,
+            "achieved_gbs": b_fmm / (far_ms * 1e-3) / 1e9, "frac_hbm": b_fmm / (far_ms * 1e-3) / 1e9 / hbm,
+            "flops": {"operator_gemms": gemm_flops, "translations": xl_flops, "shifts": shift_flops},
+            "operator_gemm_tflops_3xtf32": achieved_tf, "tf32_peak_tflops": tf32,
+            "operator_gemm_frac": achieved_tf / tf32,
+            "note": "far-field time = matvec - near field (the near field runs after the far field); GEMM rate "
+                    "over the serialised M->X and X->L stage times, which also hold the translations; TF32 "
+                    "peak = half the measured bf16 burst",
+        },
+    }
+
+
 def cpu_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -581,6 +632,7 @@ def _run_ours(args, world, rank, local, dist):
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": APPLY_TRAFFIC.get(args.workload),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                      "algorithmic_bytes_per_launch": int(alg_bytes), "launch_ms": near_ms},
+        "roofline_matvec": matvec_roofline(inf, bp.num_patches, t_max / args.steps, near_ms, ms, hbm, peaks),
         "stage_ms": {k: round(float(v), 5) for k, v in zip(
             ["near+add", "p2m", "m2m", "m2x", "x2l", "l2p_prep", "l2l", "l2p_eval"], ms)},
         "fp64_matvec_per_s": value64,
@@ -598,6 +650,8 @@ def _run_ours(args, world, rank, local, dist):
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"], parity = cpu_baseline_and_parity(bp, bp64)
         line.update(parity)
+    if rank == 0 and world == 1 and not args.no_scan and args.workload == "star":
+        line["scan_config_b"] = scan_child(local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     bp.close()
@@ -625,6 +679,7 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-scan", action="store_true", help="leave out the config-B scan key of the default line")
     ap.add_argument("--exact-cubes", action="store_true",
                     help="scan: each pose's exact bounding cube (no far-field plan sharing)")
     ap.add_argument("--prepare-inputs", metavar="NPZ", help=argparse.SUPPRESS)

@@ -168,6 +168,11 @@ typedef struct {
   double fmm_setup_ms;       /* host wall time of the far-field set-up (tables, operators, schedule) */
   double setup_ms;           /* host wall time from the tree build to a problem ready to run */
   int64_t n_scenarios;       /* independent scenarios (bp_problem_create_batch), else 1 */
+  /* work of one far-field pass (0 without FMM): columns (node, channel) of
+   * the multipole->plane-wave and plane-wave->local operators, plane-wave
+   * translation entries (each over 12 channels), columns of the M2M / L2L
+   * shifts, plane waves per direction and coefficients per channel */
+  int64_t fmm_m2x_cols, fmm_x2l_cols, fmm_translations, fmm_shift_cols, fmm_plane_waves, fmm_coefficients;
 } bp_problem_info;
 
 /* Builds the adaptive octree, the singular self-patch integrals and the
