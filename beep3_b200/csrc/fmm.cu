@@ -252,6 +252,17 @@ struct P2mItem {
 constexpr int kP2mChunk = 32;
 
 // basis[(pos + p) * 2 + g][e] for patch p of the item, group g
+// Programmatic dependent launch (PTX griddepcontrol.wait): a kernel of the
+// far-field chains launched as a programmatic dependent starts as the
+// previous kernel on its stream retires its CTAs and waits here until that
+// grid has completed and its writes are visible.  It touches no memory
+// before the wait, so every read and write keeps its order; launched
+// without the attribute the instruction does nothing.  (Releasing the
+// dependents at kernel start as well, griddepcontrol.launch_dependents, was
+// measured slower: 0.484 against 0.447 ms a matvec -- their waiting CTAs
+// hold SM slots the concurrent level streams need.)
+__device__ __forceinline__ void pdl_begin() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename T>
 __global__ void __launch_bounds__(64) p2m_basis_kernel(const __grid_constant__ Tables<T> tb,
                                                        const P2mItem* __restrict__ items,
@@ -303,6 +314,7 @@ __global__ void __launch_bounds__(128) p2m_kernel(const P2mItem* __restrict__ it
                                                   const double* __restrict__ x, int n,
                                                   const typename C2T<T>::type* __restrict__ basis,
                                                   typename C2T<T>::type* __restrict__ M) {
+  pdl_begin();
   using C = typename C2T<T>::type;
   __shared__ T q[kP2mChunk][kCh];
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -627,6 +639,7 @@ __global__ void __launch_bounds__(kXlDirThreads, 2) xl_translate_kernel(const __
                                                                         const XlEntry* __restrict__ entries,
                                                                         const typename C2T<T>::type* __restrict__ W,
                                                                         typename C2T<T>::type* __restrict__ ACC) {
+  pdl_begin();
   using C = typename C2T<T>::type;
   constexpr int CB = kXlChannels;
   constexpr int U = kXlUnroll;  // entries in flight per thread (measured: 2 beats 4, 6 and 8 spill)
@@ -1090,6 +1103,7 @@ __global__ void __launch_bounds__(kEvalThreads) l2p_eval_kernel(int nt, const Le
                                                                 const typename C2T<T>::type* __restrict__ D,
                                                                 const typename C2T<T>::type* __restrict__ Q, int n,
                                                                 double* __restrict__ y) {
+  pdl_begin();
   using C = typename C2T<T>::type;
   extern __shared__ unsigned char smem_raw[];
   const int EQ = (nt + 3) * (nt + 4) / 2, EF = (nt + 2) * (nt + 3) / 2;
@@ -1237,6 +1251,7 @@ __global__ void __launch_bounds__(kGemmThreads) shift_gemm_kernel(int E, const S
                                                                   const ShiftCol* __restrict__ cols,
                                                                   const T* __restrict__ ops,
                                                                   const T* __restrict__ X, T* __restrict__ Y) {
+  pdl_begin();
   const int R = 2 * E, RP = (R + 3) & ~3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* As = reinterpret_cast<T*>(smem_raw);  // [R][RP]
@@ -1334,6 +1349,7 @@ __global__ void __launch_bounds__(kOpThreads) op_gemm_kernel(const GemmTile* __r
                                                              const T* __restrict__ ops, int K, int RP, int R,
                                                              int seg, long long seg_stride,
                                                              const T* __restrict__ X, T* __restrict__ Y) {
+  pdl_begin();
   constexpr int KC = OpChunk<T>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* As = reinterpret_cast<T*>(smem_raw);  // [2][KC][kOpRows]
@@ -1504,6 +1520,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
     const GemmTile* __restrict__ tiles, const GemmCol* __restrict__ cols, const float* __restrict__ packed,
     int n_mtiles, int n_chunks, int K, int R, int seg, long long seg_stride, const float* __restrict__ X,
     float* __restrict__ Y, int* __restrict__ status) {
+  pdl_begin();
   static_assert(NC % 32 == 0 && NC >= 32 && NC <= 256, "tile width");
   constexpr int kXHalf = tc::kKC / 4 * NC * 16;     // bytes of the columns' hi (or lo) part of a chunk
   constexpr int kStageB = 2 * tc::kHalf + 2 * kXHalf;
@@ -1647,6 +1664,7 @@ constexpr int kXlSplit = 2;  // k ranges of the tensor-core wave -> local GEMM (
 // L[ldst[col] + r] = sum over the k-range partials of column col (in order)
 __global__ void __launch_bounds__(256) xl_reduce_kernel(int ncols, int R2, const long long* __restrict__ ldst,
                                                         const float* __restrict__ P, float* __restrict__ L) {
+  pdl_begin();
   const long long total = (long long)ncols * R2;
   for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total; o += (long long)gridDim.x * blockDim.x) {
     const int col = (int)(o / R2), r = (int)(o - (long long)col * R2);
@@ -1661,6 +1679,7 @@ __global__ void __launch_bounds__(256) xl_reduce_kernel(int ncols, int R2, const
 template <typename T>
 __global__ void __launch_bounds__(256) shift_reduce_kernel(int E, const ShiftReduce* __restrict__ items,
                                                            const T* __restrict__ P, T* __restrict__ M) {
+  pdl_begin();
   const int R = 2 * E;
   const ShiftReduce it = items[blockIdx.x];
   for (int o = threadIdx.x; o < kCh * R; o += blockDim.x) {
@@ -1693,6 +1712,7 @@ __global__ void __launch_bounds__(256) prep_csr_kernel(int E, int EQ, const Leaf
                                                        const int* __restrict__ rowptr, const int* __restrict__ cols,
                                                        const T* __restrict__ vals, const T* __restrict__ Lr,
                                                        T* __restrict__ D) {
+  pdl_begin();
   extern __shared__ unsigned char smem_raw[];
   const int R = 2 * E, rows = 8 * 2 * EQ;
   T* x = reinterpret_cast<T*>(smem_raw);  // [12 * R]
@@ -1713,6 +1733,8 @@ struct FmmState {
   // work of one far-field pass: columns (node, channel) of the M->X and
   // wave->local operators, translation entries, M2M / L2L columns
   FmmWork work;
+  // chained far-field kernels launched as programmatic dependents
+  bool pdl = true;
   // buffers a far-field plan shares among problems (see FmmPlan)
   using SharedBuf = std::shared_ptr<DevBuf>;
   SharedBuf tables_buf = std::make_shared<DevBuf>();  // one allocation holding every table
@@ -2626,27 +2648,50 @@ void fmm_setup(Problem& P) {
 // order on one stream.
 // One operator GEMM launch over tiles [first, first + count): tcgen05 for the
 // FP32 engine, the SIMT kernel for the FP64 engine.
+// A kernel launch on stream q; with pdl set, as a programmatic dependent of
+// the kernel launched just before it on q (which it follows with no event
+// wait in between): it may start while that kernel's last CTAs run and
+// waits for it in pdl_begin.
+template <typename... KArgs, typename... Args>
+static void launch_k(bool pdl, void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t q,
+                     Args... args) {
+  if (!pdl) {
+    kernel<<<grid, block, smem, q>>>(args...);
+    BP_LAUNCH_CHECK();
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = q;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BP_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+}
+
 template <typename T>
 static void launch_op_gemm(FmmState& S, int first, int count, const T* simt_ops, const float* tc_ops, int n_mt,
                            int n_ch, int K, int RP, int R, int seg, long long seg_stride, const T* X, T* Y,
-                           cudaStream_t q, int tc_cols) {
+                           cudaStream_t q, int tc_cols, bool pdl) {
   if constexpr (std::is_same<T, float>::value) {
     if (S.tensor) {
       if (tc_cols == tc::kColsM2x)
-        op_gemm_tc_kernel<tc::kColsM2x><<<count, tc::kThreads, tc::smem_bytes(tc::kColsM2x), q>>>(
-            S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride, X,
-            Y, S.tc_status.as<int>());
+        launch_k(pdl, op_gemm_tc_kernel<tc::kColsM2x>, count, tc::kThreads, tc::smem_bytes(tc::kColsM2x), q,
+                 S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride,
+                 X, Y, S.tc_status.as<int>());
       else
-        op_gemm_tc_kernel<tc::kColsXl><<<count, tc::kThreads, tc::smem_bytes(tc::kColsXl), q>>>(
-            S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride, X,
-            Y, S.tc_status.as<int>());
-      BP_LAUNCH_CHECK();
+        launch_k(pdl, op_gemm_tc_kernel<tc::kColsXl>, count, tc::kThreads, tc::smem_bytes(tc::kColsXl), q,
+                 S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(), tc_ops, n_mt, n_ch, K, R, seg, seg_stride,
+                 X, Y, S.tc_status.as<int>());
       return;
     }
   }
-  op_gemm_kernel<T><<<count, kOpThreads, S.smem_op, q>>>(S.op_tiles.as<GemmTile>() + first, S.op_cols.as<GemmCol>(),
-                                                          simt_ops, K, RP, R, seg, seg_stride, X, Y);
-  BP_LAUNCH_CHECK();
+  launch_k(pdl, op_gemm_kernel<T>, count, kOpThreads, S.smem_op, q, S.op_tiles.as<GemmTile>() + first,
+           S.op_cols.as<GemmCol>(), simt_ops, K, RP, R, seg, seg_stride, X, Y);
 }
 
 template <typename T>
@@ -2670,36 +2715,40 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   auto has_x = [&](int lev) { return S.m2x_tcount[lev] > 0 || S.xlt_count[lev] > 0; };
   // multipole -> plane waves, translations, accumulated waves -> locals of
   // one level on stream q
+  // programmatic dependent launches only inside a chain of kernels on one
+  // stream: not for the first kernel after an event wait, and not when the
+  // stages are timed one by one
+  const bool pdl_ok = overlap && S.pdl;
   auto level_x = [&](int lev, cudaStream_t q) {
+    bool chained = false;  // the previous operation on q is a kernel of this chain
     if (S.m2x_tcount[lev]) {
       begin(3, q);
       launch_op_gemm<T>(S, S.m2x_tfirst[lev], S.m2x_tcount[lev], S.m2x_ops->as<T>(), S.m2x_tc->as<float>(), S.m2x_mt,
                         S.m2x_nc, R2, S.m2x_rp, KW, 2 * NPM, (long long)kCh * 2 * NPM,
-                        reinterpret_cast<const T*>(M), reinterpret_cast<T*>(W), q, tc::kColsM2x);
+                        reinterpret_cast<const T*>(M), reinterpret_cast<T*>(W), q, tc::kColsM2x, false);
       end(1);
+      chained = true;
     }
     if (S.xlt_count[lev]) {
       begin(4, q);
       const int nb = S.xlt_count[lev] * (kCh / kXlChannels);
-      xl_translate_kernel<T><<<nb, kXlDirThreads, 0, q>>>(tb, lev - 1, S.xl_targets.as<XlTarget>() + S.xlt_first[lev],
-                                                      S.xlt_count[lev], S.xl_entries.as<XlEntry>(), W,
-                                                      S.acc.as<C>());
-      BP_LAUNCH_CHECK();
+      launch_k(pdl_ok && chained, xl_translate_kernel<T>, nb, kXlDirThreads, 0, q, tb, lev - 1,
+               S.xl_targets.as<XlTarget>() + S.xlt_first[lev], S.xlt_count[lev], S.xl_entries.as<XlEntry>(),
+               (const C*)W, S.acc.as<C>());
       if (S.tensor) {  // k-range partials, then their fixed-order sum into L
         launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops->as<T>(), S.xl_tc->as<float>(), S.xl_mt,
                           S.xl_nc, KW, S.xl_rp, R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()),
-                          reinterpret_cast<T*>(S.xl_partials.as<float>()), q, tc::kColsXl);
+                          reinterpret_cast<T*>(S.xl_partials.as<float>()), q, tc::kColsXl, pdl_ok);
         const long long total = (long long)S.xlr_count[lev] * R2;
         const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 8);
-        xl_reduce_kernel<<<grid, 256, 0, q>>>(S.xlr_count[lev], R2, S.xl_ldst.as<long long>() + S.xlr_first[lev],
-                                              S.xl_partials.as<float>() + S.xlr_pbase[lev],
-                                              reinterpret_cast<float*>(Lx));
-        BP_LAUNCH_CHECK();
+        launch_k(pdl_ok, xl_reduce_kernel, grid, 256, 0, q, S.xlr_count[lev], R2,
+                 S.xl_ldst.as<long long>() + S.xlr_first[lev], (const float*)(S.xl_partials.as<float>() + S.xlr_pbase[lev]),
+                 reinterpret_cast<float*>(Lx));
         end(3);
       } else {
         launch_op_gemm<T>(S, S.xlc_tfirst[lev], S.xlc_tcount[lev], S.xl_ops->as<T>(), S.xl_tc->as<float>(), S.xl_mt,
                           S.xl_nc, KW, S.xl_rp, R2, R2, 0LL, reinterpret_cast<const T*>(S.acc.as<C>()),
-                          reinterpret_cast<T*>(Lx), q, tc::kColsXl);
+                          reinterpret_cast<T*>(Lx), q, tc::kColsXl, pdl_ok);
         end(2);
       }
     }
@@ -2731,20 +2780,20 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   end(l_p2m);
   T* Mr = reinterpret_cast<T*>(M);
   T* Pr = S.m2m_partials.as<T>();
+  bool chained = l_p2m > 0;  // the previous operation on s is a kernel of this chain
   for (int lev = nlev - 1; lev >= 0; --lev) {
     // multipoles of level lev are complete once its children's are shifted in
     if (lev + 1 < nlev && S.m2m_tcount[lev + 1]) {
       begin(2, s);
-      shift_gemm_kernel<T><<<S.m2m_tcount[lev + 1], kGemmThreads, S.smem_gemm, s>>>(
-          S.E, S.shift_tiles.as<ShiftTile>() + S.m2m_tfirst[lev + 1], S.shift_cols.as<ShiftCol>(),
-          S.shift_ops->as<T>(), Mr, Pr);
-      BP_LAUNCH_CHECK();
-      shift_reduce_kernel<T><<<S.m2m_rcount[lev + 1], 256, 0, s>>>(
-          S.E, S.m2m_reduce.as<ShiftReduce>() + S.m2m_rfirst[lev + 1], Pr, Mr);
-      BP_LAUNCH_CHECK();
+      launch_k(pdl_ok && chained, shift_gemm_kernel<T>, S.m2m_tcount[lev + 1], kGemmThreads, S.smem_gemm, s, S.E,
+               (const ShiftTile*)(S.shift_tiles.as<ShiftTile>() + S.m2m_tfirst[lev + 1]),
+               (const ShiftCol*)S.shift_cols.as<ShiftCol>(), (const T*)S.shift_ops->as<T>(), (const T*)Mr, Pr);
+      launch_k(pdl_ok, shift_reduce_kernel<T>, S.m2m_rcount[lev + 1], 256, 0, s, S.E,
+               (const ShiftReduce*)(S.m2m_reduce.as<ShiftReduce>() + S.m2m_rfirst[lev + 1]), (const T*)Pr, Mr);
       end(2);
+      chained = true;
     }
-    fork_x(lev);
+    fork_x(lev);  // an event record on s: later kernels on s still follow a kernel
   }
   // downward pass: locals of level lev + 1 = X2L result (+) L2L of level lev
   for (int lev = 0; lev < nlev - 1; ++lev) {
@@ -2770,10 +2819,9 @@ static void run_fmm(Problem& P, FmmState& S, const Tables<T>& tb, const double* 
   }
   end(1);
   begin(7, s);
-  l2p_eval_kernel<T><<<S.n_eval, kEvalThreads, S.smem_eval, s>>>(S.nt, S.eval_items.as<LeafItem>(), contents,
-                                                                P.d_normal.as<double>(), S.leaf_exp.as<C>(),
-                                                                S.eval_basis.as<C>(), P.n, y);
-  BP_LAUNCH_CHECK();
+  launch_k(pdl_ok, l2p_eval_kernel<T>, S.n_eval, kEvalThreads, S.smem_eval, s, S.nt,
+           (const LeafItem*)S.eval_items.as<LeafItem>(), contents, (const double*)P.d_normal.as<double>(),
+           (const C*)S.leaf_exp.as<C>(), (const C*)S.eval_basis.as<C>(), P.n, y);
   end(1);
 }
 
