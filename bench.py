@@ -212,20 +212,33 @@ def stage_profile(bp, x, y, reps: int = 5):
     return ms, launches
 
 
-def scan_child(local: int) -> dict:
-    """Config B's batched rigid-body scan (64 poses of the two star
-    molecules, 2 workers x 8 poses per batch problem) in a child process on
-    the same GPU: its poses/s line, or the reason it has none."""
-    cmd = [sys.executable, str(Path(__file__).resolve()), "--workload", "scan", "--workers", "2", "--batch", "8"]
+def child_line(local: int, args: list, keys: tuple) -> dict:
+    """One bench mode run in a child process on the same GPU: the chosen
+    keys of its JSON line, or the reason it has none."""
+    cmd = [sys.executable, str(Path(__file__).resolve())] + args
     env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
     for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT"):
         env.pop(k, None)
     try:
         out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
         d = json.loads(out.stdout.strip().splitlines()[-1])
-        return {k: d[k] for k in ("value", "unit", "seconds", "mean_iterations", "config") if k in d}
+        return {k: d[k] for k in keys if k in d}
     except Exception as e:  # the headline line stands without it
         return {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+
+
+def scan_child(local: int) -> dict:
+    """Config B's batched rigid-body scan (64 poses of the two star
+    molecules, 2 workers x 8 poses per batch problem)."""
+    return child_line(local, ["--workload", "scan", "--workers", "2", "--batch", "8"],
+                      ("value", "unit", "seconds", "mean_iterations", "config"))
+
+
+def serve_child(local: int) -> dict:
+    """Config R's served request stream (Poisson arrivals, 2562-163842
+    patches, admission by HBM budget)."""
+    return child_line(local, ["--workload", "serve"],
+                      ("value", "unit", "latency_ms", "seconds", "requests", "config"))
 
 
 def matvec_roofline(inf, n, mv_ms, near_ms, stage_ms, hbm, peaks):
@@ -652,6 +665,7 @@ def _run_ours(args, world, rank, local, dist):
         line.update(parity)
     if rank == 0 and world == 1 and not args.no_scan and args.workload == "star":
         line["scan_config_b"] = scan_child(local)
+        line["serve_config_r"] = serve_child(local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     bp.close()
@@ -679,7 +693,8 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-scan", action="store_true", help="leave out the config-B scan key of the default line")
+    ap.add_argument("--no-scan", action="store_true",
+                    help="leave out the config-B scan and config-R serving keys of the default line")
     ap.add_argument("--exact-cubes", action="store_true",
                     help="scan: each pose's exact bounding cube (no far-field plan sharing)")
     ap.add_argument("--prepare-inputs", metavar="NPZ", help=argparse.SUPPRESS)
