@@ -43,10 +43,10 @@ def scenarios(meshes, precision, ctx, n=3, lone_sphere=False, **kw):
     return out
 
 
-def own_problem(scen, centre, edge, precision, ctx, **kw):
-    bp = b.BEEP(kappa=0.1, nbsize=100, precision=precision, context=ctx, **kw)
+def own_problem(scen, centre, edge, precision, ctx, kappa=0.1, **kw):
+    bp = b.BEEP(kappa=kappa, nbsize=100, precision=precision, context=ctx, **kw)
     for inst in scen.instances:
-        bp.insert_mesh_instance(inst.mesh, offset=inst.offset, rotation=inst.rotation, eps_protein=2.0)
+        bp.insert_mesh_instance(inst.mesh, offset=inst.offset, rotation=inst.rotation, eps_protein=inst.eps_protein)
     bp.set_bounding_cube(centre, edge)
     return bp
 
@@ -103,3 +103,61 @@ def test_batched_scan_matches_unbatched(meshes):
     bat = b.scan.rigid_body_scan(ma, mb, poses, kappa=0.1, nbsize=100, workers=2, batch=4)
     np.testing.assert_allclose(bat.complex_energies, one.complex_energies, rtol=2e-4)
     assert abs(bat.e_a - one.e_a) < 1e-9 * abs(one.e_a)
+
+
+def test_many_scenarios_with_restarts():
+    """24 one-sphere scenarios of different sizes, charges and permittivities, solved with
+    restarted GMRES (cycles of 4 steps): more scenarios than the dot-product
+    blocks of a single problem's solve are split into, and scenarios that
+    converge in an early cycle sit out the later ones.  Each matches its own
+    problem's restarted solve."""
+    ctx = b.EngineContext(0)
+    scen = []
+    for k in range(24):
+        V, T = b.icosphere(2 + k % 2, 8.0 + k)
+        bp = b.BEEP(kappa=0.1, nbsize=100, precision="fp64", context=ctx)
+        bp.insert_mesh_instance(b.Mesh(V, T, b.charges_in_sphere(3 + k, 5.0 + 0.5 * k, seed=500 + k)),
+                                offset=(40.0 * k, 0.0, 0.0), eps_protein=2.0 + 0.1 * k)
+        scen.append(bp)
+    batch = b.ScenarioBatch(scen, context=ctx)
+    assert batch.info().n_scenarios == 24
+    sol = batch.solve(1e-8, 200, restart=4)
+    assert all(sol.converged)
+    energies = batch.calculate_energies()
+    its = []
+    for k, s in enumerate(scen):
+        own = own_problem(s, batch.centres[k], batch.cube_edge, "fp64", ctx)
+        info = own.solve(1e-8, 200, restart=4)
+        e, _ = own.calculate_energies()
+        its.append(info.num_iterations)
+        assert info.num_iterations == sol.iterations[k]
+        assert abs(energies[k][0] - e) < 1e-9 * abs(e)
+        own.close()
+    assert len(set(its)) > 1  # the scenarios stop at different steps
+    batch.close()
+    ctx.close()
+
+
+def test_batch_iteration_limit_reports_per_scenario():
+    """A step limit below what the complexes need: bp_solve_batch returns
+    BP_ERR_NOT_CONVERGED and per-scenario residuals above the tolerance."""
+    import ctypes as C
+    from beep3_b200 import _native as N
+    V, T, shape = b.star_surface(3, 15.0, seed=520)
+    m = b.Mesh(V, T, b.charges_in_star(20, shape, seed=521))
+    ctx = b.EngineContext(0)
+    scen = []
+    for k in range(3):
+        bp = b.BEEP(kappa=0.1, nbsize=100, context=ctx)
+        bp.insert_mesh_instance(m, offset=(60.0 * k, 0.0, 0.0), eps_protein=2.0)
+        scen.append(bp)
+    batch = b.ScenarioBatch(scen, context=ctx)
+    rhs = batch.set_rhs()
+    x = np.zeros_like(rhs)
+    its = np.zeros(3, np.int32)
+    rr = np.zeros(3)
+    code = N.lib().bp_solve_batch(batch.build(), N.ptr(rhs), N.ptr(x), 1e-12, 2, 0, N.ptr(its), N.ptr(rr))
+    assert code == N.BP_ERR_NOT_CONVERGED
+    assert list(its) == [2, 2, 2] and np.all(rr > 1e-12)
+    batch.close()
+    ctx.close()
