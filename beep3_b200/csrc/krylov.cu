@@ -71,6 +71,27 @@ __device__ __forceinline__ int64_t seg_at(Seg sg, int64_t N, int64_t i) {
   return i < sg.n ? sg.a + i : N + sg.a + (i - sg.n);
 }
 
+// Programmatic dependent launch (PTX griddepcontrol.wait): a kernel of the
+// Arnoldi step launched as a programmatic dependent starts as the previous
+// kernel on the stream retires its CTAs and waits here for that grid's
+// completion and writes; it touches no memory before the wait.  Launched
+// without the attribute the instruction does nothing.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+void launch_dependent(void (*kernel)(KArgs...), dim3 grid, unsigned block, cudaStream_t q, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(block);
+  cfg.stream = q;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BP_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+}
+
 // fixed-order block sum; the total is valid in thread 0
 __device__ __forceinline__ double block_sum(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -199,6 +220,7 @@ __global__ void arnoldi_load(double* __restrict__ V, int64_t len, const Seg* __r
 __global__ void arnoldi_dots(const double* __restrict__ V, int64_t len, const double* __restrict__ w,
                              const Seg* __restrict__ seg, const KrylovCtl* __restrict__ ctl, int m,
                              double* __restrict__ partial) {
+  pdl_wait();
   const int sc = blockIdx.y;
   if (!ctl[sc].cont) return;
   const Seg sg = seg[sc];
@@ -222,6 +244,7 @@ __global__ void arnoldi_dots(const double* __restrict__ V, int64_t len, const do
 // U_s[j(j+1)/2 + k] = sum_b partial_s[k * nbs + b] (fixed order), block k <= j
 __global__ void arnoldi_reduce(const double* __restrict__ partial, int nbs, const KrylovCtl* __restrict__ ctl, int m,
                                double* __restrict__ U0, int64_t ks) {
+  pdl_wait();
   const int k = blockIdx.x, sc = blockIdx.y;
   if (!ctl[sc].cont) return;
   const int j = ctl[sc].j;
@@ -240,6 +263,7 @@ __global__ void arnoldi_reduce(const double* __restrict__ partial, int nbs, cons
 __global__ void arnoldi_orth(double* __restrict__ V, int64_t len, const double* __restrict__ w,
                              const double* __restrict__ U0, int64_t ks, const Seg* __restrict__ seg,
                              const KrylovCtl* __restrict__ ctl, int m, double* __restrict__ partial) {
+  pdl_wait();
   const int sc = blockIdx.y;
   if (!ctl[sc].cont) return;
   const Seg sg = seg[sc];
@@ -270,6 +294,7 @@ __global__ void arnoldi_orth(double* __restrict__ V, int64_t len, const double* 
 __global__ void arnoldi_finish(const double* __restrict__ partial, int nbs, int m, double* __restrict__ U0,
                                int64_t ks, KrylovCtl* __restrict__ ctl, cudaGraphConditionalHandle handle,
                                int use_handle) {
+  pdl_wait();
   const int sc = blockIdx.x;
   if (!ctl[sc].cont) return;
   const double* part = partial + (int64_t)sc * (m + 1) * nbs;
@@ -312,6 +337,7 @@ __global__ void arnoldi_finish(const double* __restrict__ partial, int nbs, int 
 // all->any = some scenario goes on; drives the WHILE node of a batch
 __global__ void any_continue(const KrylovCtl* __restrict__ ctl, int n_scen, KrylovAll* __restrict__ all,
                              cudaGraphConditionalHandle handle, int use_handle) {
+  pdl_wait();
   int any = 0;
   for (int sc = threadIdx.x; sc < n_scen; sc += blockDim.x) any |= ctl[sc].cont;
   any = __syncthreads_or(any);
@@ -543,12 +569,18 @@ void arnoldi_step_launches(Problem& P, int m, cudaStream_t st, cudaGraphConditio
   arnoldi_load<<<dim3(kv.gx, S), kThreads, 0, st>>>(V, len, seg, kv.ctl, gx);
   BP_LAUNCH_CHECK();
   matvec_launches(P, gx, gy, st, P.side, nullptr);
-  arnoldi_dots<<<dim3(kv.nbs, S), kThreads, 0, st>>>(V, len, gy, seg, kv.ctl, m, kv.partial);
-  arnoldi_reduce<<<dim3(m, S), kThreads, 0, st>>>(kv.partial, kv.nbs, kv.ctl, m, kv.U0, kv.ks);
-  arnoldi_orth<<<dim3(kv.nbs, S), kThreads, 0, st>>>(V, len, gy, kv.U0, kv.ks, seg, kv.ctl, m, kv.partial);
-  arnoldi_finish<<<S, kThreads, 0, st>>>(kv.partial, kv.nbs, m, kv.U0, kv.ks, kv.ctl, handle, use_handle);
-  if (S > 1) any_continue<<<1, kThreads, 0, st>>>(kv.ctl, S, kv.all, handle, use_handle);
-  BP_LAUNCH_CHECK();
+  // the dot products follow the near-field kernel on st; the rest of the
+  // step is a chain of dependent launches
+  launch_dependent(arnoldi_dots, dim3(kv.nbs, S), kThreads, st, (const double*)V, len, (const double*)gy, seg,
+                   (const KrylovCtl*)kv.ctl, m, kv.partial);
+  launch_dependent(arnoldi_reduce, dim3(m, S), kThreads, st, (const double*)kv.partial, kv.nbs,
+                   (const KrylovCtl*)kv.ctl, m, kv.U0, kv.ks);
+  launch_dependent(arnoldi_orth, dim3(kv.nbs, S), kThreads, st, V, len, (const double*)gy, (const double*)kv.U0,
+                   kv.ks, seg, (const KrylovCtl*)kv.ctl, m, kv.partial);
+  launch_dependent(arnoldi_finish, dim3(S), kThreads, st, (const double*)kv.partial, kv.nbs, m, kv.U0, kv.ks, kv.ctl,
+                   handle, use_handle);
+  if (S > 1)
+    launch_dependent(any_continue, dim3(1), kThreads, st, (const KrylovCtl*)kv.ctl, S, kv.all, handle, use_handle);
 }
 
 // The Arnoldi loop of one cycle as a graph: a WHILE node (condition 1 at
