@@ -764,6 +764,15 @@ void nf_assemble(Problem& P) {
     rows_per_item /= 2;
     nf.h_items = make_items(P, rows_per_item);
   }
+  // largest items (rows x neighbourhood columns) first: the persistent grid
+  // starts the long ones early instead of ending on them (measured: the
+  // apply 0.170 against 0.179 ms on the 40962-patch star).  Every item
+  // writes its own rows, so the order changes no result.
+  std::stable_sort(nf.h_items.begin(), nf.h_items.end(), [&](const NfItem& a, const NfItem& b) {
+    const long long wa = (long long)a.row_count * (nf.h_col_off[a.leaf + 1] - nf.h_col_off[a.leaf]);
+    const long long wb = (long long)b.row_count * (nf.h_col_off[b.leaf + 1] - nf.h_col_off[b.leaf]);
+    return wa > wb;
+  });
   nf.items = upload(ctx, nf.h_items);
   nf.n_items = (int)nf.h_items.size();
 }
