@@ -37,7 +37,7 @@ L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one near-field
 # apply launch, measured with ncu on each workload (a one-pass capture of the
 # same bench command; 976.9 MB of them are algorithmic on the star workload)
-APPLY_TRAFFIC = {"star": 984_270_000}
+APPLY_TRAFFIC = {"star": 983_633_408}
 
 
 def workload(name: str):
