@@ -1659,7 +1659,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) op_gemm_tc_kernel(
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NC));
 }
 
-constexpr int kXlSplit = 2;  // k ranges of the tensor-core wave -> local GEMM (measured: 2 beats 3 and 4)
+constexpr int kXlSplit = 2;  // k ranges of the tensor-core wave -> local GEMM (measured: 2 beats 1, 3 and 4)
 
 // L[ldst[col] + r] = sum over the k-range partials of column col (in order)
 __global__ void __launch_bounds__(256) xl_reduce_kernel(int ncols, int R2, const long long* __restrict__ ldst,
