@@ -63,6 +63,13 @@ def workload(name: str):
                              "kappa 0.1, qual 4 / quad 0, FMM order 9, reference tree nbsize 1500 "
                              "(profiling case)", patches=10242)
         return desc, [(mesh, None, (1, 0, 0, 0))], 0.1, 1500
+    if name == "star-large":
+        V, T, shape = b.star_surface(7, 40.0, seed=1237)
+        mesh = b.Mesh(V, T, b.charges_in_star(20000, shape, seed=1238))
+        desc = dict(workload="star-shaped molecule R=40 A, icosphere k=7 (163842 patches), 20000 charges, "
+                             "eps 2/80, kappa 0.125, qual 4 / quad 0, FMM order 9, reference tree nbsize 1500 "
+                             "(config P's size)", patches=163842)
+        return desc, [(mesh, None, (1, 0, 0, 0))], 0.125, 1500
     raise ValueError(f"unknown workload {name}")
 
 
@@ -747,7 +754,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="star", choices=["kirkwood", "star", "star-small", "scan", "serve"],
+    ap.add_argument("--workload", default="star",
+                    choices=["kirkwood", "star", "star-small", "star-large", "scan", "serve"],
                     help="scan / serve: the batched rigid-body scan and the served request stream")
     ap.add_argument("--poses", type=int, default=64, help="scan: number of poses")
     ap.add_argument("--autotune", action="store_true",
