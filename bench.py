@@ -729,7 +729,7 @@ def _run_ours(args, world, rank, local, dist):
                               "rel_err_mixed_vs_fp64": abs(e_mixed - e_fp64) / abs(e_fp64)},
         "clocks": clocks,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the CPU baseline: rank 0 at N = 1 only
         line["cpu_baseline"], parity = cpu_baseline_and_parity(bp, bp64)
         line.update(parity)
     if rank == 0 and world == 1 and not args.no_scan and args.workload == "star":
