@@ -714,6 +714,8 @@ def _run_ours(args, world, rank, local, dist):
         "stage_ms": {k: round(float(v), 5) for k, v in zip(
             ["near+add", "p2m", "m2m", "m2x", "x2l", "l2p_prep", "l2l", "l2p_eval"], ms)},
         "fp64_matvec_per_s": value64,
+        "fp64_stage_ms": {k: round(float(v), 5) for k, v in zip(
+            ["near+add", "p2m", "m2m", "m2x", "x2l", "l2p_prep", "l2l", "l2p_eval"], stage_profile(bp64, x, y)[0])},
         "mixed_over_fp64": value / value64,
         "solves_per_s": world * 1e3 / statistics.median(solve_ms),
         "fp64_solves_per_s": world * 1e3 / statistics.median(solve64_ms),
