@@ -264,7 +264,7 @@ def child_line(local: int, args: list, keys: tuple) -> dict:
     for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT"):
         env.pop(k, None)
     try:
-        out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=300, env=env)
         d = json.loads(out.stdout.strip().splitlines()[-1])
         return {k: d[k] for k in keys if k in d}
     except Exception as e:  # the headline line stands without it
