@@ -62,3 +62,33 @@ def test_posed_rhs_entry_point_validates():
     assert L.bp_rhs_posed(None, C.cast(ptrs, C.c_void_p), C.cast(counts, C.c_void_p), 80.0,
                           N.ptr(rhs)) == N.BP_ERR_INVALID
     assert b"bad argument" in L.bp_last_error()
+
+
+def test_batch_entry_points_validate_arguments():
+    """bp_problem_create_batch and bp_solve_batch reject bad arguments before
+    any device work (no GPU needed)."""
+    L = N.lib()
+    h = C.c_void_p()
+    prm = N.bp_params(0.1, 1e-10, (C.c_double * 3)(0, 0, 0), 50.0, 100, 9, N.BP_PREC_MIXED, 0)
+    centres = np.zeros(6)
+    insts = (N.bp_instance * 2)()
+    bad_first = np.array([0, 2, 2], np.int32)  # the second scenario has no instance
+    assert L.bp_problem_create_batch(None, insts, 2, N.ptr(bad_first), 2, N.ptr(centres), C.byref(prm),
+                                     C.byref(h)) == N.BP_ERR_INVALID
+    assert b"every scenario needs an instance" in L.bp_last_error()
+    short = np.array([0, 1, 1], np.int32)  # does not end at n_instances
+    assert L.bp_problem_create_batch(None, insts, 3, N.ptr(short), 2, N.ptr(centres), C.byref(prm),
+                                     C.byref(h)) == N.BP_ERR_INVALID
+    assert b"scenario_first" in L.bp_last_error()
+    nan_centres = np.array([0.0, np.nan, 0.0, 0.0, 0.0, 0.0])
+    ok_first = np.array([0, 1, 2], np.int32)
+    assert L.bp_problem_create_batch(None, insts, 2, N.ptr(ok_first), 2, N.ptr(nan_centres), C.byref(prm),
+                                     C.byref(h)) == N.BP_ERR_INVALID
+    assert L.bp_problem_create_batch(None, insts, 2, N.ptr(ok_first), 2, N.ptr(centres), C.byref(prm),
+                                     C.byref(h)) == N.BP_ERR_INVALID  # no context
+    rhs = np.zeros(4)
+    x = np.zeros(4)
+    assert L.bp_solve_batch(None, N.ptr(rhs), N.ptr(x), 1e-6, 10, 0, None, None) == N.BP_ERR_INVALID
+    its = np.zeros(2, np.int32)
+    rr = np.zeros(2)
+    assert L.bp_solve_batch(None, N.ptr(rhs), N.ptr(x), 1e-6, 10, 0, N.ptr(its), N.ptr(rr)) == N.BP_ERR_INVALID
