@@ -685,11 +685,16 @@ BP_API int32_t bp_matvec(bp_problem p, const double* x, double* y) {
     DeviceGuard g(P->ctx->device);
     const size_t bytes = sizeof(double) * 2 * (size_t)P->n;
     cudaStream_t st = P->ctx->stream;
-    BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
-    matvec_device(*P, P->d_x.as<double>(), P->d_y.as<double>());
-    BP_CUDA(cudaMemcpyAsync(y, P->d_y.get(), bytes, cudaMemcpyDeviceToHost, st));
+    // straight into and out of the matvec graph's own buffers, and the
+    // far field's timeout word read back behind y: one synchronisation
+    BP_CUDA(cudaMemcpyAsync(P->d_gx.get(), x, bytes, cudaMemcpyHostToDevice, st));
+    matvec_device(*P, P->d_gx.as<double>(), P->d_gy.as<double>());
+    BP_CUDA(cudaMemcpyAsync(y, P->d_gy.get(), bytes, cudaMemcpyDeviceToHost, st));
+    int flag = 0;
+    if (const int* sd = fmm_status_dev(*P))
+      BP_CUDA(cudaMemcpyAsync(&flag, sd, sizeof(int), cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
-    fmm_check_waits(*P);
+    fmm_raise_if(*P, flag);
     return BP_OK;
   });
 }
@@ -732,8 +737,11 @@ static int32_t solve_host(bp_problem p, const double* rhs, double* x, double tol
     const bool x0 = std::all_of(x, x + 2 * (size_t)P->n, [](double v) { return v == 0.0; });
     gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, rr.data(), its.data(), x0);
     BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
+    int flag = 0;
+    if (const int* sd = fmm_status_dev(*P))
+      BP_CUDA(cudaMemcpyAsync(&flag, sd, sizeof(int), cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
-    fmm_check_waits(*P);
+    fmm_raise_if(*P, flag);
     const double worst = *std::max_element(rr.begin(), rr.end());
     if (scenario_out) {  // bp_solve_batch: per scenario
       std::copy(its.begin(), its.end(), iterations);

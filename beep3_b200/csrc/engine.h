@@ -469,6 +469,11 @@ FmmWork fmm_work(const Problem& P);
 // a bounded wait since the problem was created (its results are then void).
 // Synchronises the context stream.
 void fmm_check_waits(Problem& P);
+// The same check split in two: the device word to copy back behind the
+// caller's last copy (null without a tensor-core far field), then the
+// value read, raising TimeoutError (and clearing the word) when set.
+const int* fmm_status_dev(Problem& P);
+void fmm_raise_if(Problem& P, int flag);
 // Timeout test switch of the tensor-core FMM kernels (see
 // bp_problem_test_wait_timeout); false when the problem has none.
 bool fmm_set_stall_test(Problem& P, bool on);

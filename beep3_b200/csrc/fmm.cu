@@ -1878,6 +1878,19 @@ void fmm_check_waits(Problem& P) {
   }
 }
 
+const int* fmm_status_dev(Problem& P) {
+  FmmState* S = P.fmm.get();
+  return S && S->tc_status.get() ? S->tc_status.as<int>() : nullptr;
+}
+
+void fmm_raise_if(Problem& P, int flag) {
+  if (!flag) return;
+  FmmState* S = P.fmm.get();
+  BP_CUDA(cudaMemsetAsync(S->tc_status.get(), 0, sizeof(int), P.ctx->stream));
+  BP_CUDA(cudaStreamSynchronize(P.ctx->stream));
+  throw TimeoutError("a tensor-core FMM kernel timed out waiting for its matrix multiplies");
+}
+
 bool fmm_set_stall_test(Problem& P, bool on) {
   FmmState* S = P.fmm.get();
   if (!S || !S->tensor || !S->tc_status.get()) return false;
