@@ -731,10 +731,13 @@ static int32_t solve_host(bp_problem p, const double* rhs, double* x, double tol
     DevBuf& b = P->scratch_b;
     if (b.bytes() < bytes) b.alloc(P->ctx, bytes);
     BP_CUDA(cudaMemcpyAsync(b.get(), rhs, bytes, cudaMemcpyHostToDevice, st));
-    BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
+    const bool x0 = std::all_of(x, x + 2 * (size_t)P->n, [](double v) { return v == 0.0; });
+    if (x0)  // a zero initial guess (the usual one) is set on the device, not copied
+      BP_CUDA(cudaMemsetAsync(P->d_x.get(), 0, bytes, st));
+    else
+      BP_CUDA(cudaMemcpyAsync(P->d_x.get(), x, bytes, cudaMemcpyHostToDevice, st));
     std::vector<double> rr(P->n_scen(), 0.0);
     std::vector<int> its(P->n_scen(), 0);
-    const bool x0 = std::all_of(x, x + 2 * (size_t)P->n, [](double v) { return v == 0.0; });
     gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, rr.data(), its.data(), x0);
     BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
     int flag = 0;
