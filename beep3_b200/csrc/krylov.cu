@@ -14,10 +14,19 @@
 // partials, their sums, orthogonalisation fused with the partials of |w|^2,
 // and the norm + Givens + stop test) plus the matvec, all reading the step
 // index from device memory, so one cycle's whole loop is one CUDA graph: a
-// WHILE conditional node whose body is the step, continued by the last
-// kernel while j < cycle and |y_j| > tol ||b||.  The host waits once per
-// cycle.  Where the conditional graph cannot be built the host launches the
-// same kernels step by step and reads the stop flag after each.
+// WHILE conditional node whose body is the step, continued while j < cycle
+// and |y_j| > tol ||b||.  The kernels after the matvec are programmatic
+// dependent launches.  The host waits once per cycle.  Where the
+// conditional graph cannot be built the host launches the same kernels
+// step by step and reads the stop flag after each.
+//
+// A batch problem runs one GMRES per scenario in the same launches: every
+// kernel takes the scenario from blockIdx.y (or one block per scenario)
+// and works on the scenario's part of the vector, with its own control
+// block, Hessenberg column, Givens rotations and stop test; a scenario that
+// has converged sits out the rest of the steps, and the WHILE node goes on
+// while any scenario does.  A solve from x = 0 starts from r = -b without
+// the first matvec.
 #include <cuda_runtime.h>
 
 #include <algorithm>
