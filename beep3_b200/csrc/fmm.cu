@@ -28,7 +28,11 @@
 //         target contracted with them (FMM_results_to_BEM,
 //         src/bem/bem_kernels.cpp:12-121)
 // M2X + X2L of a level run on the level's own stream as soon as its
-// multipoles exist.  Work that cannot reach a result is not scheduled.
+// multipoles exist; the kernels that follow one another on a stream are
+// programmatic dependent launches.  Work that cannot reach a result is not
+// scheduled.  The mixed engine's two operator GEMMs (M2X, waves -> local)
+// run on the 5th-generation tensor cores (tcgen05, 3xTF32, TMEM
+// accumulators); the FP64 engine's on the SIMT FP64 pipe.
 // Precision: T = double (FP64 engine) or float (mixed engine); tables and
 // operators are computed in FP64 and rounded to T.  Expansions are stored
 // [node][channel][tri(n, m)] as complex T; plane waves
