@@ -80,9 +80,13 @@ def estimate_device_bytes(n_patches: int, nbsize: int, precision: str) -> int:
 class BemServer:
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 64 << 30, workers: int = 4,
                  precision: str = "mixed", nbsize: int = DEFAULT_NBSIZE, restart: int = 0, runner=None,
-                 estimator=None):
+                 estimator=None, tree_for=None):
         """``runner(req, need) -> SolveResult`` and ``estimator(req) -> bytes``
-        default to the engine solve and :func:`estimate_device_bytes`."""
+        default to the engine solve and :func:`estimate_device_bytes`.
+        ``tree_for(n_patches) -> dict`` gives the BEEP tree keywords of a
+        request by its size (for example the device-built tree for the
+        largest ones, whose set-up it halves); by default every request
+        uses the reference tree at ``nbsize``."""
         self.runner = runner or self._engine_solve
         self.estimator = estimator or (lambda r: estimate_device_bytes(r.mesh.n_patches, self.nbsize,
                                                                        self.precision))
@@ -90,6 +94,7 @@ class BemServer:
         self.budget = int(hbm_budget_bytes)
         self.precision = precision
         self.nbsize = nbsize
+        self.tree_for = tree_for or (lambda n: dict(nbsize=self.nbsize))
         self.restart = restart
         self._pending: "queue.Queue[tuple[SolveRequest, Future] | None]" = queue.Queue()
         self._lock = threading.Condition()
@@ -120,7 +125,8 @@ class BemServer:
         self._contexts = []
 
     def _key(self, req: SolveRequest) -> tuple:
-        return (req.mesh.n_patches, self.precision, self.nbsize, req.kappa > 0)
+        tree = tuple(sorted(self.tree_for(req.mesh.n_patches).items()))
+        return (req.mesh.n_patches, self.precision, tree, req.kappa > 0)
 
     def footprint(self, req: SolveRequest) -> int:
         """Device bytes reserved for a request: the largest measured on an
@@ -160,8 +166,8 @@ class BemServer:
             ectx = self._contexts.pop() if self._contexts else None
         if ectx is None:
             ectx = EngineContext(self.device)
-        bp = BEEP(eps_solvent=req.eps_solvent, kappa=req.kappa, nbsize=self.nbsize, precision=self.precision,
-                  context=ectx)
+        bp = BEEP(eps_solvent=req.eps_solvent, kappa=req.kappa, precision=self.precision, context=ectx,
+                  **self.tree_for(req.mesh.n_patches))
         try:
             bp.insert_mesh_instance(req.mesh, eps_protein=req.eps_protein)
             info = bp.solve(req.tol, req.max_iterations, restart=self.restart)

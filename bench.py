@@ -583,7 +583,11 @@ def _serve_mode(args, local):
             k = levels[n_snap]
             v, t, shape = b.star_surface(k, 20.0 * (n_snap / 40962) ** 0.5, seed=5000 + k)
             meshes[n_snap] = b.Mesh(v, t, b.charges_in_star(int(0.05 * n_snap), shape, seed=6000 + k))
-    srv = BemServer(device=local, workers=args.workers)
+    tree_for = None
+    if args.serve_device_tree_from:  # the device-built tree (cap 128) for requests of at least this size
+        cut = args.serve_device_tree_from
+        tree_for = lambda n: dict(tree="device", leaf_size=128) if n >= cut else dict(nbsize=1500)
+    srv = BemServer(device=local, workers=args.workers, tree_for=tree_for)
     try:
         # warm-up: the same stream once, untimed, so that the slots' engine
         # contexts hold the meshes and far-field plans a running server would
@@ -609,7 +613,9 @@ def _serve_mode(args, local):
         "data": "synthetic", "dtype": "fp32 near field/FMM + fp64 singular/GMRES",
         "config": {"workload": "served stream: Poisson arrivals, star surfaces of 2562-163842 patches "
                                "(log-uniform), charges 0.05 x patches, kappa in {0, 0.05, 0.1, 0.15}",
-                   "requests": len(results), "rate_per_s": args.rate, "worker_slots": args.workers},
+                   "requests": len(results), "rate_per_s": args.rate, "worker_slots": args.workers,
+                   "tree": ("device tree, cap 128, from %d patches" % args.serve_device_tree_from
+                            if args.serve_device_tree_from else "reference tree, nbsize 1500")},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max())},
         "all_converged": all(r.converged for r in results),
@@ -773,6 +779,10 @@ def main():
                     help="scan: poses solved together as the scenarios of one batch problem")
     ap.add_argument("--requests", type=int, default=24, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=8.0, help="serve: Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-device-tree-from", type=int, default=100000,
+                    help="serve: requests of at least this many patches use the device-built tree (cap 128), "
+                         "whose set-up is half the reference tree's at 163842 patches; 0: the reference tree "
+                         "for all")
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
