@@ -88,3 +88,23 @@ def test_measured_footprint_replaces_the_estimate():
     srv.submit(SolveRequest(FakeMesh(50), 0.1)).result(timeout=10)  # unseen size: the estimate
     srv.close()
     assert needs == [100, 300, 50]
+
+
+def test_tree_per_request_size_keys_the_measured_footprint():
+    """tree_for picks a request's tree by its size; footprints learnt from
+    measured device bytes are kept per (size, precision, tree, screened)."""
+    def runner(req, need):
+        start = time.perf_counter()
+        return SolveResult(req.tag, 0.0, 1, True, req.mesh.n_patches, 1000 + req.mesh.n_patches, req.arrival,
+                           start, time.perf_counter())
+
+    tree_for = lambda n: dict(tree="device", leaf_size=128) if n >= 100000 else dict(nbsize=1500)
+    srv = BemServer(runner=runner, estimator=lambda r: 10, tree_for=tree_for, workers=2)
+    try:
+        small, large = SolveRequest(FakeMesh(2562), 0.1), SolveRequest(FakeMesh(163842), 0.1)
+        assert dict(srv._key(large)[2])["tree"] == "device" and dict(srv._key(small)[2])["nbsize"] == 1500
+        srv.submit(small).result()
+        srv.submit(large).result()
+        assert srv.footprint(small) == 1000 + 2562 and srv.footprint(large) == 1000 + 163842
+    finally:
+        srv.close()
