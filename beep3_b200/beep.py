@@ -213,7 +213,7 @@ class BEEP:
     def __init__(self, eps_solvent: float = 80.0, kappa: float = 0.1, nbsize: int = DEFAULT_NBSIZE,
                  nterms: int = 9, precision: str = "fp64", device: int = 0, hbm_budget_bytes: int = 0,
                  context: EngineContext | None = None, nearfield_on_demand: bool = False,
-                 tree: str = "reference", leaf_size: int = 64):
+                 tree: str = "reference", leaf_size: int = 64, compact_nearfield: bool = False):
         """``context``: an EngineContext shared with scenarios run before or
         after this one (its device and budget apply); by default the scenario
         has its own.  ``nearfield_on_demand``: recompute the near field in
@@ -222,7 +222,11 @@ class BEEP:
         matvec.  ``tree``: "reference" (the reference's octree rules, driven
         by ``nbsize``) or "device" (built on the GPU from Morton codes, at
         most ``leaf_size`` patches per leaf; same neighbourhood rule, a
-        different near/far split, so results agree to the FMM's accuracy)."""
+        different near/far split, so results agree to the FMM's accuracy).
+        ``compact_nearfield`` (mixed precision only): cache each FP32
+        near-field coefficient rounded to 24 bits, 12 bytes a pair instead of
+        16 (relative error at most 2^-16 per coefficient; no reference
+        counterpart)."""
         self.eps_solvent = float(eps_solvent)
         self.kappa = float(kappa)
         self.nbsize = int(nbsize)
@@ -231,6 +235,9 @@ class BEEP:
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.precision = precision
         self.nearfield_on_demand = bool(nearfield_on_demand)
+        self.compact_nearfield = bool(compact_nearfield)
+        if self.compact_nearfield and (precision != "mixed" or self.nearfield_on_demand):
+            raise ValueError("compact_nearfield needs precision='mixed' and cached coefficients")
         if tree not in ("reference", "device"):
             raise ValueError("tree must be 'reference' or 'device'")
         self.tree_kind = tree
@@ -384,7 +391,8 @@ class BEEP:
             insts[k].offset[:] = [float(v) for v in inst.offset]
             insts[k].dielectric_ratio = inst.dielectric_ratio
         flags = ((N.BP_FLAG_NEARFIELD_ON_DEMAND if self.nearfield_on_demand else 0) |
-                 (N.BP_FLAG_DEVICE_TREE if self.tree_kind == "device" else 0))
+                 (N.BP_FLAG_DEVICE_TREE if self.tree_kind == "device" else 0) |
+                 (N.BP_FLAG_COMPACT_NEARFIELD if self.compact_nearfield else 0))
         prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge,
                           self.leaf_size if self.tree_kind == "device" else self.nbsize, self.nterms,
                           N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED, flags)

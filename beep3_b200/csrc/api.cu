@@ -79,8 +79,12 @@ int32_t check_params(const char* who, const bp_params* prm) {
   if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
     return fail(BP_ERR_INVALID, std::string(who) + ": unknown precision");
   if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, std::string(who) + ": bad kappa");
-  if (prm->flags & ~(BP_FLAG_NEARFIELD_ON_DEMAND | BP_FLAG_DEVICE_TREE))
+  if (prm->flags & ~(BP_FLAG_NEARFIELD_ON_DEMAND | BP_FLAG_DEVICE_TREE | BP_FLAG_COMPACT_NEARFIELD))
     return fail(BP_ERR_INVALID, std::string(who) + ": unknown flags");
+  if ((prm->flags & BP_FLAG_COMPACT_NEARFIELD) &&
+      (prm->precision != BP_PREC_MIXED || (prm->flags & BP_FLAG_NEARFIELD_ON_DEMAND)))
+    return fail(BP_ERR_INVALID,
+                std::string(who) + ": the compact near field needs the mixed engine and cached coefficients");
   if (prm->nbsize <= 0) return fail(BP_ERR_INVALID, std::string(who) + ": nbsize must be positive");
   if (prm->nterms != 9)
     return fail(BP_ERR_UNSUPPORTED, std::string(who) +

@@ -258,6 +258,7 @@ struct NfItem {
 // patches of its 27-box neighbourhood.
 struct NearField {
   bool on_demand = false;  // no cached coefficients: instant_kernel every matvec
+  bool compact = false;    // FP32 coefficients rounded to 24 bits, 12 bytes a pair
   size_t instant_smem = 0;
   int n_leaves = 0;
   int64_t n_pairs = 0;
@@ -265,7 +266,7 @@ struct NearField {
   int max_qual_chunk = 0;
   int max_cols = 0;
   DevBuf rows, row_off, cols, col_off, coef_off, items;
-  DevBuf coef;  // 4 * n_pairs of float or double
+  DevBuf coef;  // 4 * n_pairs of float or double; compact: 2 * n_pairs + n_pairs words
   std::vector<int64_t> h_row_off, h_col_off, h_coef_off;
   std::vector<int32_t> h_rows, h_cols;
   std::vector<NfItem> h_items;

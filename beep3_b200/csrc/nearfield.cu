@@ -63,6 +63,67 @@ __device__ __forceinline__ double4 ld_stream(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+// Compact near field (BP_FLAG_COMPACT_NEARFIELD): each FP32 coefficient
+// rounded to its top 24 bits (sign, exponent and a 15-bit fraction: a 16-bit
+// significand, relative rounding error at most 2^-17) and the four of a pair
+// packed into 12 bytes, kept as two planes of one buffer so that every warp
+// load is contiguous: plane 0 holds (w0, w1) per pair, plane 1 w2, with
+//   w0 = a | b << 24,  w1 = b >> 8 | c << 16,  w2 = c >> 16 | d << 8
+// for the 24-bit values a, b, c, d.
+__device__ __forceinline__ uint32_t round24(float v) {
+  return (__float_as_uint(v) + 0x80u) >> 8;  // to nearest on the magnitude; carries into the exponent
+}
+__device__ __forceinline__ void pack24(float4 v, uint2& w01, uint32_t& w2) {
+  const uint32_t a = round24(v.x), b = round24(v.y), c = round24(v.z), d = round24(v.w);
+  w01.x = a | (b << 24);
+  w01.y = (b >> 8) | (c << 16);
+  w2 = (c >> 16) | (d << 8);
+}
+__device__ __forceinline__ float4 unpack24(uint2 w01, uint32_t w2) {
+  float4 v;
+  v.x = __uint_as_float(w01.x << 8);
+  v.y = __uint_as_float(((w01.x >> 16) & 0xFF00u) | (w01.y << 16));
+  v.z = __uint_as_float(((w01.y >> 8) & 0xFFFF00u) | (w2 << 24));
+  v.w = __uint_as_float(w2 & 0xFFFFFF00u);
+  return v;
+}
+
+// The coefficient quadruple of pair index k: FP32 / FP64 records, or the
+// compact planes: plane 0 holds each pair's first two words (8 bytes), plane
+// 1, starting 2 n_pairs words later, its third word (4 bytes).  A warp's 32
+// consecutive pairs read 256 contiguous bytes of plane 0 and 128 of plane 1
+// (measured: groups of 32 pairs with both parts side by side, 384 bytes a
+// group, split each warp's reads over two groups and ran the apply at 0.183
+// against 0.141 ms on the 40962-patch star).
+template <typename T, bool kCompact>
+struct CoefReader {
+  const typename Vec4<T>::type* rec;
+  __device__ __forceinline__ typename Vec4<T>::type operator()(int64_t k) const { return ld_stream(rec + k); }
+};
+template <>
+struct CoefReader<float, true> {
+  const uint2* p01;
+  const uint32_t* p2;
+  __device__ __forceinline__ float4 operator()(int64_t k) const { return unpack24(__ldcs(p01 + k), __ldcs(p2 + k)); }
+};
+template <typename T, bool kCompact>
+struct CoefWriter {
+  typename Vec4<T>::type* rec;
+  __device__ __forceinline__ void operator()(int64_t k, typename Vec4<T>::type v) const { rec[k] = v; }
+};
+template <>
+struct CoefWriter<float, true> {
+  uint2* p01;
+  uint32_t* p2;
+  __device__ __forceinline__ void operator()(int64_t k, float4 v) const {
+    uint2 w01;
+    uint32_t w2;
+    pack24(v, w01, w2);
+    p01[k] = w01;
+    p2[k] = w2;
+  }
+};
+
 // FP32: the hardware approximations with denormals flushed (PTX
 // rsqrt.approx.ftz / ex2.approx.ftz).  The arguments here are normal
 // numbers (r^2 >= 1e-9 and exponents above -126), where flushing changes
@@ -241,13 +302,13 @@ __device__ __forceinline__ void load_qpoint(const double* s, int q, double (&v)[
 // column, so one row's stores are contiguous across the block.  A column
 // with one quadrature point (quadrature rule 0) keeps it in registers for
 // all of its rows x qualocation points.
-template <typename T>
+template <typename T, bool kCompact>
 __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
     const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
     const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
     const int32_t* __restrict__ qoff, const T* __restrict__ qual, int nq, const int32_t* __restrict__ poff,
     const T* __restrict__ quad, int np, const double* __restrict__ eps, T kappa, const double* __restrict__ diag,
-    T* __restrict__ coef) {
+    const CoefWriter<T, kCompact> out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sq = reinterpret_cast<T*>(smem_raw);  // [qual_total][8]
   __shared__ int s_start[kAsmRows + 1];
@@ -282,7 +343,6 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
   const bool with_d = kappa != T(0);
   const T ek = exp_scale<T>(kappa);
   using V4 = typename Vec4<T>::type;
-  V4* out = reinterpret_cast<V4*>(coef);
   for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) {
     const int j = cols[c0 + cc];
     const T ie = T(1.0 / eps[j]);
@@ -300,7 +360,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
         v.y = T(0);
         v.z = T(0);
         v.w = T(0);
-        out[o] = v;
+        out(o, v);
         continue;
       }
       T A = 0, B = 0, C = 0, D = 0;
@@ -342,7 +402,7 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
       v.y = B;
       v.z = C;
       v.w = D * ie;
-      out[o] = v;
+      out(o, v);
     }
   }
 }
@@ -486,11 +546,11 @@ __global__ void __launch_bounds__(kAsmThreads) instant_kernel(
 // y_f[i] = sum_j B_ij f_j - A_ij h_j ; y_h[i] = sum_j D_ij f_j - C_ij h_j
 // over the leaf's columns (the cached-coefficient stream of
 // src/beep/beep.cpp:1049-1062).  Accumulation type AccT.
-template <typename T>
+template <typename T, bool kCompact>
 __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
     const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
-    const T* __restrict__ coef, const double* __restrict__ diag, int n, const double* __restrict__ x,
+    const CoefReader<T, kCompact> rd, const double* __restrict__ diag, int n, const double* __restrict__ x,
     const double* __restrict__ yfar, double* __restrict__ y, int n_items, int stage_cols) {
   extern __shared__ unsigned char smem_raw[];
   T* sf = reinterpret_cast<T*>(smem_raw);
@@ -505,14 +565,14 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     // a neighbourhood beyond the shared-memory staging: x gathered through
     // the column ids (x is L2-resident), one coefficient per lane and step
     using V4 = typename Vec4<T>::type;
-    const V4* blk = reinterpret_cast<const V4*>(coef) + coef_off[it.leaf];
+    const int64_t blk = coef_off[it.leaf];
     const int lane = threadIdx.x & 31;
     const int64_t r0 = row_off[it.leaf] + it.row_begin;
     for (int r = threadIdx.x >> 5; r < it.row_count; r += blockDim.x >> 5) {
-      const V4* rowp = blk + (int64_t)(it.row_begin + r) * ncols;
+      const int64_t rowp = blk + (int64_t)(it.row_begin + r) * ncols;
       T accf = 0, acch = 0;
       for (int cc = lane; cc < ncols; cc += 32) {
-        const V4 v = ld_stream(rowp + cc);
+        const V4 v = rd(rowp + cc);
         const int j = cols[c0 + cc];
         const T xf = T(x[j]), xh = T(x[n + j]);
         accf += v.y * xf - v.x * xh;
@@ -546,22 +606,25 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
   }
   __syncthreads();
   using V4 = typename Vec4<T>::type;
-  const V4* blk = reinterpret_cast<const V4*>(coef) + coef_off[it.leaf];
+  const int64_t blk = coef_off[it.leaf];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   const int64_t r0 = row_off[it.leaf] + it.row_begin;
   for (int r = warp; r < it.row_count; r += nwarps) {
-    const V4* rowp = blk + (int64_t)(it.row_begin + r) * ncols;
+    const int64_t rowp = blk + (int64_t)(it.row_begin + r) * ncols;
     T accf = 0, acch = 0;
     int cc = lane;
-    // eight 16-byte (FP32) / 32-byte (FP64) coefficient loads in flight per lane
-    for (; cc + 224 < ncols; cc += 256) {
-      V4 v[8];
+    // eight 16-byte (FP32) / 32-byte (FP64) / 12-byte (compact) coefficient
+    // loads in flight per lane (compact: twelve ran the apply at 0.148
+    // against 0.141 ms on the 40962-patch star)
+    constexpr int kU = 8;
+    for (; cc + 32 * (kU - 1) < ncols; cc += 32 * kU) {
+      V4 v[kU];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) v[u] = ld_stream(rowp + cc + 32 * u);
+      for (int u = 0; u < kU; ++u) v[u] = rd(rowp + cc + 32 * u);
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < kU; ++u) {
         accf += v[u].y * sf[cc + 32 * u] - v[u].x * sh[cc + 32 * u];
         acch += v[u].w * sf[cc + 32 * u] - v[u].z * sh[cc + 32 * u];
       }
@@ -569,7 +632,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
     for (; cc + 96 < ncols; cc += 128) {
       V4 v[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = ld_stream(rowp + cc + 32 * u);
+      for (int u = 0; u < 4; ++u) v[u] = rd(rowp + cc + 32 * u);
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         accf += v[u].y * sf[cc + 32 * u] - v[u].x * sh[cc + 32 * u];
@@ -577,7 +640,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(
       }
     }
     for (; cc < ncols; cc += 32) {
-      const V4 v = ld_stream(rowp + cc);
+      const V4 v = rd(rowp + cc);
       accf += v.y * sf[cc] - v.x * sh[cc];
       acch += v.w * sf[cc] - v.z * sh[cc];
     }
@@ -701,7 +764,8 @@ void nf_assemble(Problem& P) {
   P.asm_gc = upload(ctx, P.h_gc);  // geometric correction per patch
   P.asm_items = upload(ctx, asm_items);
   P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
-  if (!nf.on_demand) nf.coef.alloc(ctx, elem * 4 * (size_t)nf.n_pairs);
+  nf.compact = !P.fp64 && (P.params.flags & BP_FLAG_COMPACT_NEARFIELD) != 0;
+  if (!nf.on_demand) nf.coef.alloc(ctx, (nf.compact ? 12 : elem * 4) * (size_t)nf.n_pairs);
   BP_CUDA(cudaEventRecord(P.asm_in, ctx->stream));
   const cudaStream_t st = P.asm_stream;
   BP_CUDA(cudaStreamWaitEvent(st, P.asm_in, 0));
@@ -732,19 +796,28 @@ void nf_assemble(Problem& P) {
   }
   if (!asm_items.empty()) {
     if (P.fp64) {
-      ensure_dynamic_smem((const void*)assemble_kernel<double>, smem);
-      assemble_kernel<double><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
+      ensure_dynamic_smem((const void*)assemble_kernel<double, false>, smem);
+      assemble_kernel<double, false><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
           d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual.as<double>(), nq,
           P.d_quad_off.as<int32_t>(), P.d_quad.as<double>(), np, P.d_eps.as<double>(), P.params.kappa,
-          P.d_diag.as<double>(), nf.coef.as<double>());
-    } else {
-      ensure_dynamic_smem((const void*)assemble_kernel<float>, smem);
-      assemble_kernel<float><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
+          P.d_diag.as<double>(), CoefWriter<double, false>{nf.coef.as<double4>()});
+    } else if (nf.compact) {
+      uint2* p01 = nf.coef.as<uint2>();
+      const CoefWriter<float, true> out{p01, reinterpret_cast<uint32_t*>(p01 + nf.n_pairs)};
+      ensure_dynamic_smem((const void*)assemble_kernel<float, true>, smem);
+      assemble_kernel<float, true><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
           d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(), nq,
           P.d_quad_off.as<int32_t>(), P.d_quad_f.as<float>(), np, P.d_eps.as<double>(), (float)P.params.kappa,
-          P.d_diag.as<double>(), nf.coef.as<float>());
+          P.d_diag.as<double>(), out);
+    } else {
+      ensure_dynamic_smem((const void*)assemble_kernel<float, false>, smem);
+      assemble_kernel<float, false><<<(int)asm_items.size(), kAsmThreads, smem, st>>>(
+          d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+          nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(), nq,
+          P.d_quad_off.as<int32_t>(), P.d_quad_f.as<float>(), np, P.d_eps.as<double>(), (float)P.params.kappa,
+          P.d_diag.as<double>(), CoefWriter<float, false>{nf.coef.as<float4>()});
     }
     BP_LAUNCH_CHECK();
   }
@@ -753,9 +826,11 @@ void nf_assemble(Problem& P) {
   // a leaf's columns (leaves with more columns than fit gather x instead)
   const size_t apply_smem = 2 * elem * (size_t)std::min(nf.max_cols, apply_stage_cols(elem));
   if (P.fp64)
-    ensure_dynamic_smem((const void*)apply_kernel<double>, apply_smem);
+    ensure_dynamic_smem((const void*)apply_kernel<double, false>, apply_smem);
+  else if (nf.compact)
+    ensure_dynamic_smem((const void*)apply_kernel<float, true>, apply_smem);
   else
-    ensure_dynamic_smem((const void*)apply_kernel<float>, apply_smem);
+    ensure_dynamic_smem((const void*)apply_kernel<float, false>, apply_smem);
   // rows per apply item: 64, halved (down to 8) while the grid would hold
   // fewer than 8 blocks per SM, so small problems still fill the GPU
   int rows_per_item = kApplyRows;
@@ -810,15 +885,21 @@ int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_
   const size_t smem = 2 * elem * (size_t)std::min(nf.max_cols, stage);
   const int grid = std::min(nf.n_items, kApplyBlocksPerSm * P.ctx->sm_count);
   if (P.fp64) {
-    apply_kernel<double><<<grid, kApplyThreads, smem, stream>>>(
+    apply_kernel<double, false><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
-        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<double>(), P.d_diag.as<double>(), P.n, x_dev,
-        yfar_dev, y_dev, nf.n_items, stage);
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), CoefReader<double, false>{nf.coef.as<double4>()},
+        P.d_diag.as<double>(), P.n, x_dev, yfar_dev, y_dev, nf.n_items, stage);
+  } else if (nf.compact) {
+    apply_kernel<float, true><<<grid, kApplyThreads, smem, stream>>>(
+        nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(),
+        CoefReader<float, true>{nf.coef.as<uint2>(), reinterpret_cast<const uint32_t*>(nf.coef.as<uint2>() + nf.n_pairs)},
+        P.d_diag.as<double>(), P.n, x_dev, yfar_dev, y_dev, nf.n_items, stage);
   } else {
-    apply_kernel<float><<<grid, kApplyThreads, smem, stream>>>(
+    apply_kernel<float, false><<<grid, kApplyThreads, smem, stream>>>(
         nf.items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
-        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), nf.coef.as<float>(), P.d_diag.as<double>(), P.n, x_dev,
-        yfar_dev, y_dev, nf.n_items, stage);
+        nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), CoefReader<float, false>{nf.coef.as<float4>()},
+        P.d_diag.as<double>(), P.n, x_dev, yfar_dev, y_dev, nf.n_items, stage);
   }
   BP_LAUNCH_CHECK();
   return 1;

@@ -73,10 +73,10 @@ def workload(name: str):
     raise ValueError(f"unknown workload {name}")
 
 
-def build_beep(meshes, kappa, nbsize, precision, device, context=None, tree=None):
+def build_beep(meshes, kappa, nbsize, precision, device, context=None, tree=None, **opts):
     import beep3_b200 as b
     kw = dict(tree) if tree else dict(nbsize=nbsize)
-    bp = b.BEEP(eps_solvent=80.0, kappa=kappa, precision=precision, device=device, context=context, **kw)
+    bp = b.BEEP(eps_solvent=80.0, kappa=kappa, precision=precision, device=device, context=context, **kw, **opts)
     for mesh, off, q in meshes:
         bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
     bp.build()
@@ -117,6 +117,32 @@ def tuned_tree(meshes, kappa, nbsize, local, x, y, steps, flush):
             bp.close()
     finally:
         ctx.close()
+
+
+def compact_nearfield(meshes, kappa, nbsize, local, x, y, steps, flush, e_fp64, hbm):
+    """The mixed engine with the compact near field (BP_FLAG_COMPACT_NEARFIELD:
+    coefficients rounded to 24 bits, 12 bytes a pair) on the headline's
+    tree: matvec/s, the apply kernel's time and bandwidth, and the energy
+    against the FP64 engine's."""
+    bp = build_beep(meshes, kappa, nbsize, "mixed", local, compact_nearfield=True)
+    try:
+        inf = bp.info()
+        n2 = 2 * bp.num_patches
+        time_device_matvecs(bp, x, y, 3, flush)
+        ms = time_device_matvecs(bp, x, y, steps, flush)
+        near_ms = stage_profile(bp, x, y)[0][0]
+        alg = inf.n_nearfield_pairs * 12 + inf.n_nearfield_cols * 4 + n2 * 8 * 2 + bp.num_patches * 32
+        bp.solve(1e-6, 100)
+        e, _ = bp.calculate_energies()
+        return {"matvec_per_s": steps / (sum(ms) / 1e3), "ms_per_step": sum(ms) / steps,
+                "apply_ms": near_ms, "apply_algorithmic_bytes": int(alg),
+                "apply_gbs": alg / (near_ms * 1e-3) / 1e9, "apply_frac": alg / (near_ms * 1e-3) / 1e9 / hbm,
+                "device_bytes": int(inf.device_bytes),
+                "energy_rel_vs_fp64": abs(e - e_fp64) / abs(e_fp64),
+                "note": "near-field coefficients rounded to 24 bits (at most 2^-16 relative each), "
+                        "12 bytes a pair; an option of this engine, not the reference's FP32 cache"}
+    finally:
+        bp.close()
 
 
 # --------------------------------------------------------------------------- clocks
@@ -485,13 +511,14 @@ def _only_matvec(args, local):
     """Profiling mode: the mixed engine only, W warm-up + K timed matvecs."""
     import torch
     desc, meshes, kappa, nbsize = workload(args.workload)
-    bp = build_beep(meshes, kappa, nbsize, "mixed", local)
+    bp = build_beep(meshes, kappa, nbsize, "mixed", local, compact_nearfield=args.compact)
     dev = torch.device("cuda", local)
     x = torch.randn(2 * bp.num_patches, dtype=torch.float64, device=dev)
     y = torch.empty_like(x)
     time_device_matvecs(bp, x, y, args.warmup, None)
     ms = time_device_matvecs(bp, x, y, args.steps, None)
-    print(json.dumps({"mode": "only-matvec", "config": desc, "ms_per_step": sum(ms) / len(ms)}), flush=True)
+    print(json.dumps({"mode": "only-matvec", "config": desc, "compact_nearfield": args.compact,
+                      "ms_per_step": sum(ms) / len(ms)}), flush=True)
     bp.close()
 
 
@@ -744,6 +771,12 @@ def _run_ours(args, world, rank, local, dist):
                               "rel_err_mixed_vs_fp64": abs(e_mixed - e_fp64) / abs(e_fp64)},
         "clocks": clocks,
     }
+    if rank == 0 and world == 1:
+        try:  # an extra key: the headline line stands without it
+            line["compact_nearfield"] = compact_nearfield(meshes, kappa, nbsize, local, x, y, args.steps, flush,
+                                                          e_fp64, hbm)
+        except Exception as e:
+            line["compact_nearfield"] = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the CPU baseline: rank 0 at N = 1 only
         line["cpu_baseline"], parity = cpu_baseline_and_parity(bp, bp64)
         line.update(parity)
@@ -785,6 +818,8 @@ def main():
                          "for all")
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
+    ap.add_argument("--compact", action="store_true",
+                    help="profiling mode: the compact (24-bit) near-field coefficients")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scan", action="store_true",
                     help="leave out the config-B scan and config-R serving keys of the default line")

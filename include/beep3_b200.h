@@ -148,7 +148,17 @@ enum bp_flags {
    * children being shadows) and the FMM bookkeeping are the reference's.
    * Results equal the reference-tree problem's to the FMM's accuracy, not
    * bitwise: the near/far split of pairs differs. */
-  BP_FLAG_DEVICE_TREE = 2
+  BP_FLAG_DEVICE_TREE = 2,
+  /* Mixed engine only, cached near field only: each FP32 coefficient is
+   * rounded to its top 24 bits (sign, exponent, 15 stored significand bits;
+   * round to nearest) and stored in 12 bytes a pair instead of 16, read by
+   * the apply kernel and widened in registers.  A storage option of this
+   * engine with no reference counterpart (the reference caches FP32
+   * coefficients, src/beep/beep.cpp:768-1064): 25 % less coefficient
+   * memory and traffic per matvec for a relative error of at most 2^-16 per
+   * coefficient.  Combined with BP_PREC_FP64 or
+   * BP_FLAG_NEARFIELD_ON_DEMAND the call fails with BP_ERR_INVALID. */
+  BP_FLAG_COMPACT_NEARFIELD = 4
 };
 
 typedef struct {
