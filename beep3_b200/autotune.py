@@ -20,7 +20,12 @@ discarded, and the cheapest of the rest wins.  Two trials are provided:
   worker and batch configuration; cost = time per pose.
 
 Order 18 is tried when asked and recorded as unsupported: the engine's
-far-field kernels are laid out for order 9.
+far-field kernels are laid out for order 9.  With ``compact=(False, True)``
+every candidate tree is also tried with the compact near field
+(BEEP(compact_nearfield=True): coefficients rounded to 24 bits, 12 bytes a
+pair; mixed precision only, recorded as unsupported otherwise); the energy
+check applies to it as to any other candidate, against the reference tree
+with FP32 coefficients.
 """
 from __future__ import annotations
 
@@ -46,12 +51,17 @@ class Trial:
     energies: list = field(default_factory=list)  # the workload's energies (kJ/mol)
     status: str = "ok"  # ok / energy / unsupported
     detail: dict = field(default_factory=dict)
+    compact: bool = False  # the compact near field
 
     def settings(self) -> dict:
         """Keyword arguments of BEEP for this candidate."""
         if self.tree == "device":
-            return dict(tree="device", leaf_size=self.size, nterms=self.nterms)
-        return dict(tree="reference", nbsize=self.size, nterms=self.nterms)
+            kw = dict(tree="device", leaf_size=self.size, nterms=self.nterms)
+        else:
+            kw = dict(tree="reference", nbsize=self.size, nterms=self.nterms)
+        if self.compact:
+            kw["compact_nearfield"] = True
+        return kw
 
 
 @dataclass
@@ -83,13 +93,16 @@ def choose(trials: list[Trial], reference_energies, energy_tol: float) -> Trial:
     return best
 
 
-def autotune(trial: Callable[[str, int, int], Trial], candidates=DEFAULT_CANDIDATES, orders=(9,),
-             energy_tol: float = 1e-4) -> TuneResult:
-    """``trial(tree, size, nterms)`` runs the workload with one candidate.
-    The first candidate that runs at order 9 is the reference for the energy
-    check (by default the reference's own tree at its default nbsize)."""
-    trials = [trial(tree, size, nt) for nt in orders for tree, size in candidates]
-    ref = next(t for t in trials if t.nterms == 9 and t.status == "ok")
+def autotune(trial: Callable[..., Trial], candidates=DEFAULT_CANDIDATES, orders=(9,), energy_tol: float = 1e-4,
+             compact=(False,)) -> TuneResult:
+    """``trial(tree, size, nterms)`` runs the workload with one candidate
+    (``trial(tree, size, nterms, compact=True)`` for the compact near
+    field).  The first candidate that runs at order 9 with FP32 coefficients
+    is the reference for the energy check (by default the reference's own
+    tree at its default nbsize)."""
+    trials = [trial(tree, size, nt, compact=True) if c else trial(tree, size, nt)
+              for c in compact for nt in orders for tree, size in candidates]
+    ref = next(t for t in trials if t.nterms == 9 and not t.compact and t.status == "ok")
     best = choose(trials, ref.energies, energy_tol)
     return TuneResult(best, trials, list(ref.energies))
 
@@ -99,11 +112,15 @@ def problem_trial(make: Callable[..., BEEP], solves_per_problem: float = 1.0, to
     """A trial that builds the scenario (``make(**tree keywords)``, a BEEP
     with its instances inserted) ``repeats`` times and keeps the fastest
     set-up and solve: cost = set-up + solves_per_problem x solve."""
-    def run(tree: str, size: int, nterms: int) -> Trial:
-        t = Trial(tree, size, nterms)
+    def run(tree: str, size: int, nterms: int, compact: bool = False) -> Trial:
+        t = Trial(tree, size, nterms, compact=compact)
         best_setup = best_solve = float("inf")
         for _ in range(repeats):
-            bp = make(**t.settings())
+            try:
+                bp = make(**t.settings())
+            except ValueError:  # the compact near field outside the mixed engine
+                t.status = "unsupported"
+                return t
             try:
                 inf = bp.info()
             except N.BeepError as e:

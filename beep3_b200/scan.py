@@ -211,8 +211,11 @@ def scan_trial(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1
     from ._native import BP_ERR_UNSUPPORTED, BeepError
     from .autotune import Trial
 
-    def run(tree: str, size: int, nterms: int) -> Trial:
-        t = Trial(tree, size, nterms)
+    def run(tree: str, size: int, nterms: int, compact: bool = False) -> Trial:
+        t = Trial(tree, size, nterms, compact=compact)
+        if compact and precision != "mixed":
+            t.status = "unsupported"
+            return t
         best = float("inf")
         for _ in range(repeats):
             try:

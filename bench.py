@@ -84,10 +84,10 @@ def build_beep(meshes, kappa, nbsize, precision, device, context=None, tree=None
 
 
 def tuned_tree(meshes, kappa, nbsize, local, x, y, steps, flush):
-    """The tree the autotuner picks for a problem solved many times (100
-    solves per build) on the same molecule, and the mixed matvec/s on it:
-    the survey's performance tree for this configuration, beside the
-    headline's parity tree."""
+    """The tree and near-field storage (FP32 or compact coefficients) the
+    autotuner picks for a problem solved many times (100 solves per build)
+    on the same molecule, and the mixed matvec/s on it: the performance
+    configuration, beside the headline's parity tree and FP32 cache."""
     import beep3_b200 as b
     from beep3_b200.autotune import autotune, problem_trial
     ctx = b.EngineContext(local)
@@ -98,7 +98,7 @@ def tuned_tree(meshes, kappa, nbsize, local, x, y, steps, flush):
                 bp.insert_mesh_instance(mesh, offset=off, rotation=q, eps_protein=2.0)
             return bp
         t0 = time.perf_counter()
-        res = autotune(problem_trial(make, solves_per_problem=100.0, repeats=2))
+        res = autotune(problem_trial(make, solves_per_problem=100.0, repeats=2), compact=(False, True))
         tune_s = time.perf_counter() - t0
         bp = build_beep(meshes, kappa, nbsize, "mixed", local, context=ctx, tree=res.settings())
         try:
@@ -111,7 +111,8 @@ def tuned_tree(meshes, kappa, nbsize, local, x, y, steps, flush):
                     / abs(res.reference_energies[0]),
                     "nearfield_pairs": int(inf.n_nearfield_pairs), "tree_levels": int(inf.n_levels),
                     "tuning_seconds": tune_s,
-                    "trials": [{"tree": t.tree, "size": t.size, "cost_ms": t.cost_ms, "status": t.status}
+                    "trials": [{"tree": t.tree, "size": t.size, "compact": t.compact, "cost_ms": t.cost_ms,
+                                "status": t.status}
                                for t in res.trials]}
         finally:
             bp.close()

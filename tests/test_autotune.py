@@ -44,3 +44,34 @@ def test_autotune_drives_the_trial():
     assert res.settings() == dict(tree="reference", nbsize=700, nterms=9)
     assert res.reference_energies == [-10.0]
     assert [t.status for t in res.trials] == ["ok", "ok", "energy"] + ["unsupported"] * 3
+
+
+def test_autotune_tries_compact_storage():
+    """With compact=(False, True) every tree is tried with both near-field
+    storages; the energy reference is the first FP32-coefficient candidate,
+    and a cheaper compact candidate within the tolerance wins."""
+    seen = []
+
+    def run(tree, size, nterms, compact=False):
+        seen.append((tree, size, compact))
+        cost = {1500: 10.0, 700: 8.0}[size] - (1.5 if compact else 0.0)
+        e = -10.0 - (2e-6 if compact else 0.0) - (1e-5 if size == 700 else 0.0)
+        return Trial(tree, size, nterms, cost_ms=cost, energies=[e], compact=compact)
+
+    res = autotune(run, candidates=(("reference", 1500), ("reference", 700)), compact=(False, True))
+    assert seen == [("reference", 1500, False), ("reference", 700, False),
+                    ("reference", 1500, True), ("reference", 700, True)]
+    assert res.reference_energies == [-10.0]
+    assert res.settings() == dict(tree="reference", nbsize=700, nterms=9, compact_nearfield=True)
+    assert not res.trials[0].compact and res.trials[3].compact
+
+
+def test_compact_is_unsupported_outside_the_mixed_engine():
+    from beep3_b200.autotune import problem_trial
+
+    def make(**kw):
+        import beep3_b200 as b
+        return b.BEEP(precision="fp64", **kw)
+
+    t = problem_trial(make)("reference", 1500, 9, compact=True)
+    assert t.status == "unsupported" and t.compact

@@ -33,6 +33,26 @@ def test_autotune_problem():
     ctx.close()
 
 
+def test_autotune_compact_storage():
+    """Both near-field storages per tree: the compact candidates build,
+    solve within 1e-4 of the FP32 reference tree's energy (they are within
+    about 1e-6) and the chosen settings build a problem."""
+    V, T, shape = b.star_surface(5, 20.0, seed=407)
+    mesh = b.Mesh(V, T, b.charges_in_star(100, shape, seed=408))
+    ctx = b.EngineContext(0)
+    make = scenario_factory([(mesh, mesh.centre, (1.0, 0.0, 0.0, 0.0), 2.0)], ctx, kappa=0.1, precision="mixed")
+    res = autotune(problem_trial(make, repeats=1), candidates=(("reference", 1500), ("reference", 700)),
+                   compact=(False, True))
+    assert [t.compact for t in res.trials] == [False, False, True, True]
+    assert all(t.status == "ok" for t in res.trials)
+    ref = res.reference_energies[0]
+    assert abs(res.trials[2].energies[0] - res.trials[0].energies[0]) <= 1e-5 * abs(ref)
+    bp = make(**res.settings())
+    bp.solve(1e-6, 100)
+    bp.close()
+    ctx.close()
+
+
 def test_autotune_scan():
     va, ta, sa = b.star_surface(4, 20.0, seed=403)
     vb, tb, sb = b.star_surface(3, 12.0, seed=404)
