@@ -29,6 +29,7 @@ BP_PREC_MIXED = 1
 BP_FLAG_NEARFIELD_ON_DEMAND = 1
 BP_FLAG_DEVICE_TREE = 2
 BP_FLAG_COMPACT_NEARFIELD = 4
+BP_FLAG_MESH_PAIR_CACHE = 8
 
 _ERR_NAMES = {
     BP_ERR_INVALID: "invalid argument", BP_ERR_CUDA: "CUDA error", BP_ERR_NOMEM: "out of host memory",

@@ -51,7 +51,7 @@ class ScenarioBatch:
             same = (s.kappa == s0.kappa and s.precision == s0.precision and s.eps_solvent == s0.eps_solvent
                     and s.nterms == s0.nterms and s.tree_kind == s0.tree_kind and s.nbsize == s0.nbsize
                     and s.leaf_size == s0.leaf_size and s.nearfield_on_demand == s0.nearfield_on_demand
-                    and s.compact_nearfield == s0.compact_nearfield)
+                    and s.compact_nearfield == s0.compact_nearfield and s.cache_mesh_pairs == s0.cache_mesh_pairs)
             if not same:
                 raise ValueError("the scenarios of a batch need the same kappa, precision, solvent, order and tree")
         self.scenarios = list(scenarios)
@@ -106,7 +106,8 @@ class ScenarioBatch:
         centres = np.ascontiguousarray(self.centres.ravel())
         flags = ((N.BP_FLAG_NEARFIELD_ON_DEMAND if s0.nearfield_on_demand else 0) |
                  (N.BP_FLAG_DEVICE_TREE if s0.tree_kind == "device" else 0) |
-                 (N.BP_FLAG_COMPACT_NEARFIELD if s0.compact_nearfield else 0))
+                 (N.BP_FLAG_COMPACT_NEARFIELD if s0.compact_nearfield else 0) |
+                 (N.BP_FLAG_MESH_PAIR_CACHE if s0.cache_mesh_pairs else 0))
         prm = N.bp_params(s0.kappa, BETA0, (C.c_double * 3)(0.0, 0.0, 0.0), self.cube_edge,
                           s0.leaf_size if s0.tree_kind == "device" else s0.nbsize, s0.nterms,
                           N.BP_PREC_FP64 if s0.precision == "fp64" else N.BP_PREC_MIXED, flags)

@@ -213,7 +213,8 @@ class BEEP:
     def __init__(self, eps_solvent: float = 80.0, kappa: float = 0.1, nbsize: int = DEFAULT_NBSIZE,
                  nterms: int = 9, precision: str = "fp64", device: int = 0, hbm_budget_bytes: int = 0,
                  context: EngineContext | None = None, nearfield_on_demand: bool = False,
-                 tree: str = "reference", leaf_size: int = 64, compact_nearfield: bool = False):
+                 tree: str = "reference", leaf_size: int = 64, compact_nearfield: bool = False,
+                 cache_mesh_pairs: bool = False):
         """``context``: an EngineContext shared with scenarios run before or
         after this one (its device and budget apply); by default the scenario
         has its own.  ``nearfield_on_demand``: recompute the near field in
@@ -226,7 +227,11 @@ class BEEP:
         ``compact_nearfield`` (mixed precision only): cache each FP32
         near-field coefficient rounded to 24 bits, 12 bytes a pair instead of
         16 (relative error at most 2^-16 per coefficient; no reference
-        counterpart)."""
+        counterpart).  ``cache_mesh_pairs`` (mixed precision): keep the
+        near-field coefficients of each mesh's own close patch pairs with
+        the mesh, computed once in its frame, and look them up in every
+        later problem with that mesh and kappa (rigid moves leave them
+        unchanged; a scan's poses then integrate only the rest)."""
         self.eps_solvent = float(eps_solvent)
         self.kappa = float(kappa)
         self.nbsize = int(nbsize)
@@ -236,6 +241,7 @@ class BEEP:
         self.precision = precision
         self.nearfield_on_demand = bool(nearfield_on_demand)
         self.compact_nearfield = bool(compact_nearfield)
+        self.cache_mesh_pairs = bool(cache_mesh_pairs)
         if self.compact_nearfield and (precision != "mixed" or self.nearfield_on_demand):
             raise ValueError("compact_nearfield needs precision='mixed' and cached coefficients")
         if tree not in ("reference", "device"):
@@ -392,7 +398,8 @@ class BEEP:
             insts[k].dielectric_ratio = inst.dielectric_ratio
         flags = ((N.BP_FLAG_NEARFIELD_ON_DEMAND if self.nearfield_on_demand else 0) |
                  (N.BP_FLAG_DEVICE_TREE if self.tree_kind == "device" else 0) |
-                 (N.BP_FLAG_COMPACT_NEARFIELD if self.compact_nearfield else 0))
+                 (N.BP_FLAG_COMPACT_NEARFIELD if self.compact_nearfield else 0) |
+                 (N.BP_FLAG_MESH_PAIR_CACHE if self.cache_mesh_pairs else 0))
         prm = N.bp_params(self.kappa, BETA0, (C.c_double * 3)(*centre), edge,
                           self.leaf_size if self.tree_kind == "device" else self.nbsize, self.nterms,
                           N.BP_PREC_FP64 if self.precision == "fp64" else N.BP_PREC_MIXED, flags)

@@ -79,7 +79,8 @@ int32_t check_params(const char* who, const bp_params* prm) {
   if (prm->precision != BP_PREC_FP64 && prm->precision != BP_PREC_MIXED)
     return fail(BP_ERR_INVALID, std::string(who) + ": unknown precision");
   if (!(prm->kappa >= 0.0) || !std::isfinite(prm->kappa)) return fail(BP_ERR_INVALID, std::string(who) + ": bad kappa");
-  if (prm->flags & ~(BP_FLAG_NEARFIELD_ON_DEMAND | BP_FLAG_DEVICE_TREE | BP_FLAG_COMPACT_NEARFIELD))
+  if (prm->flags &
+      ~(BP_FLAG_NEARFIELD_ON_DEMAND | BP_FLAG_DEVICE_TREE | BP_FLAG_COMPACT_NEARFIELD | BP_FLAG_MESH_PAIR_CACHE))
     return fail(BP_ERR_INVALID, std::string(who) + ": unknown flags");
   if ((prm->flags & BP_FLAG_COMPACT_NEARFIELD) &&
       (prm->precision != BP_PREC_MIXED || (prm->flags & BP_FLAG_NEARFIELD_ON_DEMAND)))

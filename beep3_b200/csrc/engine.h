@@ -293,6 +293,23 @@ struct DevMesh {
   };
   std::vector<SelfPotential> self_potential;  // most recently used last
   static constexpr size_t kSelfPotentials = 4;
+  // Near-field coefficients of the mesh's own patch pairs closer than
+  // `radius` (centroid distance), computed once in the mesh's frame: a rigid
+  // move leaves them unchanged, so every posed problem with this mesh and
+  // kappa looks them up instead of integrating them (mixed engine, meshes
+  // with one quadrature point per patch).  Per pair six FP32 parts (A, Bu,
+  // Bg, Cg, Cu, D): B = Bu - Bg / eps, C = Cg - Cu / eps, D / eps for the
+  // instance's dielectric ratio eps.
+  struct PairCache {
+    double kappa = -1;
+    float radius = 0;
+    int64_t n_pairs = 0;
+    int max_row = 0;  // longest partner list
+    DevBuf off;   // int64 [n + 1]
+    DevBuf js;    // int32 [n_pairs]: the partners of each patch, ascending
+    DevBuf vals;  // float [n_pairs][6]
+  };
+  PairCache pair_cache;
   // posed problems placed from this mesh keep it: bp_mesh_destroy while any
   // exists leaves the deletion to the last of them
   int users = 0;
@@ -347,6 +364,7 @@ struct Problem {
   DevBuf d_qual_off, d_quad_off, d_gal_off;                 // int32
   DevBuf d_qual, d_quad, d_gal;                             // SoA of double, 7 arrays
   DevBuf d_qual_f, d_quad_f;                                // SoA of float (mixed)
+  DevBuf d_inst_of;  // int32 [n]: the placement of each patch (pair-cache lookups)
   DevBuf d_diag;                                            // 4n double (singular + corrections)
   NearField nf;
   std::unique_ptr<FmmState, void (*)(FmmState*)> fmm{nullptr, fmm_destroy};
@@ -383,7 +401,7 @@ struct Problem {
   // is set up; its inputs stay allocated until it is joined (nf_join)
   cudaStream_t asm_stream = nullptr;
   cudaEvent_t asm_in = nullptr, asm_t0 = nullptr, asm_t1 = nullptr;
-  DevBuf asm_gc, asm_items;
+  DevBuf asm_gc, asm_items, asm_views;
   ~Problem() {
     if (asm_stream) {
       cudaStreamSynchronize(asm_stream);

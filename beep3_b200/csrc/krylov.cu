@@ -409,7 +409,10 @@ inline int grid_for(int64_t len) {
 void ensure_dynamic_smem(const void* kernel, size_t bytes) {
   static std::mutex mu;
   static std::map<std::pair<int, const void*>, size_t> granted;
-  if (bytes <= 48 * 1024) return;  // the default limit
+  // the default limit holds static and dynamic shared memory together
+  cudaFuncAttributes fa;
+  BP_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  if (bytes + fa.sharedSizeBytes <= 48 * 1024) return;
   int dev = 0;
   BP_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);

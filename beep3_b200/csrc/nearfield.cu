@@ -407,6 +407,290 @@ __global__ void __launch_bounds__(kAsmThreads) assemble_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mesh pair cache (BP_FLAG_MESH_PAIR_CACHE).  The coefficients of a pair of
+// patches of one rigid mesh depend only on the mesh, kappa and the
+// instance's dielectric ratio, not on where the instance sits, so a scan
+// that places the same meshes pose after pose integrates them once, in the
+// mesh's frame, for every pair of patches closer than a radius, and each
+// pose's assembly looks them up.  Pairs beyond the radius, pairs of two
+// instances and the self pairs go through the integration as before.
+
+// One term of pair_term_unit with the dielectric factor left out: B and C
+// as their two parts (B = Bu - ie Bg, C = Cg - ie Cu) and D before its
+// factor ie.
+__device__ __forceinline__ void pair_term_parts(float qx, float qy, float qz, float qnx, float qny, float qnz, float px,
+                                                float py, float pz, float pnx, float pny, float pnz, float kappa,
+                                                float ek, bool with_d, float (&acc)[6]) {
+  const float dx = px - qx, dy = py - qy, dz = pz - qz;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  if (fabsf(r2) < 1e-9f) return;
+  const float ir = fast_rsqrt(r2);
+  const float r = r2 * ir;
+  const float e = exp_scaled(ek, r);
+  const float g = float(kOneOver4Pi) * ir;
+  const float eg = e * g;
+  const float t = ir * ir;
+  const float g3 = g * t;
+  const float u3 = eg * (t + kappa * ir);
+  const float ndx = pnx * dx + pny * dy + pnz * dz;
+  const float n0dx = qnx * dx + qny * dy + qnz * dz;
+  acc[0] += g - eg;
+  acc[1] += u3 * ndx;
+  acc[2] += g3 * ndx;
+  acc[3] += g3 * n0dx;
+  acc[4] += u3 * n0dx;
+  if (with_d) {
+    const float pu = eg * t * (kappa * (3.f * ir + kappa) + 3.f * t);
+    const float nn0 = pnx * qnx + pny * qny + pnz * qnz;
+    acc[5] -= ndx * n0dx * (3.f * g3 * t - pu) - nn0 * (g3 - u3);
+  }
+}
+
+// Partners j != i of every patch i with |c_i - c_j|^2 < r2: their count
+// (js == nullptr) or their list, ascending (from off[i]).  Every thread
+// scans all centroids through shared-memory tiles; both passes make the
+// same comparisons, so the lists have the counted lengths.
+__global__ void __launch_bounds__(256) pair_cache_scan_kernel(int n, const float4* __restrict__ c, float r2,
+                                                              int32_t* __restrict__ count,
+                                                              const int64_t* __restrict__ off,
+                                                              int32_t* __restrict__ js) {
+  __shared__ float4 tile[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const float4 ci = i < n ? c[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int64_t w = (js && i < n) ? off[i] : 0;
+  int cnt = 0;
+  for (int base = 0; base < n; base += 256) {
+    const int jj = base + threadIdx.x;
+    tile[threadIdx.x] = jj < n ? c[jj] : make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    const int lim = min(256, n - base);
+    if (i < n)
+      for (int t = 0; t < lim; ++t) {
+        // rounded operations only (no contraction), so both passes decide alike
+        const float dx = __fsub_rn(tile[t].x, ci.x), dy = __fsub_rn(tile[t].y, ci.y), dz = __fsub_rn(tile[t].z, ci.z);
+        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+        if (d2 < r2 && base + t != i) {
+          if (!js)
+            ++cnt;
+          else if (w < off[i + 1])
+            js[w++] = base + t;
+        }
+      }
+    __syncthreads();
+  }
+  if (!js && i < n) count[i] = cnt;
+}
+
+// The six parts of every listed pair, one block per patch i of the mesh:
+// i's qualocation points staged in shared memory (FP32, as the mixed
+// assembly converts them), one thread per partner j (one quadrature point
+// per patch), weights applied as in assemble_kernel.
+__global__ void __launch_bounds__(kAsmThreads) pair_cache_coef_kernel(
+    const int64_t* __restrict__ off, const int32_t* __restrict__ js, const int32_t* __restrict__ qoff,
+    const double* __restrict__ qual, int nq, const int32_t* __restrict__ poff, const double* __restrict__ quad, int np,
+    float kappa, float* __restrict__ vals) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* sq = reinterpret_cast<float*>(smem_raw);
+  const int i = blockIdx.x;
+  const int qs = qoff[i], nqi = qoff[i + 1] - qs;
+  for (int k = threadIdx.x; k < nqi; k += blockDim.x) {
+    for (int f = 0; f < 7; ++f) sq[8 * k + f] = (float)qual[(size_t)f * nq + qs + k];
+    sq[8 * k + 7] = 0.f;
+  }
+  __syncthreads();
+  const bool with_d = kappa != 0.f;
+  const float ek = exp_scale<float>(kappa);
+  for (int64_t k = off[i] + threadIdx.x; k < off[i + 1]; k += blockDim.x) {
+    const int p = poff[js[k]];
+    float p1[7];
+    for (int f = 0; f < 7; ++f) p1[f] = (float)quad[(size_t)f * np + p];
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+    for (int q = 0; q < nqi; ++q) {
+      float u[7];
+      load_qpoint(sq, q, u);
+      float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      pair_term_parts(u[0], u[1], u[2], u[3], u[4], u[5], p1[0], p1[1], p1[2], p1[3], p1[4], p1[5], kappa, ek, with_d,
+                      a);
+      for (int f = 0; f < 6; ++f) acc[f] += a[f] * u[6];
+    }
+    float2* o = reinterpret_cast<float2*>(vals + 6 * k);
+    o[0] = make_float2(acc[0] * p1[6], acc[1] * p1[6]);
+    o[1] = make_float2(acc[2] * p1[6], acc[3] * p1[6]);
+    o[2] = make_float2(acc[4] * p1[6], acc[5] * p1[6]);
+  }
+}
+
+// One placement's cache as the assembly sees it (off == nullptr: none).
+struct CacheView {
+  const int64_t* off;
+  const int32_t* js;
+  const float* vals;
+  int first;  // the placement's first patch in the problem
+};
+
+constexpr int kMissCap = 4096;  // pairs a block integrates in one pass
+
+// One (row, column) pair integrated as assemble_kernel does it (FP32).
+__device__ __forceinline__ float4 pair_integrated(const float* sq, int qs, int qe, int j, const int32_t* poff,
+                                                  const float* quad, int np, float kappa, float ek, float ie,
+                                                  bool with_d) {
+  const int ps = poff[j], pe = poff[j + 1];
+  float A = 0, B = 0, C = 0, D = 0;
+  if (pe - ps == 1) {
+    float p1[7];
+    for (int f = 0; f < 7; ++f) p1[f] = quad[(size_t)f * np + ps];
+    for (int q = qs; q < qe; ++q) {
+      float u[7];
+      load_qpoint(sq, q, u);
+      float a = 0, b = 0, c = 0, d = 0;
+      pair_term_unit<float>(u[0], u[1], u[2], u[3], u[4], u[5], p1[0], p1[1], p1[2], p1[3], p1[4], p1[5], kappa, ek,
+                            ie, with_d, a, b, c, d);
+      A += a * u[6];
+      B += b * u[6];
+      C += c * u[6];
+      D += d * u[6];
+    }
+    A *= p1[6];
+    B *= p1[6];
+    C *= p1[6];
+    D *= p1[6];
+  } else {
+    for (int q = qs; q < qe; ++q) {
+      float u[7];
+      load_qpoint(sq, q, u);
+      float a = 0, b = 0, c = 0, d = 0;
+      for (int p = ps; p < pe; ++p)
+        pair_term<float>(u[0], u[1], u[2], u[3], u[4], u[5], quad[p], quad[(size_t)np + p], quad[2 * (size_t)np + p],
+                         quad[3 * (size_t)np + p], quad[4 * (size_t)np + p], quad[5 * (size_t)np + p],
+                         quad[6 * (size_t)np + p], kappa, ie, with_d, a, b, c, d);
+      A += a * u[6];
+      B += b * u[6];
+      C += c * u[6];
+      D += d * u[6];
+    }
+  }
+  return make_float4(A, B, C, D * ie);
+}
+
+// assemble_kernel with the mesh pair caches (mixed engine): for each row,
+// its cached partner list is staged in shared memory; a thread takes the
+// row's columns, finds a column of the same placement by binary search and
+// combines its six parts with the column's dielectric factor.  Columns not
+// found (farther than the cache radius, of another placement, or of a
+// placement without a cache) are queued in shared memory and integrated
+// when the queue is full and at the end of the item, one pair per thread,
+// so that the integration runs on full warps.  Self pairs are zero, as in
+// assemble_kernel.
+template <bool kCompact>
+__global__ void __launch_bounds__(kAsmThreads) assemble_cached_kernel(
+    const NfItem* __restrict__ items, const int32_t* __restrict__ rows, const int64_t* __restrict__ row_off,
+    const int32_t* __restrict__ cols, const int64_t* __restrict__ col_off, const int64_t* __restrict__ coef_off,
+    const int32_t* __restrict__ qoff, const float* __restrict__ qual, int nq, const int32_t* __restrict__ poff,
+    const float* __restrict__ quad, int np, const double* __restrict__ eps, float kappa,
+    const int32_t* __restrict__ inst_of, const CacheView* __restrict__ views, int max_list, int qual_cap,
+    const CoefWriter<float, kCompact> out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* sq = reinterpret_cast<float*>(smem_raw);              // [qual_cap][8]
+  int32_t* s_js = reinterpret_cast<int32_t*>(sq + 8 * (size_t)qual_cap);  // [max_list]
+  __shared__ int s_miss[kMissCap];
+  __shared__ int s_nmiss;
+  __shared__ int s_start[kAsmRows + 1];
+  __shared__ int s_row[kAsmRows];
+  const NfItem it = items[blockIdx.x];
+  const int64_t r0 = row_off[it.leaf] + it.row_begin;
+  const int64_t c0 = col_off[it.leaf];
+  const int ncols = (int)(col_off[it.leaf + 1] - c0);
+  const int64_t block = coef_off[it.leaf];
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int r = 0; r < it.row_count; ++r) {
+      const int i = rows[r0 + r];
+      s_row[r] = i;
+      s_start[r] = acc;
+      acc += qoff[i + 1] - qoff[i];
+    }
+    s_start[it.row_count] = acc;
+    s_nmiss = 0;
+  }
+  __syncthreads();
+  for (int r = 0; r < it.row_count; ++r) {
+    const int i = s_row[r];
+    const int base = qoff[i];
+    const int cnt = s_start[r + 1] - s_start[r];
+    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+      float* dst = sq + 8 * (s_start[r] + k);
+      for (int f = 0; f < 7; ++f) dst[f] = qual[(size_t)f * nq + base + k];
+      dst[7] = 0.f;
+    }
+  }
+  __syncthreads();
+  const bool with_d = kappa != 0.f;
+  const float ek = exp_scale<float>(kappa);
+  // integrates the queued pairs (called by every thread, after a barrier)
+  auto flush = [&]() {
+    const int nm = s_nmiss;
+    for (int m = threadIdx.x; m < nm; m += blockDim.x) {
+      const int r = s_miss[m] >> 24, cc = s_miss[m] & 0xFFFFFF;
+      const int j = cols[c0 + cc];
+      const float ie = float(1.0 / eps[j]);
+      out(block + (int64_t)(it.row_begin + r) * ncols + cc,
+          pair_integrated(sq, s_start[r], s_start[r + 1], j, poff, quad, np, kappa, ek, ie, with_d));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_nmiss = 0;
+    __syncthreads();
+  };
+  for (int r = 0; r < it.row_count; ++r) {
+    const int i = s_row[r];
+    const int pi = inst_of[i];
+    const CacheView v = views[pi];
+    int len = 0;
+    int64_t lbase = 0;
+    if (v.off) {
+      lbase = v.off[i - v.first];
+      len = (int)(v.off[i - v.first + 1] - lbase);
+      for (int k = threadIdx.x; k < len; k += blockDim.x) s_js[k] = v.js[lbase + k];
+    }
+    __syncthreads();
+    for (int lo = 0; lo < ncols; lo += kMissCap) {
+      const int hi = min(ncols, lo + kMissCap);
+      if (s_nmiss + (hi - lo) > kMissCap) flush();  // s_nmiss is the same for every thread here
+      for (int cc = lo + threadIdx.x; cc < hi; cc += blockDim.x) {
+        const int j = cols[c0 + cc];
+        const int64_t o = block + (int64_t)(it.row_begin + r) * ncols + cc;
+        if (j == i) {
+          out(o, make_float4(0.f, 0.f, 0.f, 0.f));
+          continue;
+        }
+        bool found = false;
+        if (len > 0 && inst_of[j] == pi) {
+          const int jl = j - v.first;
+          int a = 0, b = len;  // first entry >= jl
+          while (a < b) {
+            const int m = (a + b) >> 1;
+            if (s_js[m] < jl)
+              a = m + 1;
+            else
+              b = m;
+          }
+          if (a < len && s_js[a] == jl) {
+            const float2* pv = reinterpret_cast<const float2*>(v.vals + 6 * (lbase + a));
+            const float2 x0 = pv[0], x1 = pv[1], x2 = pv[2];
+            const float ie = float(1.0 / eps[j]);
+            out(o, make_float4(x0.x, x0.y - ie * x1.x, x1.y - ie * x2.x, x2.y * ie));
+            found = true;
+          }
+        }
+        if (!found) s_miss[atomicAdd(&s_nmiss, 1)] = (r << 24) | cc;
+      }
+      __syncthreads();
+    }
+  }
+  flush();
+}
+
 // The near field without cached coefficients (the reference's
 // BEM_kernels_instant + processBEMBlockResults for its uncached OpenCL path,
 // src/bem/opencl_bem_kernels.cl:237-352, src/beep/beep.cpp:999-1008): the
@@ -719,6 +1003,84 @@ void nf_build_structure(Problem& P) {
   nf.coef_off = upload(ctx, nf.h_coef_off);
 }
 
+namespace {
+
+constexpr float kCacheRadiusEdges = 4.4f;  // cache radius in edges of the problem's smallest leaf
+constexpr double kCacheMaxBytes = 8e9;     // per mesh and kappa
+
+// The mesh's pair cache for kappa, built on `st` if missing (radius shrunk
+// while the cache would exceed kCacheMaxBytes).  The caller holds m.mu.
+// False when the mesh cannot have one (more than one quadrature point on a
+// patch, nothing within the radius).
+bool ensure_pair_cache(DevMesh& m, double kappa, float radius, cudaStream_t st) {
+  DevMesh::PairCache& pc = m.pair_cache;
+  if (pc.kappa == kappa && pc.n_pairs > 0) return true;
+  for (int i = 0; i < m.n; ++i)
+    if (m.h_quad_off[i + 1] - m.h_quad_off[i] != 1) return false;
+  Ctx* ctx = m.ctx;
+  pc.off.reset();
+  pc.js.reset();
+  pc.vals.reset();
+  pc.kappa = -1;
+  pc.n_pairs = 0;
+  const int n = m.n;
+  std::vector<float4> hc((size_t)n);
+  for (int i = 0; i < n; ++i)
+    hc[i] = make_float4((float)m.h_centroid[3 * (size_t)i], (float)m.h_centroid[3 * (size_t)i + 1],
+                        (float)m.h_centroid[3 * (size_t)i + 2], 0.f);
+  DevBuf dc = upload(ctx, hc);
+  DevBuf dcount(ctx, sizeof(int32_t) * (size_t)n);
+  std::vector<int32_t> cnt((size_t)n);
+  const int grid = (n + 255) / 256;
+  // the list pass below must use exactly the r2 of the accepted count
+  float R = 0.f, r2 = 0.f;
+  int64_t total = -1;
+  for (int attempt = 0; attempt < 6 && total < 0; ++attempt) {
+    R = radius * std::pow(0.85f, (float)attempt);
+    r2 = R * R;
+    pair_cache_scan_kernel<<<grid, 256, 0, st>>>(n, dc.as<float4>(), r2, dcount.as<int32_t>(), nullptr, nullptr);
+    BP_LAUNCH_CHECK();
+    BP_CUDA(cudaMemcpyAsync(cnt.data(), dcount.get(), sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, st));
+    BP_CUDA(cudaStreamSynchronize(st));
+    int64_t t = 0;
+    for (int32_t c : cnt) t += c;
+    if ((double)t * (sizeof(int32_t) + 6 * sizeof(float)) <= kCacheMaxBytes) total = t;
+  }
+  if (total <= 0) return false;
+  std::vector<int64_t> off((size_t)n + 1, 0);
+  int max_row = 0;
+  for (int i = 0; i < n; ++i) {
+    off[i + 1] = off[i] + cnt[i];
+    max_row = std::max(max_row, (int)cnt[i]);
+  }
+  pc.off = upload(ctx, off);
+  pc.js.alloc(ctx, sizeof(int32_t) * (size_t)total);
+  BP_CUDA(cudaMemsetAsync(pc.js.get(), 0, sizeof(int32_t) * (size_t)total, st));
+  pc.vals.alloc(ctx, 6 * sizeof(float) * (size_t)total);
+  pair_cache_scan_kernel<<<grid, 256, 0, st>>>(n, dc.as<float4>(), r2, nullptr, pc.off.as<int64_t>(),
+                                               pc.js.as<int32_t>());
+  BP_LAUNCH_CHECK();
+  DevBuf dq = upload(ctx, m.h_qual_off), dp = upload(ctx, m.h_quad_off);
+  int max_q = 0;
+  for (int i = 0; i < n; ++i) max_q = std::max(max_q, m.h_qual_off[i + 1] - m.h_qual_off[i]);
+  const size_t smem = sizeof(float) * 8 * (size_t)std::max(1, max_q);
+  if (smem > 200 * 1024) throw std::invalid_argument("too many qualocation points per patch");
+  ensure_dynamic_smem((const void*)pair_cache_coef_kernel, smem);
+  pair_cache_coef_kernel<<<n, kAsmThreads, smem, st>>>(pc.off.as<int64_t>(), pc.js.as<int32_t>(), dq.as<int32_t>(),
+                                                       m.d_qual.as<double>(), m.n_qual_pts, dp.as<int32_t>(),
+                                                       m.d_quad.as<double>(), m.n_quad_pts, (float)kappa,
+                                                       pc.vals.as<float>());
+  BP_LAUNCH_CHECK();
+  BP_CUDA(cudaStreamSynchronize(st));  // the temporaries go back to the context
+  pc.kappa = kappa;
+  pc.radius = R;
+  pc.n_pairs = total;
+  pc.max_row = max_row;
+  return true;
+}
+
+}  // namespace
+
 static std::vector<NfItem> make_items(const Problem& P, int chunk) {
   const NearField& nf = P.nf;
   std::vector<NfItem> items;
@@ -766,6 +1128,52 @@ void nf_assemble(Problem& P) {
   P.d_diag.alloc(ctx, sizeof(double) * 4 * (size_t)P.n);
   nf.compact = !P.fp64 && (P.params.flags & BP_FLAG_COMPACT_NEARFIELD) != 0;
   if (!nf.on_demand) nf.coef.alloc(ctx, (nf.compact ? 12 : elem * 4) * (size_t)nf.n_pairs);
+  // mesh pair caches (built on the context's stream, before the assembly
+  // stream is released): a view per placement, the placement of each patch
+  int max_list = 0;
+  bool use_cache = false;
+  if (!P.fp64 && !nf.on_demand && (P.params.flags & BP_FLAG_MESH_PAIR_CACHE) && !P.placements.empty() &&
+      nf.max_cols < (1 << 24) && !asm_items.empty()) {
+    double hmin = 0;
+    for (const TreeNode& nd : P.tree.nodes)
+      if ((nd.flags & TREE_LEAF) && nd.content_count > 0) hmin = hmin > 0 ? std::min(hmin, nd.edge) : nd.edge;
+    const float radius = kCacheRadiusEdges * (float)hmin;
+    std::vector<CacheView> views;
+    std::vector<int32_t> inst_of((size_t)P.n, 0);
+    int first = 0;
+    for (size_t k = 0; k < P.placements.size(); ++k) {
+      DevMesh& m = *P.placements[k].mesh;
+      CacheView v{nullptr, nullptr, nullptr, first};
+      {
+        std::lock_guard<std::mutex> lk(m.mu);
+        bool ok = false;
+        try {
+          ok = radius > 0 && ensure_pair_cache(m, P.params.kappa, radius, ctx->stream);
+        } catch (const std::exception&) {  // no room for it: integrate as usual
+          m.pair_cache.off.reset();
+          m.pair_cache.js.reset();
+          m.pair_cache.vals.reset();
+          m.pair_cache.kappa = -1;
+          m.pair_cache.n_pairs = 0;
+        }
+        if (ok) {
+          v.off = m.pair_cache.off.as<int64_t>();
+          v.js = m.pair_cache.js.as<int32_t>();
+          v.vals = m.pair_cache.vals.as<float>();
+          max_list = std::max(max_list, m.pair_cache.max_row);
+          use_cache = true;
+        }
+      }
+      for (int i = 0; i < m.n && first + i < P.n; ++i) inst_of[(size_t)first + i] = (int32_t)k;
+      first += m.n;
+      views.push_back(v);
+    }
+    if (first != P.n || smem + sizeof(int32_t) * (size_t)max_list > 180 * 1024) use_cache = false;
+    if (use_cache) {
+      P.d_inst_of = upload(ctx, inst_of);
+      P.asm_views = upload(ctx, views);
+    }
+  }
   BP_CUDA(cudaEventRecord(P.asm_in, ctx->stream));
   const cudaStream_t st = P.asm_stream;
   BP_CUDA(cudaStreamWaitEvent(st, P.asm_in, 0));
@@ -802,6 +1210,22 @@ void nf_assemble(Problem& P) {
           nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual.as<double>(), nq,
           P.d_quad_off.as<int32_t>(), P.d_quad.as<double>(), np, P.d_eps.as<double>(), P.params.kappa,
           P.d_diag.as<double>(), CoefWriter<double, false>{nf.coef.as<double4>()});
+    } else if (use_cache) {
+      const size_t csmem = smem + sizeof(int32_t) * (size_t)max_list;
+      auto launch = [&](auto kernel, auto out) {
+        ensure_dynamic_smem((const void*)kernel, csmem);
+        kernel<<<(int)asm_items.size(), kAsmThreads, csmem, st>>>(
+            d_asm_items.as<NfItem>(), nf.rows.as<int32_t>(), nf.row_off.as<int64_t>(), nf.cols.as<int32_t>(),
+            nf.col_off.as<int64_t>(), nf.coef_off.as<int64_t>(), P.d_qual_off.as<int32_t>(), P.d_qual_f.as<float>(),
+            nq, P.d_quad_off.as<int32_t>(), P.d_quad_f.as<float>(), np, P.d_eps.as<double>(), (float)P.params.kappa,
+            P.d_inst_of.as<int32_t>(), P.asm_views.as<CacheView>(), max_list, max_tq, out);
+      };
+      if (nf.compact) {
+        uint2* p01 = nf.coef.as<uint2>();
+        launch(assemble_cached_kernel<true>, CoefWriter<float, true>{p01, reinterpret_cast<uint32_t*>(p01 + nf.n_pairs)});
+      } else {
+        launch(assemble_cached_kernel<false>, CoefWriter<float, false>{nf.coef.as<float4>()});
+      }
     } else if (nf.compact) {
       uint2* p01 = nf.coef.as<uint2>();
       const CoefWriter<float, true> out{p01, reinterpret_cast<uint32_t*>(p01 + nf.n_pairs)};
@@ -858,6 +1282,7 @@ void nf_join(Problem& P) {
   // later users of these blocks run on the context's stream, after the join
   P.asm_gc.reset();
   P.asm_items.reset();
+  P.asm_views.reset();
 }
 
 int nf_apply(Problem& P, const double* x_dev, double* y_dev, const double* yfar_dev, cudaStream_t stream) {

@@ -147,7 +147,7 @@ def _batch_worker(mesh_a, mesh_b, poses, chunks, kappa, precision, nbsize, devic
 def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float = 0.1, precision: str = "mixed",
                     nbsize: int | dict = DEFAULT_NBSIZE, workers: int = 4, device: int = 0, tol: float = 1e-6,
                     max_iterations: int = 100, contexts: list | None = None,
-                    snap_cube_edges: bool = False, batch: int = 1) -> ScanResult:
+                    snap_cube_edges: bool = False, batch: int = 1, cache_pairs: bool = False) -> ScanResult:
     """``nbsize``: the reference tree's nbsize, or a dict of BEEP tree keywords
     (``TuneResult.settings()`` of autotune).  ``contexts``: EngineContexts
     for the workers (at least ``workers``), kept
@@ -161,8 +161,15 @@ def rigid_body_scan(mesh_a: Mesh, mesh_b: Mesh, poses: list[Pose], kappa: float 
     as the scenarios of one batch problem (ScenarioBatch), sorted by
     separation so that a batch's common cube edge is close to each pose's
     own; a pose's energy then differs from its own problem's by the FMM's
-    truncation error (its tree is built in the batch's cube)."""
+    truncation error (its tree is built in the batch's cube).
+    ``cache_pairs`` (mixed precision): each worker's meshes keep the
+    near-field coefficients of their own close patch pairs
+    (BEEP(cache_mesh_pairs=True)), so a pose integrates only the pairs the
+    cache does not hold; energies agree with the uncached scan to FP32
+    rounding."""
     t0 = time.perf_counter()
+    if cache_pairs:
+        nbsize = dict(_tree_kw(nbsize), cache_mesh_pairs=True)
     ident = np.array([1.0, 0.0, 0.0, 0.0])
     ca = mesh_a.centre
     workers = max(1, min(workers, len(poses)))

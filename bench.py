@@ -561,11 +561,13 @@ def _scan_mode(args, local):
         # warm-up: a scan of as many other poses, so that every context has
         # seen problems of the sizes the timed scan builds
         rigid_body_scan(ma, mb, random_poses(args.poses, seed=99), kappa=0.1, workers=args.workers, device=local,
-                        contexts=ctxs, snap_cube_edges=snap, batch=args.batch, nbsize=tree)
+                        contexts=ctxs, snap_cube_edges=snap, batch=args.batch, nbsize=tree,
+                        cache_pairs=args.cache_pairs)
         # a scan of 64 poses lasts about a second, and host threads make it
         # vary from run to run: the median of three timed scans
         runs = [rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs,
-                                snap_cube_edges=snap, batch=args.batch, nbsize=tree) for _ in range(3)]
+                                snap_cube_edges=snap, batch=args.batch, nbsize=tree, cache_pairs=args.cache_pairs)
+                for _ in range(3)]
         runs.sort(key=lambda r: r.poses_per_s)
         res = runs[1]
     finally:
@@ -581,6 +583,7 @@ def _scan_mode(args, local):
                    "poses": len(poses), "workers": args.workers,
                    "poses_per_batch": args.batch,
                    "engine_contexts": "one per worker, kept across scans",
+                   "mesh_pair_cache": bool(args.cache_pairs),
                    "cube_edges": "exact per pose" if args.exact_cubes else
                                  "rounded up to 2^(k/8): poses share far-field plans"},
         "seconds": res.seconds, "mean_iterations": float(np.mean(res.iterations)),
@@ -819,6 +822,8 @@ def main():
                          "for all")
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
+    ap.add_argument("--cache-pairs", action="store_true",
+                    help="scan: the meshes keep their own close pairs' near-field coefficients")
     ap.add_argument("--compact", action="store_true",
                     help="profiling mode: the compact (24-bit) near-field coefficients")
     ap.add_argument("--no-cpu-baseline", action="store_true")

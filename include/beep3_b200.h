@@ -158,7 +158,21 @@ enum bp_flags {
    * memory and traffic per matvec for a relative error of at most 2^-16 per
    * coefficient.  Combined with BP_PREC_FP64 or
    * BP_FLAG_NEARFIELD_ON_DEMAND the call fails with BP_ERR_INVALID. */
-  BP_FLAG_COMPACT_NEARFIELD = 4
+  BP_FLAG_COMPACT_NEARFIELD = 4,
+  /* Mixed engine, problems posed from device meshes (bp_problem_create_posed,
+   * bp_problem_create_batch): the near-field coefficients of the pairs of
+   * patches of one mesh closer than about 4.4 edges of the problem's
+   * smallest leaf are integrated once, in the mesh's frame, kept with the
+   * mesh (per kappa; 28 bytes a pair, at most 8 GB a mesh) and looked up by
+   * the assembly of every later problem with that mesh, whatever its pose:
+   * a rigid move does not change them.  The other pairs are integrated as
+   * usual.  No counterpart in the reference, which integrates every pair of
+   * every problem (src/beep/beep.cpp:768-956); results agree with the
+   * uncached assembly to FP32 rounding (the pairs' coordinates are those of
+   * the mesh's frame, not the posed ones).  Ignored by the FP64 engine, the
+   * on-demand near field and meshes with more than one quadrature point per
+   * patch. */
+  BP_FLAG_MESH_PAIR_CACHE = 8
 };
 
 typedef struct {
