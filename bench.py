@@ -300,9 +300,9 @@ def child_line(local: int, args: list, keys: tuple) -> dict:
 
 def scan_child(local: int) -> dict:
     """Config B's batched rigid-body scan (64 poses of the two star
-    molecules, 2 workers x 8 poses per batch problem, the meshes keeping
+    molecules, 4 workers x 4 poses per batch problem, the meshes keeping
     their own close pairs' coefficients)."""
-    return child_line(local, ["--workload", "scan", "--workers", "2", "--batch", "8", "--cache-pairs"],
+    return child_line(local, ["--workload", "scan", "--workers", "4", "--batch", "4", "--cache-pairs"],
                       ("value", "unit", "seconds", "mean_iterations", "config"))
 
 
