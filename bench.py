@@ -540,6 +540,8 @@ def _scan_mode(args, local):
     # device blocks of a pose stay on the device for the next
     ctxs = [b.EngineContext(local) for _ in range(args.workers)]
     tree = 1500  # the reference's nbsize
+    if args.compact:
+        tree = dict(nbsize=1500, compact_nearfield=True)
     tuned = None
     try:
         snap = not args.exact_cubes
@@ -585,6 +587,7 @@ def _scan_mode(args, local):
                    "poses_per_batch": args.batch,
                    "engine_contexts": "one per worker, kept across scans",
                    "mesh_pair_cache": bool(args.cache_pairs),
+                   "compact_nearfield": bool(args.compact),
                    "cube_edges": "exact per pose" if args.exact_cubes else
                                  "rounded up to 2^(k/8): poses share far-field plans"},
         "seconds": res.seconds, "mean_iterations": float(np.mean(res.iterations)),
@@ -826,7 +829,7 @@ def main():
     ap.add_argument("--cache-pairs", action="store_true",
                     help="scan: the meshes keep their own close pairs' near-field coefficients")
     ap.add_argument("--compact", action="store_true",
-                    help="profiling mode: the compact (24-bit) near-field coefficients")
+                    help="profiling and scan modes: the compact (24-bit) near-field coefficients")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scan", action="store_true",
                     help="leave out the config-B scan and config-R serving keys of the default line")
