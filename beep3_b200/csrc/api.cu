@@ -695,11 +695,10 @@ BP_API int32_t bp_matvec(bp_problem p, const double* x, double* y) {
     BP_CUDA(cudaMemcpyAsync(P->d_gx.get(), x, bytes, cudaMemcpyHostToDevice, st));
     matvec_device(*P, P->d_gx.as<double>(), P->d_gy.as<double>());
     BP_CUDA(cudaMemcpyAsync(y, P->d_gy.get(), bytes, cudaMemcpyDeviceToHost, st));
-    int flag = 0;
-    if (const int* sd = fmm_status_dev(*P))
-      BP_CUDA(cudaMemcpyAsync(&flag, sd, sizeof(int), cudaMemcpyDeviceToHost, st));
+    const int* sd = fmm_status_dev(*P);
+    if (sd) BP_CUDA(cudaMemcpyAsync(P->h_status, sd, sizeof(int), cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
-    fmm_raise_if(*P, flag);
+    fmm_raise_if(*P, sd ? *P->h_status : 0);
     return BP_OK;
   });
 }
@@ -745,11 +744,10 @@ static int32_t solve_host(bp_problem p, const double* rhs, double* x, double tol
     std::vector<int> its(P->n_scen(), 0);
     gmres_device(*P, b.as<double>(), P->d_x.as<double>(), tol, max_iters, restart, rr.data(), its.data(), x0);
     BP_CUDA(cudaMemcpyAsync(x, P->d_x.get(), bytes, cudaMemcpyDeviceToHost, st));
-    int flag = 0;
-    if (const int* sd = fmm_status_dev(*P))
-      BP_CUDA(cudaMemcpyAsync(&flag, sd, sizeof(int), cudaMemcpyDeviceToHost, st));
+    const int* sd = fmm_status_dev(*P);
+    if (sd) BP_CUDA(cudaMemcpyAsync(P->h_status, sd, sizeof(int), cudaMemcpyDeviceToHost, st));
     BP_CUDA(cudaStreamSynchronize(st));
-    fmm_raise_if(*P, flag);
+    fmm_raise_if(*P, sd ? *P->h_status : 0);
     const double worst = *std::max_element(rr.begin(), rr.end());
     if (scenario_out) {  // bp_solve_batch: per scenario
       std::copy(its.begin(), its.end(), iterations);

@@ -379,6 +379,7 @@ struct Problem {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool graph_failed = false;
+  int* h_status = nullptr;  // pinned host word: the far field's status read back behind a result
   // Krylov workspace
   DevBuf d_V, d_w, d_scal, d_seg;
   // one GMRES cycle's Arnoldi loop as a graph with a device-side WHILE node
@@ -414,6 +415,7 @@ struct Problem {
       if (mesh_release(pl.mesh)) delete pl.mesh;
     if (graph) cudaGraphExecDestroy(graph);
     if (gmres_graph) cudaGraphExecDestroy(gmres_graph);
+    if (h_status) cudaFreeHost(h_status);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);

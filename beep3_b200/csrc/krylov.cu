@@ -439,6 +439,9 @@ void matvec_setup(Problem& P) {
   BP_CUDA(cudaStreamCreateWithPriority(&P.side, cudaStreamNonBlocking, hi));
   BP_CUDA(cudaEventCreateWithFlags(&P.ev_fork, cudaEventDisableTiming));
   BP_CUDA(cudaEventCreateWithFlags(&P.ev_join, cudaEventDisableTiming));
+  // a pinned word, so that reading the status behind a result is a plain
+  // asynchronous copy, not a staged one
+  BP_CUDA(cudaHostAlloc((void**)&P.h_status, sizeof(int), cudaHostAllocDefault));
 }
 
 // One matvec as kernel launches: the near field on `main` (writes y), the
