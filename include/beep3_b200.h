@@ -163,9 +163,11 @@ enum bp_flags {
    * bp_problem_create_batch): the near-field coefficients of the pairs of
    * patches of one mesh closer than about 4.4 edges of the problem's
    * smallest leaf are integrated once, in the mesh's frame, kept with the
-   * mesh (per kappa; 28 bytes a pair, at most 8 GB a mesh) and looked up by
-   * the assembly of every later problem with that mesh, whatever its pose:
-   * a rigid move does not change them.  The other pairs are integrated as
+   * mesh (for one kappa at a time, at the radius of the problem that built
+   * them; 28 bytes a pair, at most 8 GB a mesh, the radius shrunk to fit)
+   * and looked up by the assembly of every later problem with that mesh and
+   * kappa, whatever its pose: a rigid move does not change them.  A cache
+   * that does not fit the context's budget is not built.  The other pairs are integrated as
    * usual.  No counterpart in the reference, which integrates every pair of
    * every problem (src/beep/beep.cpp:768-956); results agree with the
    * uncached assembly to FP32 rounding (the pairs' coordinates are those of
