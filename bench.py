@@ -314,7 +314,7 @@ def serve_child(local: int) -> dict:
 
 
 def matvec_roofline(inf, n, mv_ms, near_ms, stage_ms, hbm, peaks):
-    """The whole matvec against HBM with the survey's algorithmic bytes,
+    """The whole matvec against HBM with its algorithmic bytes,
     B_mv = P_nf (16 B coefficients + 4 B column id) + 4N x 8 B (x, y) + B_fmm,
     B_fmm = nodes x 12 channels x (2 x E x 8 B (M, L read + write) + 6 x np x
     2 x 8 B (plane waves written and read)), FP32 complex; and the far field

@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 # tolerances: FP64 path vs the FP64 oracle (same formulas, different
 # summation order); mixed path (FP32 near field) vs the reference-faithful
-# FP32 oracle at the north-star bars (1e-5 on f/h, 1e-4 on energy)
+# FP32 oracle at the parity bars (1e-5 on f/h, 1e-4 on energy)
 TOL_FP64 = 1e-10
 TOL_MIXED = 1e-5
 
