@@ -155,14 +155,18 @@ class ScenarioBatch:
         self.rhs = rhs
         return rhs
 
-    def solve(self, gmres_stop_criteria: float = 1e-6, max_iterations: int = 100, restart: int = 0) -> BatchSolve:
-        """Right-hand sides, then every scenario's GMRES in shared launches."""
+    def solve(self, gmres_stop_criteria: float = 1e-6, max_iterations: int = 100, restart: int = 0,
+              x0=None) -> BatchSolve:
+        """Right-hand sides, then every scenario's GMRES in shared launches,
+        from ``x0`` (the batch's f for all patches, then h) or from zero."""
         p = self.build()
         t0 = time.perf_counter()
         self.set_rhs()
         t1 = time.perf_counter()
         S = len(self.scenarios)
         x = np.zeros(2 * self.num_patches)
+        if x0 is not None:
+            x[:] = np.asarray(x0, float).reshape(-1)
         its = np.zeros(S, np.int32)
         rr = np.zeros(S)
         code = N.lib().bp_solve_batch(p, N.ptr(self.rhs), N.ptr(x), gmres_stop_criteria, max_iterations, restart,

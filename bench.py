@@ -565,11 +565,12 @@ def _scan_mode(args, local):
         # seen problems of the sizes the timed scan builds
         rigid_body_scan(ma, mb, random_poses(args.poses, seed=99), kappa=0.1, workers=args.workers, device=local,
                         contexts=ctxs, snap_cube_edges=snap, batch=args.batch, nbsize=tree,
-                        cache_pairs=args.cache_pairs)
+                        cache_pairs=args.cache_pairs, warm_start=args.warm_start)
         # a scan of 64 poses lasts about a second, and host threads make it
         # vary from run to run: the median of three timed scans
         runs = [rigid_body_scan(ma, mb, poses, kappa=0.1, workers=args.workers, device=local, contexts=ctxs,
-                                snap_cube_edges=snap, batch=args.batch, nbsize=tree, cache_pairs=args.cache_pairs)
+                                snap_cube_edges=snap, batch=args.batch, nbsize=tree, cache_pairs=args.cache_pairs,
+                                warm_start=args.warm_start)
                 for _ in range(3)]
         runs.sort(key=lambda r: r.poses_per_s)
         res = runs[1]
@@ -588,6 +589,7 @@ def _scan_mode(args, local):
                    "engine_contexts": "one per worker, kept across scans",
                    "mesh_pair_cache": bool(args.cache_pairs),
                    "compact_nearfield": bool(args.compact),
+                   "warm_start": bool(args.warm_start),
                    "cube_edges": "exact per pose" if args.exact_cubes else
                                  "rounded up to 2^(k/8): poses share far-field plans"},
         "seconds": res.seconds, "mean_iterations": float(np.mean(res.iterations)),
@@ -826,6 +828,8 @@ def main():
                          "for all")
     ap.add_argument("--workers", type=int, default=4, help="scan / serve: concurrent solves")
     ap.add_argument("--only-matvec", action="store_true", help="profiling mode: matvecs of the mixed engine only")
+    ap.add_argument("--warm-start", action="store_true",
+                    help="scan: every pose's GMRES starts from the isolated molecules' solutions")
     ap.add_argument("--cache-pairs", action="store_true",
                     help="scan: the meshes keep their own close pairs' near-field coefficients")
     ap.add_argument("--compact", action="store_true",

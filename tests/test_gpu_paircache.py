@@ -110,3 +110,26 @@ def test_batch_and_scan_with_the_cache():
     finally:
         for c in ctxs:
             c.close()
+
+
+@pytest.mark.parametrize("batch", [1, 2])
+def test_scan_warm_start(batch):
+    """Poses started from the isolated molecules' solutions: fewer GMRES
+    iterations, energies within the GMRES tolerance's reach (1e-5) of the
+    scan started from zero."""
+    ma, mb = meshes()
+    poses = random_poses(4, seed=508)
+    for p in poses:
+        p.offset = p.offset / np.linalg.norm(p.offset) * 40.0
+    ctxs = [b.EngineContext(0), b.EngineContext(0)]
+    try:
+        cold = rigid_body_scan(ma, mb, poses, kappa=0.1, nbsize=300, workers=2, contexts=ctxs, batch=batch)
+        warm = rigid_body_scan(ma, mb, poses, kappa=0.1, nbsize=300, workers=2, contexts=ctxs, batch=batch,
+                               warm_start=True)
+        e0, e1 = np.array(cold.complex_energies), np.array(warm.complex_energies)
+        assert np.all(np.abs(e1 - e0) <= 1e-5 * np.abs(e0))
+        assert abs(warm.e_a - cold.e_a) <= 1e-9 * abs(cold.e_a)
+        assert np.mean(warm.iterations) < np.mean(cold.iterations)
+    finally:
+        for c in ctxs:
+            c.close()
