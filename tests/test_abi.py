@@ -92,3 +92,14 @@ def test_batch_entry_points_validate_arguments():
     its = np.zeros(2, np.int32)
     rr = np.zeros(2)
     assert L.bp_solve_batch(None, N.ptr(rhs), N.ptr(x), 1e-6, 10, 0, N.ptr(its), N.ptr(rr)) == N.BP_ERR_INVALID
+
+
+def test_header_constants_match_the_binding():
+    """Every enum constant of the C header (status codes, precisions, flags)
+    has the same value in the Python binding."""
+    h = (Path(__file__).resolve().parents[1] / "include" / "beep3_b200.h").read_text()
+    h = re.sub(r"/\*.*?\*/", "", h, flags=re.S)
+    consts = dict((k, int(v)) for k, v in re.findall(r"\b(BP_[A-Z0-9_]+)\s*=\s*(\d+)", h))
+    assert {"BP_OK", "BP_ERR_NOT_CONVERGED", "BP_PREC_MIXED", "BP_FLAG_MESH_PAIR_CACHE"} <= set(consts)
+    for k, v in consts.items():
+        assert getattr(N, k) == v, k
